@@ -1,0 +1,290 @@
+/*
+ * higflow_b200 — C ABI of the B200 (sm_100a) engine for HigFlow's per-time-step
+ * hot path: explicit intermediate velocity, kernel-conformation constitutive
+ * update, pressure-Poisson projection.
+ *
+ * Two layers are exposed, both with plain pointers and sizes only:
+ *
+ *  1. The step engine (hf_case_*): consumes a flattened "step program" — every
+ *     stencil query one reference time step makes, recorded once from HigTree's
+ *     own stencil builder — and runs whole time steps on the GPU with the fields
+ *     resident in HBM.  It replaces, per step,
+ *        higflow_solver_step               higflow/src/hig-flow-step.c:1363-1413
+ *        higflow_solver_step_viscoelastic  higflow/src/hig-flow-step-viscoelastic.c:2091-2163
+ *     for the configurations listed under hf_params.
+ *
+ *  2. The linear-solver engine (hf_slv_*): a GPU implementation of HigTree's
+ *     solver plugin, one entry point per slot of _solver_vtable
+ *     (higtree/src/solver.h:42-60), for callers that keep assembling the
+ *     Poisson system on the host (solver.c:38-202 call sites).
+ *
+ * Every function returns an int status: 0 on success, a negative HF_ERR_* code
+ * otherwise (the reference has no status returns; it exits, utils.h:46-52).
+ * No entry point falls back to the CPU: without a usable CUDA device the
+ * create calls return HF_ERR_NO_DEVICE.
+ */
+#ifndef HIGFLOW_B200_H
+#define HIGFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+#define HF_OK                  0
+#define HF_ERR_INVALID        -1  /* malformed program / argument            */
+#define HF_ERR_UNSUPPORTED    -2  /* configuration outside the GPU path       */
+#define HF_ERR_NOT_CONVERGED  -3  /* Poisson solve hit its iteration limit    */
+#define HF_ERR_NAN            -4  /* NaN/Inf detected in a field or residual  */
+#define HF_ERR_OOM_BUDGET     -5  /* request exceeds the HBM budget           */
+#define HF_ERR_CUDA           -6  /* CUDA runtime error                       */
+#define HF_ERR_NO_DEVICE      -7  /* no CUDA device / extension unusable      */
+#define HF_ERR_TIMEOUT        -8  /* a bounded device-side wait gave up       */
+
+/* ------------------------------------------------------------------ */
+/* enumerations mirroring the reference's controllers                 */
+/* (higflow/src/hig-flow-kernel.h:27-31, 152-193, 295-313)             */
+/* ------------------------------------------------------------------ */
+enum { HF_NEWTONIAN = 0, HF_VISCOELASTIC = 3 };                 /* flow_type      */
+enum { HF_NON_INCREMENTAL = 0, HF_INCREMENTAL = 1 };            /* projection     */
+enum { HF_CENTRAL = 0, HF_FIRST_ORDER = 1, HF_SECOND_ORDER = 2 };/* convecdiscr   */
+enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order   */
+enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2 };        /* VE model       */
+enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
+enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
+
+/* precision forms */
+enum {
+    HF_PREC_FP64 = 0,   /* plain: every gather, update and Poisson iterate in FP64 */
+    HF_PREC_MIXED = 1   /* FP32 stencil gathers + FP32 inner PCG inside FP64
+                           iterative refinement; FP64 eigen/kernel transform,
+                           outer residual and time accumulation              */
+};
+
+/* Poisson solver choice */
+enum {
+    HF_POISSON_AUTO = 0,    /* CG when the reduced matrix is symmetric, else BiCGStab */
+    HF_POISSON_CG = 1,
+    HF_POISSON_BICGSTAB = 2
+};
+
+/* ------------------------------------------------------------------ */
+/* step-program slot layouts                                           */
+/*                                                                     */
+/* A slot holds one recorded stencil query as an int32 code:           */
+/*   code >= 0 : the query is a centre hit with weight 1 and no        */
+/*               boundary term; its value is field[code]               */
+/*   code <  0 : general query r = -code-1; its value is               */
+/*               -rhs[r] + sum_k w[k]*field[col[k]], k in row r,       */
+/*               accumulated in that order (pdomain.c:1026-1053)       */
+/* Which field a slot reads is fixed by its position (listed below).   */
+/* Slot arrays are slot-major: slots[s * nelem + e].                   */
+/* ------------------------------------------------------------------ */
+
+/* Velocity stage, one element per facet normal to d
+ * (higflow_computational_cell, higflow/src/hig-flow-discret.c:86-259;
+ *  higflow_computational_cell_viscoelastic, :541-569). */
+#define HF_V_FU   0   /* facet source FU[d] at the facet centre (sfdF[d])         */
+#define HF_V_PL   1   /* p at centre - 0.5*delta_d (sdp); reused for dp in the    */
+#define HF_V_PR   2   /*   final velocity (hig-flow-step.c:242-308)               */
+#define HF_V_FL   3   /* cell source F at centre -/+ 0.5*delta_d (sdF)           */
+#define HF_V_FR   4
+#define HF_V_BLK0 5   /* first per-direction block                                */
+#define HF_V_NB   10  /* slots per direction d2:                                  */
+#define HF_V_V4   0   /*   +0..3 u[d2] at (+,+),(+,-),(-,+),(-,-) half-deltas in  */
+                      /*         (d, d2)  (compute_facet_u_2, hig-flow-eval.c:65) */
+#define HF_V_UL   4   /*   +4 u[d] at centre - 1*delta_d2                         */
+#define HF_V_UR   5   /*   +5 u[d] at centre + 1*delta_d2                         */
+#define HF_V_ULL  6   /*   +6 u[d] at centre - 2*delta_d2                         */
+#define HF_V_URR  7   /*   +7 u[d] at centre + 2*delta_d2                         */
+#define HF_V_VCR  8   /*   +8 u[d2] at centre + 0.5*delta_d2 (CUBISTA v1bar)      */
+#define HF_V_VCL  9   /*   +9 u[d2] at centre - 0.5*delta_d2 (CUBISTA v2bar)      */
+#define HF_V_NSLOT_NEWT(D) (HF_V_BLK0 + HF_V_NB * (D))
+/* viscoelastic extension, per direction d2, on S[d][d2] (sdED):
+ *   +0 SL_A  +1 SL_B  +2 SR_A  +3 SR_B
+ *   d2 == d : SL_A = centre - 0.5*delta_d, SR_A = centre + 0.5*delta_d
+ *   d2 != d : compute_center_p_left_2 / _right_2 (hig-flow-eval.c:454-487):
+ *             SL_A/SL_B at d2 - delta_d2 with d -/+ 0.5*delta_d,
+ *             SR_A/SR_B at d2 + delta_d2 with d -/+ 0.5*delta_d            */
+#define HF_V_NS   4
+#define HF_V_NSLOT_VE(D) (HF_V_NSLOT_NEWT(D) + HF_V_NS * (D))
+/* velocity-stage flag bits: for direction d2, bit 4*d2+k is the infacet
+ * flag of UL, UR, ULL, URR (k = 0..3) (sfd_get_facet_with_point)          */
+
+/* Divergence stage, one element per cell: u*[d] at centre -/+ 0.5*delta_d
+ * (higflow_pressure, hig-flow-step.c:58-80). */
+#define HF_P_UL(d) (2 * (d))
+#define HF_P_UR(d) (2 * (d) + 1)
+#define HF_P_NSLOT(D) (2 * (D))
+
+/* Viscoelastic cell stage, one element per cell
+ * (higflow_compute_velocity_derivative_tensor, hig-flow-step-generalized-
+ *  newtonian.c:14-97; higflow_explicit_euler_constitutive_equation,
+ *  hig-flow-step-viscoelastic.c:352-544; higflow_compute_polymeric_tensor,
+ *  :212-347; hig_flow_convective_cell_term_cubista, hig-flow-step.c:1185). */
+#define HF_C_SELF 0   /* Du, S, Kernel at the cell centre (sdED)                  */
+#define HF_C_BLK0 1
+#define HF_C_NB   6   /* per direction d:                                         */
+#define HF_C_UVL  0   /*   +0 u[d] at centre - 0.5*delta_d                        */
+#define HF_C_UVR  1   /*   +1 u[d] at centre + 0.5*delta_d                        */
+#define HF_C_KL   2   /*   +2 Kernel at centre - delta_d   (sdED)                 */
+#define HF_C_KR   3   /*   +3 Kernel at centre + delta_d                          */
+#define HF_C_KLL  4   /*   +4 Kernel at centre - 2*delta_d                        */
+#define HF_C_KRR  5   /*   +5 Kernel at centre + 2*delta_d                        */
+/* then, for each ordered pair (d, d2), d2 != d, in row-major order, 4 slots on
+ * u[d] for the corner values of compute_facet_u_4_left/_right
+ * (hig-flow-eval.c:95-195):
+ *   +0 (d + 0.5, d2 - 1)  +1 (d - 0.5, d2 - 1)  +2 (d + 0.5, d2 + 1)  +3 (d - 0.5, d2 + 1)
+ * (in units of delta); the (d -/+ 0.5, d2) values are UVL/UVR.              */
+#define HF_C_NQ   4
+#define HF_C_NSLOT(D) (HF_C_BLK0 + HF_C_NB * (D) + HF_C_NQ * (D) * ((D) - 1))
+/* cell-stage flag bits: for direction d, bit 4*d+k is the incell flag of
+ * KL, KR, KLL, KRR (k = 0..3) (sd_get_cell_with_point != NULL)             */
+
+/* field identifiers for hf_case_set_field / hf_case_get_field */
+enum {
+    HF_FIELD_U = 0,       /* comp = d: facet velocity u[d]                   */
+    HF_FIELD_USTAR = 1,   /* comp = d: intermediate velocity u*[d]           */
+    HF_FIELD_P = 2,       /* cell pressure                                   */
+    HF_FIELD_DP = 3,      /* cell pressure increment (incremental projection)*/
+    HF_FIELD_F = 4,       /* cell source term                                */
+    HF_FIELD_FU = 5,      /* comp = d: facet source term                     */
+    HF_FIELD_KERNEL = 6,  /* comp = i*D+j: kernel tensor                      */
+    HF_FIELD_S = 7,       /* comp = i*D+j: polymeric tensor                  */
+    HF_FIELD_DU = 8       /* comp = i*D+j: velocity-gradient tensor          */
+};
+
+/* physical and numerical parameters (hig-flow-kernel.h:108-214, 425-457) */
+typedef struct hf_params {
+    int32_t dim;                  /* 2 or 3                                  */
+    int32_t flowtype;             /* HF_NEWTONIAN / HF_VISCOELASTIC          */
+    int32_t projtype;             /* HF_INCREMENTAL / HF_NON_INCREMENTAL     */
+    int32_t convecdiscrtype;      /* HF_CENTRAL / HF_FIRST_ORDER / HF_SECOND_ORDER */
+    int32_t secondconvecdiscrtype;/* HF_MCU / HF_CUBISTA / HF_QUICK          */
+    int32_t ve_model;             /* HF_OLDROYD_B / HF_GIESEKUS / HF_LPTT    */
+    int32_t ve_convecdiscrtype;   /* HF_CELL_CENTRAL / HF_CELL_CUBISTA       */
+    int32_t kernel;               /* HF_KERNEL_*                             */
+    double Re, dt;
+    double De, beta, kernel_tol, alpha, epsilon, xi;
+} hf_params;
+
+/* A flattened step program (host memory, read-only for the engine). */
+typedef struct hf_program {
+    hf_params par;
+    int32_t ncell;                 /* leaf cells (pressure unknowns)           */
+    int32_t nfacet[3];             /* interior facets normal to each direction */
+
+    /* distinct cell/facet deltas; elements store an index into these tables */
+    int32_t ndelta;
+    const double *delta;           /* ndelta * dim                             */
+
+    /* general stencil rows, deduplicated by content */
+    int64_t nrows;
+    int64_t nnz;
+    const int64_t *row_ptr;        /* nrows + 1 */
+    const int32_t *row_col;        /* nnz       */
+    const double  *row_w;          /* nnz       */
+    const double  *row_rhs;        /* nrows     */
+
+    /* velocity stage per direction d < dim */
+    int32_t vel_nslot;             /* HF_V_NSLOT_NEWT or HF_V_NSLOT_VE         */
+    const int32_t  *vel_slots[3];  /* vel_nslot * nfacet[d], slot-major        */
+    const uint32_t *vel_flags[3];  /* nfacet[d]                                */
+    const uint16_t *vel_delta[3];  /* nfacet[d]: index into delta              */
+
+    /* divergence stage */
+    const int32_t  *div_slots;     /* HF_P_NSLOT * ncell                       */
+    const uint16_t *cell_delta;    /* ncell: index into delta                  */
+
+    /* Poisson matrix (global ids == cell ids on one rank), constant per mesh */
+    int64_t pnnz;
+    const int64_t *p_ptr;          /* ncell + 1 */
+    const int32_t *p_col;          /* pnnz      */
+    const double  *p_val;          /* pnnz      */
+    const double  *p_brhs;         /* ncell: boundary part of each row's rhs   */
+    int32_t pin_row;               /* desingularised row, -1 if none           */
+    double  pin_value;             /* get_pressure at the pinned cell centre   */
+
+    /* viscoelastic cell stage (flowtype == HF_VISCOELASTIC) */
+    int32_t cell_nslot;            /* HF_C_NSLOT(dim) or 0                     */
+    const int32_t  *cell_slots;    /* cell_nslot * ncell                       */
+    const uint32_t *cell_flags;    /* ncell                                    */
+} hf_program;
+
+/* ------------------------------------------------------------------ */
+/* step engine                                                         */
+/* ------------------------------------------------------------------ */
+typedef struct hf_case hf_case;
+
+typedef struct hf_options {
+    int32_t precision;        /* HF_PREC_FP64 / HF_PREC_MIXED                 */
+    int32_t poisson;          /* HF_POISSON_*                                 */
+    double  poisson_rtol;     /* relative residual target (reference: 1e-10)  */
+    double  poisson_atol;     /* absolute residual target (reference: 1e-10)  */
+    int32_t poisson_maxit;    /* iteration cap; 0 = 20000                      */
+    int32_t device;           /* CUDA device ordinal                          */
+} hf_options;
+
+typedef struct hf_stats {
+    int64_t steps;            /* steps taken since create                      */
+    int32_t last_iters;       /* Poisson iterations of the last step (inner)   */
+    int32_t last_outer;       /* refinement sweeps of the last step (mixed)    */
+    double  last_residual;    /* relative true residual of the last solve      */
+    int64_t total_iters;      /* all Poisson iterations since create           */
+    int64_t kernel_launches;  /* kernels launched by hf_case_step so far       */
+    double  device_bytes;     /* HBM held by this case                         */
+} hf_stats;
+
+/* Replaces higflow_solver_step / _viscoelastic for one case.
+ * hf_case_create copies the program to the device; the program memory can be
+ * freed afterwards.  Fields start at zero; set them with hf_case_set_field. */
+int  hf_case_create(const hf_program *prog, const hf_options *opt, hf_case **out);
+int  hf_case_set_field(hf_case *c, int32_t field, int32_t comp, const double *host, int64_t n);
+int  hf_case_get_field(hf_case *c, int32_t field, int32_t comp, double *host, int64_t n);
+/* Advance nsteps time steps (each one the full reference sub-step order). */
+int  hf_case_step(hf_case *c, int32_t nsteps);
+int  hf_case_stats(hf_case *c, hf_stats *out);
+int  hf_case_synchronize(hf_case *c);
+void hf_case_destroy(hf_case *c);
+
+/* Device memory the engine would hold for a program (admission control). */
+int  hf_case_device_bytes(const hf_program *prog, const hf_options *opt, int64_t *bytes);
+
+/* Last error message of the calling thread (static storage). */
+const char *hf_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* linear-solver engine: one entry point per _solver_vtable slot       */
+/* (higtree/src/solver.h:42-87).  Row/column indices are global ids in */
+/* [first_gid, first_gid + size).                                      */
+/* ------------------------------------------------------------------ */
+typedef struct hf_slv hf_slv;
+
+int  hf_slv_create(int32_t first_gid, int32_t size, hf_slv **out);             /* _slv_create_petsc */
+int  hf_slv_set_maxnonzeros(hf_slv *s, int32_t maxnz);                         /* set_maxnonzeros   */
+int  hf_slv_set_Ai(hf_slv *s, int32_t i, int32_t numjs, const int32_t *j, const double *v); /* set_Ai */
+int  hf_slv_set_bi(hf_slv *s, int32_t i, double v);                            /* set_bi            */
+int  hf_slv_add_bi(hf_slv *s, int32_t i, double v);                            /* add_bi            */
+int  hf_slv_set_xi(hf_slv *s, int32_t i, double v);                            /* set_xi            */
+int  hf_slv_set_x(hf_slv *s, const double *x);                                 /* set_x             */
+int  hf_slv_get_xi(hf_slv *s, int32_t i, double *v);                           /* get_xi            */
+int  hf_slv_get_x(hf_slv *s, double *x);                                       /* get_x             */
+int  hf_slv_get_x_scatter(hf_slv *s, int32_t size, const int32_t *idx, double *x); /* get_x_scatter */
+int  hf_slv_assemble_matrix(hf_slv *s);                                        /* assemble_matrix   */
+int  hf_slv_assemble_rhs(hf_slv *s);                                           /* assemble_rhs      */
+int  hf_slv_assemble_output(hf_slv *s);                                        /* assemble_output   */
+int  hf_slv_set_tolerances(hf_slv *s, double rtol, double atol, int32_t maxit);
+int  hf_slv_solve(hf_slv *s);                                                  /* solve             */
+int  hf_slv_result(hf_slv *s, int32_t *iterations, double *residual, int32_t *converged);
+void hf_slv_destroy(hf_slv *s);                                                /* destroy           */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
