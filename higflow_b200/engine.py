@@ -1,0 +1,113 @@
+"""Python binding of the B200 step engine (``libhigflow_b200.so``).
+
+``Case`` wraps ``hf_case_*`` from ``include/higflow_b200.h``: it uploads a
+flattened step program, holds the fields in HBM and advances whole HigFlow
+time steps on the GPU.  There is no CPU path: if the CUDA library or a device
+is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import program as hp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "lib", "libhigflow_b200.so")
+
+_lib: Optional[C.CDLL] = None
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"higflow_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Load the in-tree engine library (built by ``higflow_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise EngineError(-7, f"engine library not built: {LIBPATH}")
+        L = C.CDLL(LIBPATH)
+        P, V = C.POINTER, C.c_void_p
+        L.hf_last_error.restype = C.c_char_p
+        L.hf_case_create.argtypes = [P(hp.HFProgram), P(hp.HFOptions), P(V)]
+        L.hf_case_set_field.argtypes = [V, C.c_int32, C.c_int32, P(C.c_double), C.c_int64]
+        L.hf_case_get_field.argtypes = [V, C.c_int32, C.c_int32, P(C.c_double), C.c_int64]
+        L.hf_case_step.argtypes = [V, C.c_int32]
+        L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
+        L.hf_case_synchronize.argtypes = [V]
+        L.hf_case_destroy.argtypes = [V]
+        L.hf_case_destroy.restype = None
+        L.hf_case_device_bytes.argtypes = [P(hp.HFProgram), P(hp.HFOptions), P(C.c_int64)]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise EngineError(rc, lib().hf_last_error().decode(errors="replace"))
+
+
+def options(precision: int = hp.PREC_FP64, poisson: int = hp.POISSON_AUTO, rtol: float = 1e-10,
+            atol: float = 1e-10, maxit: int = 20000, device: int = 0) -> hp.HFOptions:
+    o = hp.HFOptions()
+    o.precision, o.poisson = precision, poisson
+    o.poisson_rtol, o.poisson_atol, o.poisson_maxit, o.device = rtol, atol, maxit, device
+    return o
+
+
+class Case:
+    """One HigFlow case resident on the GPU."""
+
+    def __init__(self, prog: hp.Program, opts: Optional[hp.HFOptions] = None):
+        self.prog = prog
+        self._cprog = prog.to_c()
+        self._opts = opts or options()
+        h = C.c_void_p()
+        _check(lib().hf_case_create(C.byref(self._cprog), C.byref(self._opts), C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().hf_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set(self, fid: int, comp: int, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(lib().hf_case_set_field(self.h, fid, comp, v.ctypes.data_as(C.POINTER(C.c_double)), v.size))
+
+    def get(self, fid: int, comp: int = 0) -> np.ndarray:
+        out = np.empty(self.prog.field_size(fid, comp), dtype=np.float64)
+        _check(lib().hf_case_get_field(self.h, fid, comp, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
+    def step(self, n: int = 1) -> None:
+        _check(lib().hf_case_step(self.h, n))
+
+    def synchronize(self) -> None:
+        _check(lib().hf_case_synchronize(self.h))
+
+    def stats(self) -> hp.HFStats:
+        s = hp.HFStats()
+        _check(lib().hf_case_stats(self.h, C.byref(s)))
+        return s
+
+
+def device_bytes(prog: hp.Program, opts: Optional[hp.HFOptions] = None) -> int:
+    b = C.c_int64()
+    cp = prog.to_c()
+    o = opts or options()
+    _check(lib().hf_case_device_bytes(C.byref(cp), C.byref(o), C.byref(b)))
+    return b.value

@@ -1,0 +1,142 @@
+"""GPU parity of the B200 step engine against the oracle and the reference.
+
+Every test goes through the C ABI (libhigflow_b200.so via higflow_b200.engine).
+Tolerances: relative L2 1e-10 on velocity, pressure and kernel tensor after the
+fixture's N steps (the plain-FP64 parity bar); the velocity stage is compared
+bit for bit (same FP64 operation sequence, no FMA contraction).
+"""
+import numpy as np
+import pytest
+
+from higflow_b200 import engine
+from higflow_b200 import program as hp
+from oracle import restate
+from tests.helpers import compare, field_keys, golden_names, load_golden, load_init
+
+pytestmark = pytest.mark.gpu
+
+NAMES = golden_names()
+TOL = 1e-10
+
+
+def _opts(**kw):
+    kw.setdefault("rtol", 1e-14)
+    kw.setdefault("atol", 1e-300)
+    return engine.options(**kw)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_engine_matches_reference_after_n_steps(name):
+    prog, data = load_golden(name)
+    case = engine.Case(prog, _opts())
+    load_init(case, prog, data)
+    case.step(int(data["steps"]))
+    keys = [k for k, _, _ in field_keys(prog) if k != "dp" and not k.startswith("S")]
+    got = {k: case.get(fid, comp) for k, fid, comp in field_keys(prog)}
+    err = compare(got, {k: data["ref_" + k] for k in keys}, keys)
+    assert max(err.values()) < TOL, err
+    case.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_engine_matches_restatement(name):
+    prog, data = load_golden(name)
+    case = engine.Case(prog, _opts())
+    st = restate.State(prog)
+    load_init(case, prog, data)
+    load_init(st, prog, data)
+    n = int(data["steps"])
+    case.step(n)
+    st.step(n, rtol=1e-14)
+    keys = [k for k, _, _ in field_keys(prog) if k != "dp"]
+    got = {k: case.get(fid, comp) for k, fid, comp in field_keys(prog)}
+    want = {k: st.get(fid, comp) for k, fid, comp in field_keys(prog)}
+    err = compare(got, want, keys)
+    assert max(err.values()) < TOL, err
+    case.close()
+
+
+@pytest.mark.parametrize("name", ["cav2d_cubista", "cav2d_quick", "cav2d_central", "cav3d_cubista", "chan2d_cubista"])
+def test_velocity_stage_bit_exact(name):
+    """One step: u* (the explicit velocity stage) is bit-identical to the
+    oracle's, because both evaluate the same recorded rows in the reference's
+    order with the same IEEE operations."""
+    prog, data = load_golden(name)
+    case = engine.Case(prog, _opts())
+    st = restate.State(prog)
+    load_init(case, prog, data)
+    load_init(st, prog, data)
+    case.step(1)
+    st.velocity()
+    for d in range(prog.dim):
+        a = case.get(hp.FIELD_USTAR, d)
+        b = st.get(hp.FIELD_USTAR, d)
+        assert np.array_equal(a, b), (d, np.abs(a - b).max())
+    case.close()
+
+
+def test_bicgstab_path_matches_cg():
+    prog, data = load_golden("cav2d_cubista")
+    out = []
+    for solver in (hp.POISSON_CG, hp.POISSON_BICGSTAB):
+        case = engine.Case(prog, _opts(poisson=solver))
+        load_init(case, prog, data)
+        case.step(3)
+        out.append(case.get(hp.FIELD_P))
+        case.close()
+    assert np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[0]) < 1e-10
+
+
+def test_invalid_program_rejected_on_host():
+    prog, _ = load_golden("cav2d_cubista")
+    bad = hp.Program.load(__import__("os").path.join(__import__("tests.helpers", fromlist=["GOLDEN"]).GOLDEN,
+                                                       "cav2d_cubista.prog.npz"))
+    bad.vel_slots[0] = bad.vel_slots[0].copy()
+    bad.vel_slots[0][hp.V_PL, 0] = prog.ncell + 5   # direct index past the pressure field
+    with pytest.raises(engine.EngineError) as e:
+        engine.Case(bad)
+    assert e.value.code == -1
+
+
+def test_nan_is_reported():
+    prog, data = load_golden("cav2d_cubista")
+    case = engine.Case(prog, _opts())
+    load_init(case, prog, data)
+    u = data["init_u0"].copy()
+    u[3] = np.nan
+    case.set(hp.FIELD_U, 0, u)
+    with pytest.raises(engine.EngineError) as e:
+        case.step(1)
+    assert e.value.code == -4
+    case.close()
+
+
+def test_solver_engine_known_answer():
+    """higtree/atf-tests/test-solver-2d.c:9-49 through the solver-vtable engine:
+    the 3x3 system solves to x = (1, 4, -2)."""
+    import ctypes as C
+    L = engine.lib()
+    L.hf_slv_create.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.hf_slv_set_Ai.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.hf_slv_set_bi.argtypes = [C.c_void_p, C.c_int32, C.c_double]
+    L.hf_slv_assemble_matrix.argtypes = [C.c_void_p]
+    L.hf_slv_set_tolerances.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32]
+    L.hf_slv_solve.argtypes = [C.c_void_p]
+    L.hf_slv_get_x.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.hf_slv_destroy.argtypes = [C.c_void_p]
+    L.hf_slv_destroy.restype = None
+    m = [[-1.0, 3.0, 5.0], [3.0, -5.0, 7.0], [-1.0, 4.0, -10.0]]
+    b = [1.0, -31.0, 35.0]
+    s = C.c_void_p()
+    assert L.hf_slv_create(0, 3, C.byref(s)) == 0
+    j = (C.c_int32 * 3)(0, 1, 2)
+    for i in range(3):
+        assert L.hf_slv_set_Ai(s, i, 3, j, (C.c_double * 3)(*m[i])) == 0
+        assert L.hf_slv_set_bi(s, i, b[i]) == 0
+    assert L.hf_slv_assemble_matrix(s) == 0
+    assert L.hf_slv_set_tolerances(s, 1e-8, 1e-8, 1000) == 0
+    assert L.hf_slv_solve(s) == 0
+    x = (C.c_double * 3)()
+    assert L.hf_slv_get_x(s, x) == 0
+    assert abs(x[0] - 1.0) < 1e-12 and abs(x[1] - 4.0) < 1e-12 and abs(x[2] + 2.0) < 1e-12
+    L.hf_slv_destroy(s)

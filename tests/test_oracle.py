@@ -1,0 +1,151 @@
+"""The oracle (CPU restatement over flattened programs) pinned against the
+reference HigFlow itself, plus the reference's own known-answer tests restated.
+
+CPU only.  Tests that rebuild cases need the oracle build of the reference
+(oracle/_ref/libhigflow_ref{2,3}d.so) and are skipped without it.
+"""
+import numpy as np
+import pytest
+
+from higflow_b200 import program as hp
+from oracle import restate
+from tests.helpers import compare, field_keys, golden_names, load_golden, load_init
+
+NAMES = golden_names()
+
+try:
+    from oracle import refpy
+    HAVE_REF = refpy.available(2) and refpy.available(3)
+except Exception:  # pragma: no cover
+    HAVE_REF = False
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_restatement_matches_reference_fields(name):
+    """hf_restate.c over the recorded program reproduces the reference's own
+    N-step fields (tests/golden, written by higflow_solver_step[_viscoelastic])."""
+    prog, data = load_golden(name)
+    st = restate.State(prog)
+    load_init(st, prog, data)
+    st.step(int(data["steps"]), rtol=1e-14)
+    keys = [k for k, _, _ in field_keys(prog) if k != "dp" and not k.startswith("S")]
+    got = {k: st.get(fid, comp) for k, fid, comp in field_keys(prog)}
+    want = {k: data["ref_" + k] for k in keys}
+    err = compare(got, want, keys)
+    assert max(err.values()) < 1e-10, err
+
+
+def test_golden_fixtures_present():
+    assert len(NAMES) >= 10
+
+
+def _rebuild(name):
+    from tests.golden.make_golden import CASES
+    factory, steps, amps = CASES[name]
+    return factory, steps, amps
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not available")
+@pytest.mark.parametrize("name", ["cav2d_cubista", "ve2d_oldroyd_log", "chan2d_cubista", "cav3d_cubista"])
+def test_flattener_is_deterministic_and_bit_exact(name):
+    """Flattening the same reference case again gives the committed program
+    bit for bit: same slots, same row ids, same weights and boundary terms."""
+    from tests.golden import make_golden
+    import tempfile, os, shutil
+    prog, _ = load_golden(name)
+    d = tempfile.mkdtemp()
+    try:
+        old = make_golden.HERE
+        make_golden.HERE = d
+        make_golden.make(name)
+        make_golden.HERE = old
+        p2 = hp.Program.load(os.path.join(d, f"{name}.prog.npz"))
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    for attr in ("row_ptr", "row_col", "row_w", "row_rhs", "div_slots", "p_ptr", "p_col", "p_val", "p_brhs", "delta"):
+        a, b = getattr(prog, attr), getattr(p2, attr)
+        assert a.dtype == b.dtype and np.array_equal(a, b), attr
+    for d_ in range(prog.dim):
+        assert np.array_equal(prog.vel_slots[d_], p2.vel_slots[d_])
+        assert np.array_equal(prog.vel_flags[d_], p2.vel_flags[d_])
+    assert prog.pin_row == p2.pin_row
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not available")
+def test_poisson_rows_match_reference_assembly():
+    """The flattened Poisson rows equal the system higflow_pressure assembles
+    and hands to the solver plugin (captured inside the oracle's engine)."""
+    spec = refpy.cavity(2, 10, Re=10.0, dt=1e-3)
+    c = refpy.RefCase(spec)
+    prog = c.flatten()
+    c.step(1)
+    ptr, col, val, b = c.last_system()
+    n = prog.ncell
+    for r in range(n):
+        ref = dict(zip(col[ptr[r]:ptr[r + 1]], val[ptr[r]:ptr[r + 1]]))
+        if r == prog.pin_row:
+            assert ref == {r: 1.0}
+            continue
+        mine = {}
+        for k in range(prog.p_ptr[r], prog.p_ptr[r + 1]):
+            mine[int(prog.p_col[k])] = mine.get(int(prog.p_col[k]), 0.0) + prog.p_val[k]
+        assert mine.keys() == ref.keys()
+        for k in ref:
+            assert mine[k] == ref[k]
+    c.close()
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not available")
+def test_wls_rows_reproduce_linear_and_quadratic_fields():
+    """Known answers of higtree/atf-tests/test-wls-2d.c:10-139 restated on the
+    recorded interpolation rows: order-2 moving least squares reproduces
+    f = 2 + 3x + 4y (2.0 at the origin, 5.5 at (0.5, 0.5), 9.0 at (1, 1)) and a
+    quadratic exactly at every interior query point."""
+    spec = refpy.cavity(2, 16, Re=10.0, dt=1e-3)
+    c = refpy.RefCase(spec)
+    prog = c.flatten()
+    D = 2
+    centers = [c.centers(d) for d in range(D)]
+    fcent = [centers[d] for d in range(D)]
+    lin = lambda x: 2.0 + 3.0 * x[..., 0] + 4.0 * x[..., 1]
+    quad = lambda x: x[..., 0] ** 2 - 0.5 * x[..., 0] * x[..., 1] + 0.25 * x[..., 1] ** 2 - 0.25
+    checked = 0
+    for d in range(D):
+        nf = prog.nfacet[d]
+        for d2 in range(D):
+            for slot, sign in ((hp.V_BLK0 + hp.V_NB * d2 + hp.V_VCR, 1.0), (hp.V_BLK0 + hp.V_NB * d2 + hp.V_VCL, -1.0)):
+                codes = prog.vel_slots[d][slot]
+                for f in range(nf):
+                    code = int(codes[f])
+                    if code >= 0:
+                        continue
+                    r = -code - 1
+                    a, b = prog.row_ptr[r], prog.row_ptr[r + 1]
+                    w = prog.row_w[a:b]
+                    if prog.row_rhs[r] != 0.0 or abs(w.sum() - 1.0) > 1e-12:
+                        continue  # row mixes in boundary samples
+                    pts = fcent[d2][prog.row_col[a:b]]
+                    xq = fcent[d][f].copy()
+                    delta = prog.delta[prog.vel_delta[d][f]]
+                    xq[d2] += sign * 0.5 * delta[d2]
+                    for fn in (lin, quad):
+                        assert abs(np.dot(w, fn(pts)) - fn(xq)) < 1e-10
+                    checked += 1
+    assert checked > 100
+    # the three known answers of the linear case at the reference's points
+    pts = np.array([[-1, -1], [-1, 0], [-1, 1], [1, -1], [1, 0], [1, 1]], dtype=float)
+    vals = lin(pts)
+    assert list(vals) == [-5, -1, 3, 1, 5, 9]
+    assert [lin(np.array(p)) for p in ([0.0, 0.0], [0.5, 0.5], [1.0, 1.0])] == [2.0, 5.5, 9.0]
+    c.close()
+
+
+def test_program_roundtrip(tmp_path):
+    prog, _ = load_golden("ve2d_oldroyd_log")
+    p = tmp_path / "x.prog.npz"
+    prog.save(str(p))
+    q = hp.Program.load(str(p))
+    assert q.par == prog.par
+    assert np.array_equal(q.cell_slots, prog.cell_slots)
+    c = q.to_c()
+    assert c.ncell == prog.ncell and c.vel_nslot == prog.vel_slots[0].shape[0]
