@@ -613,11 +613,21 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
         int64_t z = 0;
         vec_push(&F.rows.ptr, &z);
     }
+    /* one template per recorded row, base 0 */
     P->nrows = (int64_t)F.rows.rhs.n;
+    P->ntmpl = P->nrows;
     P->nnz = (int64_t)F.rows.col.n;
-    P->row_ptr = F.rows.ptr.p;
-    P->row_col = F.rows.col.p;
-    P->row_w = F.rows.w.p;
+    {
+        int32_t *tm = malloc(sizeof(int32_t) * (size_t)(P->nrows ? P->nrows : 1));
+        int32_t *bs = calloc((size_t)(P->nrows ? P->nrows : 1), sizeof(int32_t));
+        if (!tm || !bs) { free(tm); free(bs); rc = HF_ERR_INVALID; goto fail; }
+        for (int64_t r = 0; r < P->nrows; r++) tm[r] = (int32_t)r;
+        P->row_tmpl = tm;
+        P->row_base = bs;
+    }
+    P->tmpl_ptr = F.rows.ptr.p;
+    P->tmpl_col = F.rows.col.p;
+    P->tmpl_w = F.rows.w.p;
     P->row_rhs = F.rows.rhs.p;
     F.rows.ptr.p = F.rows.col.p = F.rows.w.p = F.rows.rhs.p = NULL;
     P->ndelta = (int32_t)F.deltas.n;
@@ -656,7 +666,8 @@ void hf_program_free(hf_program *P)
 {
     if (!P) return;
     free((void *)P->delta);
-    free((void *)P->row_ptr); free((void *)P->row_col); free((void *)P->row_w); free((void *)P->row_rhs);
+    free((void *)P->row_tmpl); free((void *)P->row_base); free((void *)P->row_rhs);
+    free((void *)P->tmpl_ptr); free((void *)P->tmpl_col); free((void *)P->tmpl_w);
     for (int d = 0; d < 3; d++) {
         free((void *)P->vel_slots[d]); free((void *)P->vel_flags[d]); free((void *)P->vel_delta[d]);
     }

@@ -16,24 +16,29 @@ namespace hf {
 // General stencil rows, in FP64 or FP32 storage.
 template <typename W>
 struct Rows {
-    const int64_t *ptr;
+    const int32_t *tmpl;    // per row: template
+    const int32_t *base;    // per row: offset added to the template's columns
+    const W *rhs;           // per row: boundary term
+    const int64_t *tptr;    // per template: CSR pointer
     const int32_t *col;
     const W *w;
-    const W *rhs;
 };
 
 // Value of one recorded query (dp_interpolate_from_stencil, pdomain.c:1026-1053):
-// code >= 0 is a centre hit, otherwise -rhs + sum_k w_k * f[col_k] in row order.
+// code >= 0 is a centre hit, otherwise -rhs + sum_k w_k * f[base + col_k] in
+// template order.
 template <typename W, typename F>
 __device__ __forceinline__ W query(const Rows<W> &R, int32_t code, const F *__restrict__ f)
 {
     if (code >= 0) return (W)__ldg(f + code);
     const int64_t r = -(int64_t)code - 1;
+    const int32_t t = __ldg(R.tmpl + r);
+    const F *__restrict__ fb = f + __ldg(R.base + r);
     W res = (W)0;
     res += -__ldg(R.rhs + r);
-    const int64_t e = __ldg(R.ptr + r + 1);
-    for (int64_t k = __ldg(R.ptr + r); k < e; k++)
-        res += (W)__ldg(f + __ldg(R.col + k)) * __ldg(R.w + k);
+    const int64_t e = __ldg(R.tptr + t + 1);
+    for (int64_t k = __ldg(R.tptr + t); k < e; k++)
+        res += (W)__ldg(fb + __ldg(R.col + k)) * __ldg(R.w + k);
     return res;
 }
 

@@ -907,7 +907,36 @@ struct hf_case {
     hf_stats stats;
     double bytes = 0;
     int nfacet_total = 0;
+    // optional per-phase timing with CUDA events on the engine stream
+    bool profile = false;
+    cudaEvent_t ev[2 * HF_NPHASE] = {};
+    double phase_ms[HF_NPHASE] = {};
+    int64_t phase_launches[HF_NPHASE] = {};
 };
+
+namespace {
+
+struct PhaseTimer {
+    hf_case *C;
+    int phase;
+    int64_t launches0;
+    PhaseTimer(hf_case *c, int p, int64_t l) : C(c), phase(p), launches0(l)
+    {
+        if (C->profile) cudaEventRecord(C->ev[2 * p], C->stream);
+    }
+    void stop(int64_t launches)
+    {
+        if (!C->profile) return;
+        cudaEventRecord(C->ev[2 * phase + 1], C->stream);
+        cudaEventSynchronize(C->ev[2 * phase + 1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, C->ev[2 * phase], C->ev[2 * phase + 1]);
+        C->phase_ms[phase] += ms;
+        C->phase_launches[phase] += launches - launches0;
+    }
+};
+
+}  // namespace
 
 namespace {
 
@@ -977,7 +1006,12 @@ int check_program(const hf_program *pg)
         return c >= 0 ? (int64_t)c < nfield : (-(int64_t)c - 1) < pg->nrows;
     };
     for (int64_t k = 0; k < pg->nnz; k++)
-        if (pg->row_col[k] < 0) return fail(HF_ERR_INVALID, "negative row column");
+        if (pg->tmpl_col[k] < 0) return fail(HF_ERR_INVALID, "negative template column");
+    for (int64_t r = 0; r < pg->nrows; r++)
+        if (pg->row_tmpl[r] < 0 || pg->row_tmpl[r] >= pg->ntmpl || pg->row_base[r] < 0)
+            return fail(HF_ERR_INVALID, "row template/base out of range");
+    for (int64_t t = 0; t < pg->ntmpl; t++)
+        if (pg->tmpl_ptr[t + 1] < pg->tmpl_ptr[t] || pg->tmpl_ptr[t + 1] > pg->nnz) return fail(HF_ERR_INVALID, "template pointer");
     for (int d = 0; d < D; d++) {
         const int64_t nf = pg->nfacet[d];
         for (int s = 0; s < pg->vel_nslot; s++) {
@@ -1066,11 +1100,12 @@ int check_rows(const hf_program *pg)
             for (int64_t c = 0; c < pg->ncell; c++) note(pg->cell_slots[(size_t)s * pg->ncell + c], nfield);
         }
     }
-    for (int64_t r = 0; r < pg->nrows; r++) {
-        if (pg->row_ptr[r + 1] < pg->row_ptr[r] || pg->row_ptr[r + 1] > pg->nnz) return fail(HF_ERR_INVALID, "row pointer");
-        for (int64_t k = pg->row_ptr[r]; k < pg->row_ptr[r + 1]; k++)
-            if ((int64_t)pg->row_col[k] >= limit[r]) return fail(HF_ERR_INVALID, "row column out of its field");
-    }
+    // largest column of each template, then base + max column < field size for every row
+    std::vector<int64_t> tmax((size_t)pg->ntmpl, -1);
+    for (int64_t t = 0; t < pg->ntmpl; t++)
+        for (int64_t k = pg->tmpl_ptr[t]; k < pg->tmpl_ptr[t + 1]; k++) tmax[t] = std::max(tmax[t], (int64_t)pg->tmpl_col[k]);
+    for (int64_t r = 0; r < pg->nrows; r++)
+        if ((int64_t)pg->row_base[r] + tmax[pg->row_tmpl[r]] >= limit[r]) return fail(HF_ERR_INVALID, "row column out of its field");
     return HF_OK;
 }
 
@@ -1079,31 +1114,43 @@ int launch_step(hf_case *C)
 {
     cudaStream_t st = C->stream;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
-    long launches = 0;
+    int64_t launches = 0;
     if (ve) {
+        PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
         k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
         launches++;
         for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
+        t.stop(launches);
     }
-    if (ve) k_velocity<D, true><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
-    else k_velocity<D, false><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
-    launches++;
+    {
+        PhaseTimer t(C, HF_PHASE_VELOCITY, launches);
+        if (ve) k_velocity<D, true><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
+        else k_velocity<D, false><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
+        launches++;
+        t.stop(launches);
+    }
     HF_CK(cudaGetLastError());
     const double rtol = C->opt.poisson_rtol, atol = C->opt.poisson_atol;
     const int n = C->P.ncell;
     int rc = HF_OK;
     if (C->use_cg) {
-        k_cg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
-        launches++;
+        {
+            PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
+            k_cg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
+            launches++;
+            t.stop(launches);
+        }
         double *pa = C->cg.pa, *pb = C->cg.pb;
         int chunk = 8;
         for (;;) {
+            PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
             for (int k = 0; k < chunk; k++) {
                 k_cg_dir_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pa, pb);
                 k_cg_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pb);
                 std::swap(pa, pb);
                 launches += 2;
             }
+            t.stop(launches);
             HF_CK(cudaMemcpyAsync(C->h_scal, C->cg.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
             HF_CK(cudaStreamSynchronize(st));
             if (C->h_scal->done) break;
@@ -1116,10 +1163,15 @@ int launch_step(hf_case *C)
         int restarts = 0;
         int from_step = 1;
         for (;;) {
-            k_bi_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->bi, rtol, atol, from_step);
-            launches++;
+            {
+                PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
+                k_bi_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->bi, rtol, atol, from_step);
+                launches++;
+                t.stop(launches);
+            }
             int chunk = 4;
             for (;;) {
+                PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
                 for (int k = 0; k < chunk; k++) {
                     k_bi_p<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
                     k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.ph, C->bi.v, 0);
@@ -1128,6 +1180,7 @@ int launch_step(hf_case *C)
                     k_bi_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
                     launches += 5;
                 }
+                t.stop(launches);
                 HF_CK(cudaMemcpyAsync(C->h_scal, C->bi.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
                 HF_CK(cudaStreamSynchronize(st));
                 if (C->h_scal->done) break;
@@ -1138,8 +1191,12 @@ int launch_step(hf_case *C)
         }
         if (C->h_scal->status) rc = fail(C->h_scal->status == 1 ? HF_ERR_NOT_CONVERGED : C->h_scal->status, "Poisson BiCGStab failed");
     }
-    k_final<D><<<blocks(C->nfacet_total + n), kBlock, 0, st>>>(C->P, C->F);
-    launches++;
+    {
+        PhaseTimer t(C, HF_PHASE_FINAL, launches);
+        k_final<D><<<blocks(C->nfacet_total + n), kBlock, 0, st>>>(C->P, C->F);
+        launches++;
+        t.stop(launches);
+    }
     HF_CK(cudaGetLastError());
     C->stats.last_iters = C->h_scal->iters;
     C->stats.total_iters += C->h_scal->iters;
@@ -1164,7 +1221,7 @@ extern "C" int hf_case_device_bytes(const hf_program *pg, const hf_options *opt,
     int64_t nfac = 0;
     for (int d = 0; d < D; d++) nfac += pg->nfacet[d];
     int64_t b = 0;
-    b += pg->nnz * 12 + pg->nrows * 16 + 8;
+    b += pg->nnz * 12 + pg->ntmpl * 8 + pg->nrows * 16 + 8;
     b += nfac * ((int64_t)pg->vel_nslot * 4 + 4 + 2);
     b += (int64_t)pg->ncell * (2 * D * 4 + 2);
     b += pg->pnnz * 12 + (int64_t)pg->ncell * 4 * 8;
@@ -1226,10 +1283,12 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     auto &own = C->owned;
 #define UP(dst, src, n) do { if ((rc = upload(own, dst, src, (size_t)(n), B))) return cleanup(rc); } while (0)
     UP((double **)&P.delta, pg->delta, (size_t)pg->ndelta * D);
-    UP((int64_t **)&P.rows.ptr, pg->row_ptr, pg->nrows + 1);
-    UP((int32_t **)&P.rows.col, pg->row_col, pg->nnz);
-    UP((double **)&P.rows.w, pg->row_w, pg->nnz);
+    UP((int32_t **)&P.rows.tmpl, pg->row_tmpl, pg->nrows);
+    UP((int32_t **)&P.rows.base, pg->row_base, pg->nrows);
     UP((double **)&P.rows.rhs, pg->row_rhs, pg->nrows);
+    UP((int64_t **)&P.rows.tptr, pg->tmpl_ptr, pg->ntmpl + 1);
+    UP((int32_t **)&P.rows.col, pg->tmpl_col, pg->nnz);
+    UP((double **)&P.rows.w, pg->tmpl_w, pg->nnz);
     for (int d = 0; d < D; d++) {
         UP((int32_t **)&P.vslots[d], pg->vel_slots[d], (size_t)pg->vel_nslot * pg->nfacet[d]);
         UP((uint32_t **)&P.vflags[d], pg->vel_flags[d], pg->nfacet[d]);
@@ -1393,10 +1452,39 @@ extern "C" int hf_case_stats(hf_case *C, hf_stats *out)
     return HF_OK;
 }
 
+extern "C" int hf_case_stream(hf_case *C, void **stream)
+{
+    if (!C || !stream) return fail(HF_ERR_INVALID, "null argument");
+    *stream = (void *)C->stream;
+    return HF_OK;
+}
+
+extern "C" int hf_case_profile(hf_case *C, int32_t enable)
+{
+    if (!C) return fail(HF_ERR_INVALID, "null case");
+    if (enable && !C->ev[0])
+        for (int k = 0; k < 2 * HF_NPHASE; k++) HF_CK(cudaEventCreate(&C->ev[k]));
+    C->profile = enable != 0;
+    for (int k = 0; k < HF_NPHASE; k++) { C->phase_ms[k] = 0.0; C->phase_launches[k] = 0; }
+    return HF_OK;
+}
+
+extern "C" int hf_case_phase_times(hf_case *C, double *ms, int64_t *launches, int32_t n)
+{
+    if (!C || n < 0) return fail(HF_ERR_INVALID, "bad argument");
+    for (int k = 0; k < n && k < HF_NPHASE; k++) {
+        if (ms) ms[k] = C->phase_ms[k];
+        if (launches) launches[k] = C->phase_launches[k];
+    }
+    return HF_OK;
+}
+
 extern "C" void hf_case_destroy(hf_case *C)
 {
     if (!C) return;
     if (C->stream) cudaStreamSynchronize(C->stream);
+    for (int k = 0; k < 2 * HF_NPHASE; k++)
+        if (C->ev[k]) cudaEventDestroy(C->ev[k]);
     for (void *p : C->owned) cudaFree(p);
     if (C->h_scal) cudaFreeHost(C->h_scal);
     if (C->stream) cudaStreamDestroy(C->stream);

@@ -45,6 +45,9 @@ def lib() -> C.CDLL:
         L.hf_case_destroy.argtypes = [V]
         L.hf_case_destroy.restype = None
         L.hf_case_device_bytes.argtypes = [P(hp.HFProgram), P(hp.HFOptions), P(C.c_int64)]
+        L.hf_case_stream.argtypes = [V, P(C.c_void_p)]
+        L.hf_case_profile.argtypes = [V, C.c_int32]
+        L.hf_case_phase_times.argtypes = [V, P(C.c_double), P(C.c_int64), C.c_int32]
         _lib = L
     return _lib
 
@@ -103,6 +106,26 @@ class Case:
         s = hp.HFStats()
         _check(lib().hf_case_stats(self.h, C.byref(s)))
         return s
+
+    def stream(self) -> int:
+        """Handle of the cudaStream_t all of this case's kernels run on."""
+        p = C.c_void_p()
+        _check(lib().hf_case_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        """Turn per-phase CUDA-event timing on/off (resets the counters)."""
+        _check(lib().hf_case_profile(self.h, 1 if enable else 0))
+
+    PHASES = ("ve_cell", "velocity", "poisson_init", "poisson_iter", "final")
+
+    def phase_times(self):
+        """{phase: (device ms, kernel launches)} accumulated since profile()."""
+        n = len(self.PHASES)
+        ms = (C.c_double * n)()
+        la = (C.c_int64 * n)()
+        _check(lib().hf_case_phase_times(self.h, ms, la, n))
+        return {p: (ms[i], la[i]) for i, p in enumerate(self.PHASES)}
 
 
 def device_bytes(prog: hp.Program, opts: Optional[hp.HFOptions] = None) -> int:

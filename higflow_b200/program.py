@@ -69,9 +69,10 @@ class HFProgram(C.Structure):
         ("nfacet", C.c_int32 * 3),
         ("ndelta", C.c_int32),
         ("delta", _P(C.c_double)),
-        ("nrows", C.c_int64), ("nnz", C.c_int64),
-        ("row_ptr", _P(C.c_int64)), ("row_col", _P(C.c_int32)),
-        ("row_w", _P(C.c_double)), ("row_rhs", _P(C.c_double)),
+        ("nrows", C.c_int64),
+        ("row_tmpl", _P(C.c_int32)), ("row_base", _P(C.c_int32)), ("row_rhs", _P(C.c_double)),
+        ("ntmpl", C.c_int64), ("nnz", C.c_int64),
+        ("tmpl_ptr", _P(C.c_int64)), ("tmpl_col", _P(C.c_int32)), ("tmpl_w", _P(C.c_double)),
         ("vel_nslot", C.c_int32),
         ("vel_slots", _P(C.c_int32) * 3),
         ("vel_flags", _P(C.c_uint32) * 3),
@@ -125,10 +126,12 @@ class Program:
     ncell: int
     nfacet: list
     delta: np.ndarray                     # (ndelta, dim) float64
-    row_ptr: np.ndarray                   # int64
-    row_col: np.ndarray                   # int32
-    row_w: np.ndarray                     # float64
-    row_rhs: np.ndarray                   # float64
+    row_tmpl: np.ndarray                  # int32, per general row
+    row_base: np.ndarray                  # int32, per general row
+    row_rhs: np.ndarray                   # float64, per general row
+    tmpl_ptr: np.ndarray                  # int64, ntmpl + 1
+    tmpl_col: np.ndarray                  # int32
+    tmpl_w: np.ndarray                    # float64
     vel_slots: list                       # per dim: (nslot, nfacet) int32
     vel_flags: list                       # per dim: (nfacet,) uint32
     vel_delta: list                       # per dim: (nfacet,) uint16
@@ -172,10 +175,12 @@ class Program:
         return cls(
             par=par, ncell=ncell, nfacet=nf,
             delta=_np_from(p.delta, p.ndelta * dim, np.float64).reshape(p.ndelta, dim),
-            row_ptr=_np_from(p.row_ptr, p.nrows + 1, np.int64),
-            row_col=_np_from(p.row_col, p.nnz, np.int32),
-            row_w=_np_from(p.row_w, p.nnz, np.float64),
+            row_tmpl=_np_from(p.row_tmpl, p.nrows, np.int32),
+            row_base=_np_from(p.row_base, p.nrows, np.int32),
             row_rhs=_np_from(p.row_rhs, p.nrows, np.float64),
+            tmpl_ptr=_np_from(p.tmpl_ptr, p.ntmpl + 1, np.int64),
+            tmpl_col=_np_from(p.tmpl_col, p.nnz, np.int32),
+            tmpl_w=_np_from(p.tmpl_w, p.nnz, np.float64),
             vel_slots=vel_slots, vel_flags=vel_flags, vel_delta=vel_delta,
             div_slots=_np_from(p.div_slots, 2 * dim * ncell, np.int32).reshape(2 * dim, ncell),
             cell_delta=_np_from(p.cell_delta, ncell, np.uint16),
@@ -207,11 +212,14 @@ class Program:
         p.ndelta = self.delta.shape[0]
         p.delta = a(self.delta.ravel(), np.float64, C.c_double)
         p.nrows = self.row_rhs.size
-        p.nnz = self.row_col.size
-        p.row_ptr = a(self.row_ptr, np.int64, C.c_int64)
-        p.row_col = a(self.row_col, np.int32, C.c_int32)
-        p.row_w = a(self.row_w, np.float64, C.c_double)
+        p.row_tmpl = a(self.row_tmpl, np.int32, C.c_int32)
+        p.row_base = a(self.row_base, np.int32, C.c_int32)
         p.row_rhs = a(self.row_rhs, np.float64, C.c_double)
+        p.ntmpl = self.tmpl_ptr.size - 1
+        p.nnz = self.tmpl_col.size
+        p.tmpl_ptr = a(self.tmpl_ptr, np.int64, C.c_int64)
+        p.tmpl_col = a(self.tmpl_col, np.int32, C.c_int32)
+        p.tmpl_w = a(self.tmpl_w, np.float64, C.c_double)
         p.vel_nslot = self.vel_slots[0].shape[0]
         for d in range(self.dim):
             p.vel_slots[d] = a(self.vel_slots[d].ravel(), np.int32, C.c_int32)
@@ -240,8 +248,8 @@ class Program:
         arrs = dict(
             par_keys=np.array(_PARAM_NAMES), par_vals=np.array([float(self.par[n]) for n in _PARAM_NAMES]),
             ncell=np.int64(self.ncell), nfacet=np.array(self.nfacet, dtype=np.int64),
-            delta=self.delta, row_ptr=self.row_ptr, row_col=self.row_col, row_w=self.row_w,
-            row_rhs=self.row_rhs, div_slots=self.div_slots, cell_delta=self.cell_delta,
+            delta=self.delta, row_tmpl=self.row_tmpl, row_base=self.row_base, row_rhs=self.row_rhs,
+            tmpl_ptr=self.tmpl_ptr, tmpl_col=self.tmpl_col, tmpl_w=self.tmpl_w, div_slots=self.div_slots, cell_delta=self.cell_delta,
             p_ptr=self.p_ptr, p_col=self.p_col, p_val=self.p_val, p_brhs=self.p_brhs,
             pin=np.array([self.pin_row], dtype=np.int64), pin_value=np.float64(self.pin_value),
         )
@@ -266,8 +274,8 @@ class Program:
         dim = par["dim"]
         return cls(
             par=par, ncell=int(z["ncell"]), nfacet=[int(x) for x in z["nfacet"]],
-            delta=z["delta"], row_ptr=z["row_ptr"], row_col=z["row_col"], row_w=z["row_w"],
-            row_rhs=z["row_rhs"],
+            delta=z["delta"], row_tmpl=z["row_tmpl"], row_base=z["row_base"], row_rhs=z["row_rhs"],
+            tmpl_ptr=z["tmpl_ptr"], tmpl_col=z["tmpl_col"], tmpl_w=z["tmpl_w"],
             vel_slots=[z[f"vel_slots{d}"] for d in range(dim)],
             vel_flags=[z[f"vel_flags{d}"] for d in range(dim)],
             vel_delta=[z[f"vel_delta{d}"] for d in range(dim)],

@@ -80,8 +80,12 @@ enum {
 /*   code >= 0 : the query is a centre hit with weight 1 and no        */
 /*               boundary term; its value is field[code]               */
 /*   code <  0 : general query r = -code-1; its value is               */
-/*               -rhs[r] + sum_k w[k]*field[col[k]], k in row r,       */
-/*               accumulated in that order (pdomain.c:1026-1053)       */
+/*               -rhs[r] + sum_k w[k]*field[base[r] + col[k]] over the */
+/*               entries k of template tmpl[r], accumulated in that    */
+/*               order (pdomain.c:1026-1053).  A recorded program has  */
+/*               one template per row and base 0; rows that are        */
+/*               translates of each other on a uniform grid share one  */
+/*               template and differ only in base.                     */
 /* Which field a slot reads is fixed by its position (listed below).   */
 /* Slot arrays are slot-major: slots[s * nelem + e].                   */
 /* ------------------------------------------------------------------ */
@@ -183,13 +187,17 @@ typedef struct hf_program {
     int32_t ndelta;
     const double *delta;           /* ndelta * dim                             */
 
-    /* general stencil rows, deduplicated by content */
+    /* general stencil rows: template, base offset and boundary term per row */
     int64_t nrows;
+    const int32_t *row_tmpl;       /* nrows: template index                    */
+    const int32_t *row_base;       /* nrows: added to every template column    */
+    const double  *row_rhs;        /* nrows                                    */
+    /* stencil templates (CSR of ids and weights), deduplicated by content */
+    int64_t ntmpl;
     int64_t nnz;
-    const int64_t *row_ptr;        /* nrows + 1 */
-    const int32_t *row_col;        /* nnz       */
-    const double  *row_w;          /* nnz       */
-    const double  *row_rhs;        /* nrows     */
+    const int64_t *tmpl_ptr;       /* ntmpl + 1 */
+    const int32_t *tmpl_col;       /* nnz       */
+    const double  *tmpl_w;         /* nnz       */
 
     /* velocity stage per direction d < dim */
     int32_t vel_nslot;             /* HF_V_NSLOT_NEWT or HF_V_NSLOT_VE         */
@@ -251,6 +259,23 @@ int  hf_case_step(hf_case *c, int32_t nsteps);
 int  hf_case_stats(hf_case *c, hf_stats *out);
 int  hf_case_synchronize(hf_case *c);
 void hf_case_destroy(hf_case *c);
+
+/* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
+int  hf_case_stream(hf_case *c, void **stream);
+
+/* Per-phase device time: with profiling on, each phase of hf_case_step is
+ * bracketed by CUDA events on the case stream; times accumulate (ms) with the
+ * number of kernel launches per phase until the next hf_case_profile call. */
+enum {
+    HF_PHASE_VE_CELL = 0,       /* viscoelastic cell stage                 */
+    HF_PHASE_VELOCITY = 1,      /* intermediate velocity                   */
+    HF_PHASE_POISSON_INIT = 2,  /* divergence rhs + first residual         */
+    HF_PHASE_POISSON_ITER = 3,  /* Krylov iterations                       */
+    HF_PHASE_FINAL = 4,         /* final velocity and pressure             */
+    HF_NPHASE = 5
+};
+int  hf_case_profile(hf_case *c, int32_t enable);
+int  hf_case_phase_times(hf_case *c, double *ms, int64_t *launches, int32_t n);
 
 /* Device memory the engine would hold for a program (admission control). */
 int  hf_case_device_bytes(const hf_program *prog, const hf_options *opt, int64_t *bytes);

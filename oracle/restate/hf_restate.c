@@ -35,9 +35,11 @@ static double q(const hf_program *P, int32_t code, const double *f)
 {
     if (code >= 0) return f[code];
     int64_t r = -(int64_t)code - 1;
+    int64_t t = P->row_tmpl[r];
+    const double *fb = f + P->row_base[r];
     double res = 0.0;
     res += -P->row_rhs[r];
-    for (int64_t k = P->row_ptr[r]; k < P->row_ptr[r + 1]; k++) res += f[P->row_col[k]] * P->row_w[k];
+    for (int64_t k = P->tmpl_ptr[t]; k < P->tmpl_ptr[t + 1]; k++) res += fb[P->tmpl_col[k]] * P->tmpl_w[k];
     return res;
 }
 

@@ -62,7 +62,8 @@ def test_flattener_is_deterministic_and_bit_exact(name):
         p2 = hp.Program.load(os.path.join(d, f"{name}.prog.npz"))
     finally:
         shutil.rmtree(d, ignore_errors=True)
-    for attr in ("row_ptr", "row_col", "row_w", "row_rhs", "div_slots", "p_ptr", "p_col", "p_val", "p_brhs", "delta"):
+    for attr in ("row_tmpl", "row_base", "row_rhs", "tmpl_ptr", "tmpl_col", "tmpl_w", "div_slots", "p_ptr",
+                 "p_col", "p_val", "p_brhs", "delta"):
         a, b = getattr(prog, attr), getattr(p2, attr)
         assert a.dtype == b.dtype and np.array_equal(a, b), attr
     for d_ in range(prog.dim):
@@ -120,11 +121,12 @@ def test_wls_rows_reproduce_linear_and_quadratic_fields():
                     if code >= 0:
                         continue
                     r = -code - 1
-                    a, b = prog.row_ptr[r], prog.row_ptr[r + 1]
-                    w = prog.row_w[a:b]
+                    t = prog.row_tmpl[r]
+                    a, b = prog.tmpl_ptr[t], prog.tmpl_ptr[t + 1]
+                    w = prog.tmpl_w[a:b]
                     if prog.row_rhs[r] != 0.0 or abs(w.sum() - 1.0) > 1e-12:
                         continue  # row mixes in boundary samples
-                    pts = fcent[d2][prog.row_col[a:b]]
+                    pts = fcent[d2][prog.row_base[r] + prog.tmpl_col[a:b]]
                     xq = fcent[d][f].copy()
                     delta = prog.delta[prog.vel_delta[d][f]]
                     xq[d2] += sign * 0.5 * delta[d2]
