@@ -1,0 +1,244 @@
+// Smoothed-aggregation algebraic multigrid, used as the preconditioner of the
+// Poisson CG (one V-cycle per iteration).
+//
+// Host: the hierarchy is built once per program from the reduced Poisson
+// operator itself (no mesh geometry is needed, so AMR programs work too):
+// greedy aggregation on strong connections (|a_ij| >= theta sqrt(a_ii a_jj)),
+// a tentative piecewise-constant prolongator smoothed by one damped-Jacobi
+// step (P = (I - w D^-1 A) T, w = 4/3 over the Gershgorin bound of D^-1 A),
+// Galerkin coarse operators A_c = P^T A P, and a dense inverse of the coarsest
+// operator.
+//
+// Device: a V-cycle with one damped-Jacobi pre- and post-smoothing sweep per
+// level; restriction and prolongation are CSR products with R = P^T and P, the
+// coarsest solve is a dense matrix-vector product.  The symmetric V-cycle keeps
+// the preconditioned operator symmetric positive definite, as CG requires.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+namespace hf {
+
+struct HostCSR {
+    int n = 0, m = 0;  // rows, columns
+    std::vector<int> ptr, col;
+    std::vector<double> val;
+};
+
+inline HostCSR csr_transpose(const HostCSR &A)
+{
+    HostCSR T;
+    T.n = A.m;
+    T.m = A.n;
+    T.ptr.assign(T.n + 1, 0);
+    for (int k = 0; k < A.ptr[A.n]; k++) T.ptr[A.col[k] + 1]++;
+    for (int i = 0; i < T.n; i++) T.ptr[i + 1] += T.ptr[i];
+    T.col.resize(A.ptr[A.n]);
+    T.val.resize(A.ptr[A.n]);
+    std::vector<int> pos(T.ptr.begin(), T.ptr.end() - 1);
+    for (int i = 0; i < A.n; i++)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++) {
+            int p = pos[A.col[k]]++;
+            T.col[p] = i;
+            T.val[p] = A.val[k];
+        }
+    return T;
+}
+
+// C = A * B with a dense accumulator per row (columns kept in first-touch order)
+inline HostCSR csr_multiply(const HostCSR &A, const HostCSR &B)
+{
+    HostCSR C;
+    C.n = A.n;
+    C.m = B.m;
+    C.ptr.assign(C.n + 1, 0);
+    std::vector<double> acc(B.m, 0.0);
+    std::vector<int> mark(B.m, -1);
+    std::vector<int> cols;
+    for (int i = 0; i < A.n; i++) {
+        cols.clear();
+        for (int ka = A.ptr[i]; ka < A.ptr[i + 1]; ka++) {
+            const int j = A.col[ka];
+            const double a = A.val[ka];
+            for (int kb = B.ptr[j]; kb < B.ptr[j + 1]; kb++) {
+                const int c = B.col[kb];
+                if (mark[c] != i) {
+                    mark[c] = i;
+                    acc[c] = 0.0;
+                    cols.push_back(c);
+                }
+                acc[c] += a * B.val[kb];
+            }
+        }
+        std::sort(cols.begin(), cols.end());
+        for (int c : cols) {
+            C.col.push_back(c);
+            C.val.push_back(acc[c]);
+        }
+        C.ptr[i + 1] = (int)C.col.size();
+    }
+    return C;
+}
+
+// greedy aggregation on strong connections; returns the aggregate count
+inline int aggregate(const HostCSR &A, std::vector<int> &agg, double theta = 0.08)
+{
+    const int n = A.n;
+    std::vector<double> diag(n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++)
+            if (A.col[k] == i) diag[i] = A.val[k];
+    auto strong = [&](int i, int k) {
+        const int j = A.col[k];
+        return j != i && std::fabs(A.val[k]) >= theta * std::sqrt(std::fabs(diag[i] * diag[j]));
+    };
+    agg.assign(n, -1);
+    int na = 0;
+    // pass 1: a node with no aggregated strong neighbour seeds an aggregate with them
+    for (int i = 0; i < n; i++) {
+        if (agg[i] >= 0) continue;
+        bool free_nb = true, any = false;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++)
+            if (strong(i, k)) {
+                any = true;
+                if (agg[A.col[k]] >= 0) { free_nb = false; break; }
+            }
+        if (!any || !free_nb) continue;
+        agg[i] = na;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++)
+            if (strong(i, k)) agg[A.col[k]] = na;
+        na++;
+    }
+    // pass 2: join the aggregate of the strongest aggregated neighbour
+    std::vector<int> add(n, -1);
+    for (int i = 0; i < n; i++) {
+        if (agg[i] >= 0) continue;
+        double best = -1.0;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++)
+            if (strong(i, k) && agg[A.col[k]] >= 0 && std::fabs(A.val[k]) > best) {
+                best = std::fabs(A.val[k]);
+                add[i] = agg[A.col[k]];
+            }
+    }
+    for (int i = 0; i < n; i++)
+        if (agg[i] < 0 && add[i] >= 0) agg[i] = add[i];
+    // pass 3: leftovers become their own aggregates
+    for (int i = 0; i < n; i++)
+        if (agg[i] < 0) agg[i] = na++;
+    return na;
+}
+
+struct HostLevel {
+    HostCSR A, P, R;
+    std::vector<double> dinv;
+};
+
+// Build the hierarchy; the last level keeps A only (its dense inverse is made by
+// the caller).  Stops at <= max_coarse rows or when coarsening stalls.
+inline std::vector<HostLevel> build_hierarchy(HostCSR A, int max_coarse = 256, int max_levels = 20)
+{
+    std::vector<HostLevel> L;
+    for (int lev = 0; lev < max_levels; lev++) {
+        HostLevel h;
+        h.dinv.assign(A.n, 1.0);
+        double rho = 0.0;
+        for (int i = 0; i < A.n; i++) {
+            double d = 0.0, s = 0.0;
+            for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++) {
+                if (A.col[k] == i) d = A.val[k];
+                s += std::fabs(A.val[k]);
+            }
+            h.dinv[i] = d != 0.0 ? 1.0 / d : 1.0;
+            if (d != 0.0) rho = std::max(rho, s / std::fabs(d));
+        }
+        if (A.n <= max_coarse) {
+            h.A = std::move(A);
+            L.push_back(std::move(h));
+            break;
+        }
+        std::vector<int> agg;
+        const int na = aggregate(A, agg);
+        if (na >= A.n * 0.95) {  // coarsening stalled: stop here
+            h.A = std::move(A);
+            L.push_back(std::move(h));
+            break;
+        }
+        // tentative prolongator T and its damped-Jacobi smoothing
+        HostCSR T;
+        T.n = A.n;
+        T.m = na;
+        T.ptr.resize(A.n + 1);
+        T.col.resize(A.n);
+        T.val.assign(A.n, 1.0);
+        for (int i = 0; i <= A.n; i++) T.ptr[i] = i;
+        for (int i = 0; i < A.n; i++) T.col[i] = agg[i];
+        HostCSR AT = csr_multiply(A, T);
+        const double w = (4.0 / 3.0) / (rho > 0.0 ? rho : 2.0);
+        HostCSR P;
+        P.n = A.n;
+        P.m = na;
+        P.ptr.assign(A.n + 1, 0);
+        for (int i = 0; i < A.n; i++) {
+            // P_i = T_i - w dinv_i (A T)_i ; T_i has the single entry (agg[i], 1)
+            bool has_own = false;
+            for (int k = AT.ptr[i]; k < AT.ptr[i + 1]; k++) {
+                double v = -w * h.dinv[i] * AT.val[k];
+                if (AT.col[k] == agg[i]) { v += 1.0; has_own = true; }
+                if (v != 0.0) { P.col.push_back(AT.col[k]); P.val.push_back(v); }
+            }
+            if (!has_own) { P.col.push_back(agg[i]); P.val.push_back(1.0); }
+            P.ptr[i + 1] = (int)P.col.size();
+        }
+        HostCSR R = csr_transpose(P);
+        HostCSR AP = csr_multiply(A, P);
+        HostCSR Ac = csr_multiply(R, AP);
+        h.A = std::move(A);
+        h.P = std::move(P);
+        h.R = std::move(R);
+        L.push_back(std::move(h));
+        A = std::move(Ac);
+    }
+    return L;
+}
+
+// dense inverse by Gauss-Jordan with partial pivoting (row-major n x n)
+inline bool dense_inverse(const HostCSR &A, std::vector<double> &inv)
+{
+    const int n = A.n;
+    std::vector<double> a((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++) a[(size_t)i * n + A.col[k]] += A.val[k];
+    inv.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; c++) {
+        int p = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::fabs(a[(size_t)r * n + c]) > std::fabs(a[(size_t)p * n + c])) p = r;
+        if (a[(size_t)p * n + c] == 0.0) return false;
+        if (p != c)
+            for (int k = 0; k < n; k++) {
+                std::swap(a[(size_t)p * n + k], a[(size_t)c * n + k]);
+                std::swap(inv[(size_t)p * n + k], inv[(size_t)c * n + k]);
+            }
+        const double piv = 1.0 / a[(size_t)c * n + c];
+        for (int k = 0; k < n; k++) {
+            a[(size_t)c * n + k] *= piv;
+            inv[(size_t)c * n + k] *= piv;
+        }
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            const double f = a[(size_t)r * n + c];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; k++) {
+                a[(size_t)r * n + k] -= f * a[(size_t)c * n + k];
+                inv[(size_t)r * n + k] -= f * inv[(size_t)c * n + k];
+            }
+        }
+    }
+    return true;
+}
+
+}  // namespace hf

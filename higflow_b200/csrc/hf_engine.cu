@@ -40,6 +40,7 @@
 #include <string>
 #include <vector>
 
+#include "hf_amg.cuh"
 #include "hf_device.cuh"
 #include "higflow_b200.h"
 
@@ -79,8 +80,14 @@ struct DevProg {
     const int32_t *cslots;
     const uint32_t *cflags;
     int cns;
-    int pin;
+    int pin;               // single-instance path: instance 0's pin and parameters (par)
     double pin_value;
+    // per-instance parameters and element -> instance maps (batches)
+    int ninst;
+    const hf_params *ipar;
+    const int32_t *cinst;
+    const int32_t *finst[3];
+    const double *ipinv;
 };
 
 struct DevFields {
@@ -191,9 +198,10 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
     const double *fd = P.delta + (size_t)__ldg(P.vdelta[d] + f) * D;
     const uint32_t fl = __ldg(P.vflags[d] + f);
     const hf::Rows<double> &R = P.rows;
+    const hf_params &par = P.ipar[__ldg(P.finst[d] + f)];
     const double a = 1.7500, b = 0.3750, c = 0.7500, dd = 0.1250, ee = 0.2500;
-    int convec = P.par.convecdiscrtype;
-    const int second = P.par.secondconvecdiscrtype;
+    int convec = par.convecdiscrtype;
+    const int second = par.secondconvecdiscrtype;
     double conv1 = 0.0, conv2 = 0.0;
     const double ufacet = F.u[d][f];
     double Fs = hf::query(R, SL(HF_V_FU), F.FU[d]);
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
         for (int d2 = 0; d2 < D; d2++) tens += dSdx[d2];
     }
 #undef SL
-    const double pterm = P.par.projtype == HF_INCREMENTAL ? dpdx : 0.0;
+    const double pterm = par.projtype == HF_INCREMENTAL ? dpdx : 0.0;
     double conv = 0.0;
     if (convec == HF_CENTRAL) {
 #pragma unroll
@@ -362,7 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
     double diff = 0.0;
 #pragma unroll
     for (int d2 = 0; d2 < D; d2++) diff += du2dx2[d2];
-    diff /= P.par.Re;
+    diff /= par.Re;
     double rhs = 0.0;
     if (!VE) {
         rhs -= pterm;
@@ -376,7 +384,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
         rhs -= conv;
         rhs += diff;
     }
-    F.us[d][f] = ufacet + P.par.dt * rhs;
+    F.us[d][f] = ufacet + par.dt * rhs;
 }
 
 // ---------------------------------------------------------------------------
@@ -392,7 +400,7 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
 #define CS(s) __ldg(P.cslots + (size_t)(s) * n + cc)
     const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
     const uint32_t fl = __ldg(P.cflags + cc);
-    const hf_params &pr = P.par;
+    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
     // velocity at the faces of this cell, shared by Du, u_c and the CUBISTA flux
     double vl[D], vr[D];
 #pragma unroll
@@ -653,7 +661,9 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(DevMat M, CGVec V, const
         Scal &s = *V.sc;
         s.pq = tot[0];
         if (!(tot[0] > 0.0) || !finite(tot[0])) {
-            s.status = finite(tot[0]) ? HF_ERR_NOT_CONVERGED : HF_ERR_NAN;
+            // p.q <= 0: the recurrence has reached rounding level.  Accept when
+            // the residual is within 100x of the target, else report it.
+            s.status = !finite(tot[0]) ? HF_ERR_NAN : (s.rr <= 1e4 * s.tol2 ? 0 : HF_ERR_NOT_CONVERGED);
             s.done = 1;
         } else {
             s.alpha = s.rz / tot[0];
@@ -686,6 +696,185 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(DevMat M, CGVec V, const d
         s.iters += 1;
         if (!finite(tot[0]) || !finite(tot[1])) { s.status = HF_ERR_NAN; s.done = 1; }
         else if (!(tot[1] > s.tol2)) s.done = 1;
+        else if (s.iters >= s.maxit) { s.status = HF_ERR_NOT_CONVERGED; s.done = 1; }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CG preconditioned by an AMG V-cycle (hf_amg.cuh): the residual update and the
+// preconditioner are separate launches; the last V-cycle kernel on the finest
+// level finishes r.z and the CG beta.
+// ---------------------------------------------------------------------------
+constexpr int kMaxLevels = 20;
+
+struct DevCSR {
+    int n;
+    const int32_t *ptr;
+    const int32_t *col;
+    const double *val;
+};
+
+struct DevLevel {
+    DevCSR A, P, R;
+    const double *dinv;
+    double *b, *x, *r, *out;
+};
+
+struct DevAMG {
+    int nlev;        // levels with a smoother; the coarsest has a dense inverse
+    DevLevel lev[kMaxLevels];
+    int cn;
+    const double *cinv;
+    double *cb, *cx;
+};
+
+constexpr double kSmoothW = 2.0 / 3.0;
+
+__device__ __forceinline__ double csr_row(const DevCSR &A, int i, const double *__restrict__ x)
+{
+    double s = 0.0;
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++) s += A.val[k] * x[A.col[k]];
+    return s;
+}
+
+__global__ void __launch_bounds__(kBlock) k_vc_smooth0(DevLevel L, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.A.n) L.x[i] = kSmoothW * L.dinv[i] * L.b[i];
+}
+
+__global__ void __launch_bounds__(kBlock) k_vc_residual(DevLevel L, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.A.n) L.r[i] = L.b[i] - csr_row(L.A, i, L.x);
+}
+
+// b_next = R r
+__global__ void __launch_bounds__(kBlock) k_vc_restrict(DevCSR R, const double *__restrict__ r, double *bn, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < R.n) bn[i] = csr_row(R, i, r);
+}
+
+// x = inv b on the coarsest level (dense, row-major)
+__global__ void __launch_bounds__(kBlock) k_vc_coarse(int n, const double *__restrict__ inv, const double *__restrict__ b,
+                                                    double *x, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int k = 0; k < n; k++) s += inv[(size_t)i * n + k] * b[k];
+    x[i] = s;
+}
+
+// x += P e
+__global__ void __launch_bounds__(kBlock) k_vc_prolong(DevLevel L, const double *__restrict__ e, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.P.n) L.x[i] += csr_row(L.P, i, e);
+}
+
+// out = x + w D^-1 (b - A x)
+__global__ void __launch_bounds__(kBlock) k_vc_post(DevLevel L, const Scal *sc)
+{
+    if (sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.A.n) L.out[i] = L.x[i] + kSmoothW * L.dinv[i] * (L.b[i] - csr_row(L.A, i, L.x));
+}
+
+// finest-level post-smoothing writes z and finishes r.z -> beta
+__global__ void __launch_bounds__(kBlock) k_vc_post_fine(DevLevel L, CGVec V)
+{
+    if (V.sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[1] = {0.0};
+    if (i < L.A.n) {
+        const double z = L.x[i] + kSmoothW * L.dinv[i] * (L.b[i] - csr_row(L.A, i, L.x));
+        V.z[i] = z;
+        part[0] = L.b[i] * z;   // b of the finest level is the CG residual
+    }
+    double tot[1];
+    if (grid_sum<1>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
+        Scal &s = *V.sc;
+        if (s.iters == 0) s.beta = 0.0;
+        else s.beta = tot[0] / s.rz;
+        s.rz = tot[0];
+        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
+    }
+}
+
+// first residual of the AMG-preconditioned solve (z comes from the V-cycle)
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, DevMat M, CGVec V, double rtol, double atol)
+{
+    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P.ncell;
+    double part[2] = {0.0, 0.0};  // r.r, b.b
+    if (cc < n) {
+        const double pinv = P.pin >= 0
+            ? (P.par.projtype == HF_INCREMENTAL ? P.pin_value - F.p[P.pin] : P.pin_value) : 0.0;
+        double borig;
+        if (cc == P.pin) {
+            borig = pinv;
+        } else {
+            const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
+            double sumdudx = 0.0;
+#pragma unroll
+            for (int dim = 0; dim < D; dim++) {
+                const double ustarl = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UL(dim) * n + cc), F.us[dim]);
+                const double ustarr = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UR(dim) * n + cc), F.us[dim]);
+                sumdudx += (ustarr - ustarl) / (2.0 * 0.5 * cd[dim]);
+            }
+            borig = sumdudx / P.par.dt + M.brhs[cc];
+        }
+        const double bred = cc == P.pin ? pinv : -(borig - M.apin[cc] * pinv);
+        double ax = 0.0;
+        for (int k = M.ptr[cc]; k < M.ptr[cc + 1]; k++) ax += M.val[k] * V.x[M.col[k]];
+        const double r = bred - ax;
+        V.r[cc] = r;
+        part[0] = r * r;
+        part[1] = borig * borig;
+    }
+    double tot[2];
+    if (grid_sum<2>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
+        Scal &s = *V.sc;
+        s.rr = tot[0];
+        s.bb = tot[1];
+        const double t = fmax(rtol * sqrt(tot[1]), atol);
+        s.tol2 = t * t;
+        s.beta = 0.0;
+        s.iters = 0;
+        s.status = 0;
+        s.done = !(tot[0] > s.tol2);
+        if (!finite(tot[0]) || !finite(tot[1])) { s.status = HF_ERR_NAN; s.done = 1; }
+    }
+}
+
+// x += alpha p ; r -= alpha q ; convergence on ||r||
+__global__ void __launch_bounds__(kBlock) k_pcg_update(DevMat M, CGVec V, const double *__restrict__ pn)
+{
+    if (V.sc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double alpha = V.sc->alpha;
+    double part[1] = {0.0};
+    if (i < M.n) {
+        V.x[i] += alpha * pn[i];
+        const double r = V.r[i] - alpha * V.q[i];
+        V.r[i] = r;
+        part[0] = r * r;
+    }
+    double tot[1];
+    if (grid_sum<1>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
+        Scal &s = *V.sc;
+        s.rr = tot[0];
+        s.iters += 1;
+        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
+        else if (!(tot[0] > s.tol2)) s.done = 1;
         else if (s.iters >= s.maxit) { s.status = HF_ERR_NOT_CONVERGED; s.done = 1; }
     }
 }
@@ -847,29 +1036,26 @@ template <int D>
 __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const double *pp = P.par.projtype == HF_INCREMENTAL ? F.dp : F.p;
     if (e < P.off[D]) {
         int d = 0;
 #pragma unroll
         for (int k = 1; k < D; k++) d += (e >= P.off[k]);
         const int f = e - P.off[d];
         const int nf = P.nf[d];
+        const hf_params &par = P.ipar[__ldg(P.finst[d] + f)];
+        const double *pp = par.projtype == HF_INCREMENTAL ? F.dp : F.p;
         const double *fd = P.delta + (size_t)__ldg(P.vdelta[d] + f) * D;
         const double pl = hf::query(P.rows, __ldg(P.vslots[d] + (size_t)HF_V_PL * nf + f), pp);
         const double pr = hf::query(P.rows, __ldg(P.vslots[d] + (size_t)HF_V_PR * nf + f), pp);
         const double dpdx = (pr - pl) / (2.0 * 0.5 * fd[d]);
-        F.u[d][f] = F.us[d][f] - P.par.dt * dpdx;
-    } else if (P.par.projtype == HF_INCREMENTAL) {
+        F.u[d][f] = F.us[d][f] - par.dt * dpdx;
+    } else {
         const int c = e - P.off[D];
-        if (c < P.ncell) F.p[c] = F.p[c] + F.dp[c];
+        if (c < P.ncell && P.ipar[__ldg(P.cinst + c)].projtype == HF_INCREMENTAL) F.p[c] = F.p[c] + F.dp[c];
     }
 }
 
-__global__ void k_fill(double *x, double v, size_t n)
-{
-    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (i < n) x[i] = v;
-}
+#include "hf_batch.cuh"
 
 // ---------------------------------------------------------------------------
 // host side
@@ -901,6 +1087,22 @@ struct hf_case {
     CGVec cg;
     BiVec bi;
     bool use_cg;
+    bool use_amg = false;
+    DevAMG amg{};
+    int amg_levels = 0;
+    // instances and the persistent per-instance Poisson solver (hf_batch.cuh)
+    int ninst = 1;
+    std::vector<int> coff;          // ninst + 1
+    std::vector<int> foff[3];       // ninst + 1 per direction
+    bool persistent = false;
+    InstSolve *d_inst = nullptr;
+    ILevel<double> *d_l64 = nullptr;
+    ILevel<float> *d_l32 = nullptr;
+    int *d_res_i = nullptr;         // iters, outer, status per instance (3 * ninst)
+    double *d_res_d = nullptr;      // residual per instance
+    int *h_res_i = nullptr;         // pinned mirrors
+    double *h_res_d = nullptr;
+    int64_t batch_levels = 0;
     std::vector<void *> owned;
     cudaStream_t stream = nullptr;
     Scal *h_scal = nullptr;   // pinned host mirror
@@ -941,17 +1143,20 @@ struct PhaseTimer {
 namespace {
 
 // Build the reduced, negated Poisson operator on the host.
-int build_matrix(const hf_program *pg, std::vector<int32_t> &ptr, std::vector<int32_t> &col,
+int build_matrix(const hf_program *pg, const std::vector<int> &pins, std::vector<int32_t> &ptr, std::vector<int32_t> &col,
                  std::vector<double> &val, std::vector<double> &dinv, std::vector<double> &apin, bool &symmetric)
 {
-    const int n = pg->ncell, pin = pg->pin_row;
+    const int n = pg->ncell;
+    std::vector<char> pinned(n, 0);
+    for (int p : pins)
+        if (p >= 0) pinned[p] = 1;
     ptr.assign(n + 1, 0);
     col.clear();
     val.clear();
     dinv.assign(n, 1.0);
     apin.assign(n, 0.0);
     for (int r = 0; r < n; r++) {
-        if (r == pin) {
+        if (pinned[r]) {
             col.push_back(r);
             val.push_back(1.0);
         } else {
@@ -960,7 +1165,7 @@ int build_matrix(const hf_program *pg, std::vector<int32_t> &ptr, std::vector<in
                 int c = pg->p_col[k];
                 if (c < 0 || c >= n) return fail(HF_ERR_INVALID, "Poisson column out of range");
                 double v = pg->p_val[k];
-                if (c == pin) { apin[r] += v; continue; }
+                if (pinned[c]) { apin[r] += v; continue; }   // a row only reaches its own instance's pin
                 col.push_back(c);
                 val.push_back(-v);
                 if (c == r) diag += -v;
@@ -1109,6 +1314,203 @@ int check_rows(const hf_program *pg)
     return HF_OK;
 }
 
+// Host staging for many small device arrays: one allocation, one copy.
+struct Arena {
+    std::vector<char> host;
+    size_t add(const void *src, size_t bytes)
+    {
+        const size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + (bytes ? bytes : 8), 0);
+        if (src && bytes) memcpy(host.data() + off, src, bytes);
+        return off;
+    }
+    template <typename T>
+    size_t vec(const std::vector<T> &v) { return add(v.data(), v.size() * sizeof(T)); }
+    template <typename T>
+    size_t zeros(size_t n) { return add(nullptr, n * sizeof(T)); }
+};
+
+template <typename T>
+std::vector<T> cast_vec(const std::vector<double> &v)
+{
+    return std::vector<T>(v.begin(), v.end());
+}
+
+// Per-instance AMG hierarchies and work vectors for the persistent solver.
+int build_batch_solver(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<int32_t> &mcol,
+                       const std::vector<double> &mval, const double *apin_dev, const double *brhs_dev,
+                       const std::vector<int> &pins, bool mixed)
+{
+    const int ni = C->ninst;
+    struct LvlOff { int n; size_t Ap, Ac, Av, Av32, Pp, Pc, Pv, Pv32, Rp, Rc, Rv, Rv32, d, d32, x, b, r, out, x32, b32, r32, out32; };
+    struct InstOff {
+        int n, coff, nlev, cn, pin;
+        size_t cinv, cinv32, cb, cx, cb32, cx32, b, r, z, p, q, r32a, e32, t32, z32, p32, q32;
+        std::vector<LvlOff> lv;
+    };
+    Arena ar;
+    std::vector<InstOff> io(ni);
+    for (int i = 0; i < ni; i++) {
+        InstOff &o = io[i];
+        const int c0 = C->coff[i], n = C->coff[i + 1] - C->coff[i];
+        o.n = n;
+        o.coff = c0;
+        o.pin = pins[i] >= 0 ? pins[i] - c0 : -1;
+        hf::HostCSR A;
+        A.n = A.m = n;
+        A.ptr.assign(n + 1, 0);
+        for (int r = 0; r < n; r++) {
+            for (int k = mptr[c0 + r]; k < mptr[c0 + r + 1]; k++) {
+                const int c = mcol[k] - c0;
+                if (c < 0 || c >= n) return fail(HF_ERR_INVALID, "Poisson row reaches another instance");
+                A.col.push_back(c);
+                A.val.push_back(mval[k]);
+            }
+            A.ptr[r + 1] = (int)A.col.size();
+        }
+        std::vector<hf::HostLevel> H = hf::build_hierarchy(A, 64);
+        const hf::HostCSR &Cc = H.back().A;
+        if (Cc.n > 2048) return fail(HF_ERR_UNSUPPORTED, "AMG coarsening stalled above 2048 rows");
+        std::vector<double> inv;
+        if (!hf::dense_inverse(Cc, inv)) return fail(HF_ERR_INVALID, "singular coarsest AMG level");
+        o.nlev = (int)H.size() - 1;
+        o.cn = Cc.n;
+        o.cinv = ar.vec(inv);
+        o.cinv32 = mixed ? ar.vec(cast_vec<float>(inv)) : 0;
+        o.cb = ar.zeros<double>(o.cn);
+        o.cx = ar.zeros<double>(o.cn);
+        o.cb32 = mixed ? ar.zeros<float>(o.cn) : 0;
+        o.cx32 = mixed ? ar.zeros<float>(o.cn) : 0;
+        const int nl = std::max(o.nlev, 1);
+        for (int l = 0; l < nl; l++) {
+            const hf::HostLevel &h = H[l];
+            LvlOff L{};
+            L.n = h.A.n;
+            L.Ap = ar.vec(h.A.ptr);
+            L.Ac = ar.vec(h.A.col);
+            L.Av = ar.vec(h.A.val);
+            L.d = ar.vec(h.dinv);
+            if (l < o.nlev) {
+                L.Pp = ar.vec(h.P.ptr); L.Pc = ar.vec(h.P.col); L.Pv = ar.vec(h.P.val);
+                L.Rp = ar.vec(h.R.ptr); L.Rc = ar.vec(h.R.col); L.Rv = ar.vec(h.R.val);
+            }
+            L.x = ar.zeros<double>(L.n); L.b = ar.zeros<double>(L.n);
+            L.r = ar.zeros<double>(L.n); L.out = ar.zeros<double>(L.n);
+            if (mixed) {
+                L.Av32 = ar.vec(cast_vec<float>(h.A.val));
+                L.d32 = ar.vec(cast_vec<float>(h.dinv));
+                if (l < o.nlev) { L.Pv32 = ar.vec(cast_vec<float>(h.P.val)); L.Rv32 = ar.vec(cast_vec<float>(h.R.val)); }
+                L.x32 = ar.zeros<float>(L.n); L.b32 = ar.zeros<float>(L.n);
+                L.r32 = ar.zeros<float>(L.n); L.out32 = ar.zeros<float>(L.n);
+            }
+            o.lv.push_back(L);
+        }
+        o.b = ar.zeros<double>(n); o.r = ar.zeros<double>(n); o.z = ar.zeros<double>(n);
+        o.p = ar.zeros<double>(n); o.q = ar.zeros<double>(n);
+        if (mixed) {
+            o.r32a = ar.zeros<float>(n); o.e32 = ar.zeros<float>(n); o.t32 = ar.zeros<float>(n);
+            o.z32 = ar.zeros<float>(n); o.p32 = ar.zeros<float>(n); o.q32 = ar.zeros<float>(n);
+        }
+        C->batch_levels += nl;
+    }
+    char *base = nullptr;
+    HF_CK(cudaMalloc((void **)&base, ar.host.size()));
+    C->owned.push_back(base);
+    C->bytes += (double)ar.host.size();
+    HF_CK(cudaMemcpy(base, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice));
+    auto I = [&](size_t off) { return (int32_t *)(base + off); };
+    auto Dp = [&](size_t off) { return (double *)(base + off); };
+    auto Fp = [&](size_t off) { return mixed ? (float *)(base + off) : (float *)nullptr; };
+    std::vector<ILevel<double>> l64;
+    std::vector<ILevel<float>> l32;
+    std::vector<InstSolve> is(ni);
+    // largest instance first, so the longest solves start in the first wave
+    std::vector<int> order(ni);
+    for (int i = 0; i < ni; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return io[a].n > io[b].n; });
+    for (int k = 0; k < ni; k++) {
+        const int i = order[k];
+        const InstOff &o = io[i];
+        InstSolve &s = is[k];
+        s.inst = i;
+        s.n = o.n;
+        s.coff = o.coff;
+        s.nlev = o.nlev;
+        s.lev = (int)l64.size();
+        s.cn = o.cn;
+        s.cinv64 = Dp(o.cinv);
+        s.cinv32 = mixed ? (const float *)(base + o.cinv32) : nullptr;
+        s.cb64 = Dp(o.cb); s.cx64 = Dp(o.cx);
+        s.cb32 = Fp(o.cb32); s.cx32 = Fp(o.cx32);
+        s.Mp = I(o.lv[0].Ap); s.Mc = I(o.lv[0].Ac); s.Mv = Dp(o.lv[0].Av);
+        s.apin = apin_dev + o.coff;
+        s.brhs = brhs_dev + o.coff;
+        s.pin = o.pin;
+        s.b = Dp(o.b); s.r = Dp(o.r); s.z = Dp(o.z); s.p = Dp(o.p); s.q = Dp(o.q);
+        s.r32 = Fp(o.r32a); s.e32 = Fp(o.e32); s.t32 = Fp(o.t32);
+        s.z32 = Fp(o.z32); s.p32 = Fp(o.p32); s.q32 = Fp(o.q32);
+        s.iters = C->d_res_i + 3 * i;
+        s.outer = C->d_res_i + 3 * i + 1;
+        s.status = C->d_res_i + 3 * i + 2;
+        s.res = C->d_res_d + i;
+        for (const LvlOff &L : o.lv) {
+            ILevel<double> a{};
+            a.n = L.n;
+            a.Ap = I(L.Ap); a.Ac = I(L.Ac); a.Av = Dp(L.Av);
+            a.Pp = L.Pp ? I(L.Pp) : nullptr; a.Pc = L.Pc ? I(L.Pc) : nullptr; a.Pv = L.Pv ? Dp(L.Pv) : nullptr;
+            a.Rp = L.Rp ? I(L.Rp) : nullptr; a.Rc = L.Rc ? I(L.Rc) : nullptr; a.Rv = L.Rv ? Dp(L.Rv) : nullptr;
+            a.dinv = Dp(L.d);
+            a.x = Dp(L.x); a.b = Dp(L.b); a.r = Dp(L.r); a.out = Dp(L.out);
+            l64.push_back(a);
+            ILevel<float> f{};
+            if (mixed) {
+                f.n = L.n;
+                f.Ap = a.Ap; f.Ac = a.Ac; f.Av = Fp(L.Av32);
+                f.Pp = a.Pp; f.Pc = a.Pc; f.Pv = L.Pv32 ? Fp(L.Pv32) : nullptr;
+                f.Rp = a.Rp; f.Rc = a.Rc; f.Rv = L.Rv32 ? Fp(L.Rv32) : nullptr;
+                f.dinv = Fp(L.d32);
+                f.x = Fp(L.x32); f.b = Fp(L.b32); f.r = Fp(L.r32); f.out = Fp(L.out32);
+            }
+            l32.push_back(f);
+        }
+    }
+    double bytes = 0;
+    int rc;
+    if ((rc = upload(C->owned, &C->d_inst, is.data(), is.size(), bytes))) return rc;
+    if ((rc = upload(C->owned, &C->d_l64, l64.data(), l64.size(), bytes))) return rc;
+    if ((rc = upload(C->owned, &C->d_l32, l32.data(), l32.size(), bytes))) return rc;
+    C->bytes += bytes;
+    return HF_OK;
+}
+
+// one V-cycle z = V(r) on the case stream (hf_amg.cuh)
+int64_t launch_vcycle(hf_case *C)
+{
+    const DevAMG &A = C->amg;
+    cudaStream_t st = C->stream;
+    const Scal *sc = C->cg.sc;
+    int64_t launches = 0;
+    for (int l = 0; l < A.nlev; l++) {
+        const DevLevel &L = A.lev[l];
+        k_vc_smooth0<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
+        k_vc_residual<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
+        double *bn = l + 1 < A.nlev ? A.lev[l + 1].b : A.cb;
+        k_vc_restrict<<<blocks(L.R.n), kBlock, 0, st>>>(L.R, L.r, bn, sc);
+        launches += 3;
+    }
+    k_vc_coarse<<<blocks(A.cn), kBlock, 0, st>>>(A.cn, A.cinv, A.cb, A.cx, sc);
+    launches++;
+    for (int l = A.nlev - 1; l >= 0; l--) {
+        const DevLevel &L = A.lev[l];
+        const double *e = l + 1 < A.nlev ? A.lev[l + 1].out : A.cx;
+        k_vc_prolong<<<blocks(L.P.n), kBlock, 0, st>>>(L, e, sc);
+        if (l == 0) k_vc_post_fine<<<blocks(L.A.n), kBlock, 0, st>>>(L, C->cg);
+        else k_vc_post<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
+        launches += 2;
+    }
+    return launches;
+}
+
 template <int D>
 int launch_step(hf_case *C)
 {
@@ -1133,7 +1535,63 @@ int launch_step(hf_case *C)
     const double rtol = C->opt.poisson_rtol, atol = C->opt.poisson_atol;
     const int n = C->P.ncell;
     int rc = HF_OK;
-    if (C->use_cg) {
+    if (C->persistent) {
+        {
+            PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
+            k_batch_poisson<D><<<C->ninst, kPB, 0, st>>>(C->P, C->F, C->d_inst, C->d_l64, C->d_l32,
+                                                          C->opt.precision == HF_PREC_MIXED, rtol, atol,
+                                                          C->opt.poisson_maxit);
+            launches++;
+            t.stop(launches);
+        }
+        HF_CK(cudaGetLastError());
+        HF_CK(cudaMemcpyAsync(C->h_res_i, C->d_res_i, sizeof(int) * 3 * C->ninst, cudaMemcpyDeviceToHost, st));
+        HF_CK(cudaMemcpyAsync(C->h_res_d, C->d_res_d, sizeof(double) * C->ninst, cudaMemcpyDeviceToHost, st));
+        HF_CK(cudaStreamSynchronize(st));
+        int it_max = 0, out_max = 0;
+        int64_t it_sum = 0;
+        double res_max = 0.0;
+        for (int i = 0; i < C->ninst; i++) {
+            it_max = std::max(it_max, C->h_res_i[3 * i]);
+            out_max = std::max(out_max, C->h_res_i[3 * i + 1]);
+            it_sum += C->h_res_i[3 * i];
+            res_max = std::max(res_max, C->h_res_d[i]);
+            if (C->h_res_i[3 * i + 2] && rc == HF_OK)
+                rc = fail(C->h_res_i[3 * i + 2], "Poisson solve failed in instance " + std::to_string(i));
+        }
+        C->h_scal->iters = it_max;
+        C->h_scal->rr = res_max * res_max;
+        C->h_scal->bb = 1.0;
+        C->stats.last_outer = out_max;
+        C->stats.total_iters += it_sum - it_max;   // the common update below adds it_max
+    } else if (C->use_cg && C->use_amg) {
+        {
+            PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
+            k_pcg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
+            launches++;
+            launches += launch_vcycle(C);
+            t.stop(launches);
+        }
+        double *pa = C->cg.pa, *pb = C->cg.pb;
+        int chunk = 4;
+        for (;;) {
+            PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
+            for (int k = 0; k < chunk; k++) {
+                k_cg_dir_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pa, pb);
+                k_pcg_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pb);
+                launches += 2 + launch_vcycle(C);
+                std::swap(pa, pb);
+            }
+            t.stop(launches);
+            HF_CK(cudaMemcpyAsync(C->h_scal, C->cg.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+            HF_CK(cudaStreamSynchronize(st));
+            if (C->h_scal->done) break;
+            chunk = std::min(chunk * 2, 16);
+        }
+        C->cg.pa = pa;
+        C->cg.pb = pb;
+        if (C->h_scal->status) rc = fail(C->h_scal->status, "Poisson AMG-CG failed");
+    } else if (C->use_cg) {
         {
             PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
             k_cg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
@@ -1277,11 +1735,59 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     C->nfacet_total = P.off[D];
     P.vns = pg->vel_nslot;
     P.cns = pg->cell_nslot;
-    P.pin = pg->pin_row;
-    P.pin_value = pg->pin_value;
     double &B = C->bytes;
     auto &own = C->owned;
 #define UP(dst, src, n) do { if ((rc = upload(own, dst, src, (size_t)(n), B))) return cleanup(rc); } while (0)
+    // instances: a plain program is a batch of one
+    std::vector<hf_params> ipar;
+    std::vector<int> pins;
+    std::vector<double> pinv;
+    if (pg->ninst > 0) {
+        C->ninst = pg->ninst;
+        for (int i = 0; i < pg->ninst; i++) {
+            ipar.push_back(pg->inst_par[i]);
+            pins.push_back(pg->inst_pin[i]);
+            pinv.push_back(pg->inst_pin_value[i]);
+            if (pg->inst_par[i].dim != D || pg->inst_par[i].flowtype != pg->par.flowtype)
+                return cleanup(fail(HF_ERR_INVALID, "batch members differ in dim or flow type"));
+        }
+        C->coff.assign(pg->cell_off, pg->cell_off + pg->ninst + 1);
+        for (int d = 0; d < D; d++) C->foff[d].assign(pg->facet_off[d], pg->facet_off[d] + pg->ninst + 1);
+    } else {
+        C->ninst = 1;
+        ipar.push_back(pg->par);
+        pins.push_back(pg->pin_row);
+        pinv.push_back(pg->pin_value);
+        C->coff = {0, pg->ncell};
+        for (int d = 0; d < D; d++) C->foff[d] = {0, pg->nfacet[d]};
+    }
+    const int ni = C->ninst;
+    if (C->coff[0] != 0 || C->coff[ni] != pg->ncell) return cleanup(fail(HF_ERR_INVALID, "cell offsets"));
+    for (int d = 0; d < D; d++)
+        if (C->foff[d][0] != 0 || C->foff[d][ni] != pg->nfacet[d]) return cleanup(fail(HF_ERR_INVALID, "facet offsets"));
+    for (int i = 0; i < ni; i++) {
+        if (C->coff[i + 1] <= C->coff[i]) return cleanup(fail(HF_ERR_INVALID, "empty instance"));
+        if (pins[i] >= 0 && (pins[i] < C->coff[i] || pins[i] >= C->coff[i + 1]))
+            return cleanup(fail(HF_ERR_INVALID, "pin outside its instance"));
+    }
+    P.par = ipar[0];
+    P.pin = pins[0];
+    P.pin_value = pinv[0];
+    P.ninst = ni;
+    {
+        std::vector<int32_t> cinst(pg->ncell);
+        for (int i = 0; i < ni; i++)
+            for (int c = C->coff[i]; c < C->coff[i + 1]; c++) cinst[c] = i;
+        UP((int32_t **)&P.cinst, cinst.data(), cinst.size());
+        for (int d = 0; d < D; d++) {
+            std::vector<int32_t> finst(pg->nfacet[d]);
+            for (int i = 0; i < ni; i++)
+                for (int f = C->foff[d][i]; f < C->foff[d][i + 1]; f++) finst[f] = i;
+            UP((int32_t **)&P.finst[d], finst.data(), finst.size());
+        }
+        UP((hf_params **)&P.ipar, ipar.data(), ipar.size());
+        UP((double **)&P.ipinv, pinv.data(), pinv.size());
+    }
     UP((double **)&P.delta, pg->delta, (size_t)pg->ndelta * D);
     UP((int32_t **)&P.rows.tmpl, pg->row_tmpl, pg->nrows);
     UP((int32_t **)&P.rows.base, pg->row_base, pg->nrows);
@@ -1323,9 +1829,17 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     std::vector<int32_t> mptr, mcol;
     std::vector<double> mval, dinv, apin;
     bool sym = false;
-    if ((rc = build_matrix(pg, mptr, mcol, mval, dinv, apin, sym))) return cleanup(rc);
+    if ((rc = build_matrix(pg, pins, mptr, mcol, mval, dinv, apin, sym))) return cleanup(rc);
     C->use_cg = opt.poisson == HF_POISSON_CG || (opt.poisson == HF_POISSON_AUTO && sym);
     if (opt.poisson == HF_POISSON_CG && !sym) return cleanup(fail(HF_ERR_UNSUPPORTED, "CG requested on a non-symmetric Poisson matrix"));
+    // the persistent per-instance solver serves batches and small single cases;
+    // one large case keeps the multi-kernel solver
+    int maxn = 0;
+    for (int i = 0; i < ni; i++) maxn = std::max(maxn, C->coff[i + 1] - C->coff[i]);
+    C->persistent = C->use_cg && opt.precond != HF_PRECOND_JACOBI && (ni > 1 || maxn <= 131072);
+    if (ni > 1 && !C->persistent) return cleanup(fail(HF_ERR_UNSUPPORTED, "batches need the AMG-CG Poisson solver"));
+    if (opt.precision == HF_PREC_MIXED && !C->persistent)
+        return cleanup(fail(HF_ERR_UNSUPPORTED, "the mixed form runs on the persistent per-instance solver"));
     DevMat &M = C->M;
     M.n = pg->ncell;
     UP((int32_t **)&M.ptr, mptr.data(), mptr.size());
@@ -1354,6 +1868,61 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         UP(&C->cg.q, (const double *)nullptr, n);
         C->cg.partials = partials;
         C->cg.sc = sc;
+        C->use_amg = opt.precond != HF_PRECOND_JACOBI && !C->persistent;
+        if (C->persistent) {
+            UP(&C->d_res_i, (const int *)nullptr, (size_t)3 * ni);
+            UP(&C->d_res_d, (const double *)nullptr, (size_t)ni);
+            if (cudaMallocHost((void **)&C->h_res_i, sizeof(int) * 3 * ni) != cudaSuccess ||
+                cudaMallocHost((void **)&C->h_res_d, sizeof(double) * ni) != cudaSuccess)
+                return cleanup(fail(HF_ERR_CUDA, "pinned results"));
+            if ((rc = build_batch_solver(C, mptr, mcol, mval, M.apin, M.brhs, pins, opt.precision == HF_PREC_MIXED)))
+                return cleanup(rc);
+        }
+        if (C->use_amg) {
+            hf::HostCSR M0;
+            M0.n = M0.m = n;
+            M0.ptr.assign(mptr.begin(), mptr.end());
+            M0.col.assign(mcol.begin(), mcol.end());
+            M0.val = mval;
+            std::vector<hf::HostLevel> H = hf::build_hierarchy(std::move(M0));
+            if ((int)H.size() - 1 > kMaxLevels) return cleanup(fail(HF_ERR_UNSUPPORTED, "AMG hierarchy too deep"));
+            DevAMG &A = C->amg;
+            A.nlev = (int)H.size() - 1;
+            C->amg_levels = (int)H.size();
+            for (int l = 0; l < A.nlev; l++) {
+                DevLevel &L = A.lev[l];
+                const hf::HostLevel &h = H[l];
+                auto up_csr = [&](DevCSR &d, const hf::HostCSR &s) {
+                    d.n = s.n;
+                    int r2;
+                    if ((r2 = upload(own, (int32_t **)&d.ptr, s.ptr.data(), s.ptr.size(), B))) return r2;
+                    if ((r2 = upload(own, (int32_t **)&d.col, s.col.data(), s.col.size(), B))) return r2;
+                    return upload(own, (double **)&d.val, s.val.data(), s.val.size(), B);
+                };
+                if (l == 0) {
+                    L.A = DevCSR{n, M.ptr, M.col, M.val};
+                } else if ((rc = up_csr(L.A, h.A))) {
+                    return cleanup(rc);
+                }
+                if ((rc = up_csr(L.P, h.P)) || (rc = up_csr(L.R, h.R))) return cleanup(rc);
+                UP((double **)&L.dinv, h.dinv.data(), h.dinv.size());
+                if (l == 0) {
+                    L.b = C->cg.r;
+                    L.out = C->cg.z;
+                } else {
+                    UP(&L.b, (const double *)nullptr, h.A.n);
+                    UP(&L.out, (const double *)nullptr, h.A.n);
+                }
+                UP(&L.x, (const double *)nullptr, h.A.n);
+                UP(&L.r, (const double *)nullptr, h.A.n);
+            }
+            std::vector<double> inv;
+            if (!hf::dense_inverse(H.back().A, inv)) return cleanup(fail(HF_ERR_INVALID, "singular coarsest AMG level"));
+            A.cn = H.back().A.n;
+            UP((double **)&A.cinv, inv.data(), inv.size());
+            UP(&A.cb, (const double *)nullptr, A.cn);
+            UP(&A.cx, (const double *)nullptr, A.cn);
+        }
     } else {
         BiVec &V = C->bi;
         V.x = pg->par.projtype == HF_INCREMENTAL ? F.dp : F.p;
@@ -1448,7 +2017,58 @@ extern "C" int hf_case_stats(hf_case *C, hf_stats *out)
 {
     if (!C || !out) return fail(HF_ERR_INVALID, "null argument");
     *out = C->stats;
-    out->last_outer = 1;
+    if (!C->persistent) out->last_outer = 1;
+    return HF_OK;
+}
+
+extern "C" int hf_case_instances(hf_case *C, int32_t *ninst)
+{
+    if (!C || !ninst) return fail(HF_ERR_INVALID, "null argument");
+    *ninst = C->ninst;
+    return HF_OK;
+}
+
+extern "C" int hf_case_instance_result(hf_case *C, int32_t inst, int32_t *iters, int32_t *outer, int32_t *status,
+                                       double *residual)
+{
+    if (!C || inst < 0 || inst >= C->ninst) return fail(HF_ERR_INVALID, "bad instance");
+    if (!C->persistent) {
+        if (iters) *iters = C->stats.last_iters;
+        if (outer) *outer = 1;
+        if (status) *status = 0;
+        if (residual) *residual = C->stats.last_residual;
+        return HF_OK;
+    }
+    if (iters) *iters = C->h_res_i[3 * inst];
+    if (outer) *outer = C->h_res_i[3 * inst + 1];
+    if (status) *status = C->h_res_i[3 * inst + 2];
+    if (residual) *residual = C->h_res_d[inst];
+    return HF_OK;
+}
+
+extern "C" int hf_case_solver_info(hf_case *C, int32_t *method, int32_t *nlev, int64_t *rows, int64_t *nnz_a,
+                                   int64_t *nnz_p, int64_t *nnz_r, int32_t max_levels)
+{
+    if (!C || !method || !nlev) return fail(HF_ERR_INVALID, "null argument");
+    *method = C->use_cg ? (C->use_amg ? HF_PRECOND_AMG : HF_PRECOND_JACOBI) : -1;
+    *nlev = C->use_amg ? C->amg.nlev + 1 : 1;
+    for (int l = 0; l < *nlev && l < max_levels; l++) {
+        if (!C->use_amg) {
+            if (rows) rows[l] = C->M.n;
+            continue;
+        }
+        const bool coarse = l == C->amg.nlev;
+        std::vector<int32_t> hp(2);
+        auto nnz = [&](const DevCSR &d) -> int64_t {
+            int32_t last = 0;
+            if (d.ptr && cudaMemcpy(&last, d.ptr + d.n, sizeof last, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+            return last;
+        };
+        if (rows) rows[l] = coarse ? C->amg.cn : C->amg.lev[l].A.n;
+        if (nnz_a) nnz_a[l] = coarse ? (int64_t)C->amg.cn * C->amg.cn : nnz(C->amg.lev[l].A);
+        if (nnz_p) nnz_p[l] = coarse ? 0 : nnz(C->amg.lev[l].P);
+        if (nnz_r) nnz_r[l] = coarse ? 0 : nnz(C->amg.lev[l].R);
+    }
     return HF_OK;
 }
 
@@ -1487,6 +2107,8 @@ extern "C" void hf_case_destroy(hf_case *C)
         if (C->ev[k]) cudaEventDestroy(C->ev[k]);
     for (void *p : C->owned) cudaFree(p);
     if (C->h_scal) cudaFreeHost(C->h_scal);
+    if (C->h_res_i) cudaFreeHost(C->h_res_i);
+    if (C->h_res_d) cudaFreeHost(C->h_res_d);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;
 }

@@ -46,6 +46,11 @@ def lib() -> C.CDLL:
         L.hf_case_destroy.restype = None
         L.hf_case_device_bytes.argtypes = [P(hp.HFProgram), P(hp.HFOptions), P(C.c_int64)]
         L.hf_case_stream.argtypes = [V, P(C.c_void_p)]
+        L.hf_case_instances.argtypes = [V, P(C.c_int32)]
+        L.hf_case_instance_result.argtypes = [V, C.c_int32, P(C.c_int32), P(C.c_int32), P(C.c_int32),
+                                              P(C.c_double)]
+        L.hf_case_solver_info.argtypes = [V, P(C.c_int32), P(C.c_int32), P(C.c_int64), P(C.c_int64),
+                                          P(C.c_int64), P(C.c_int64), C.c_int32]
         L.hf_case_profile.argtypes = [V, C.c_int32]
         L.hf_case_phase_times.argtypes = [V, P(C.c_double), P(C.c_int64), C.c_int32]
         _lib = L
@@ -58,10 +63,12 @@ def _check(rc: int) -> None:
 
 
 def options(precision: int = hp.PREC_FP64, poisson: int = hp.POISSON_AUTO, rtol: float = 1e-10,
-            atol: float = 1e-10, maxit: int = 20000, device: int = 0) -> hp.HFOptions:
+            atol: float = 1e-10, maxit: int = 20000, device: int = 0,
+            precond: int = hp.PRECOND_AUTO) -> hp.HFOptions:
     o = hp.HFOptions()
     o.precision, o.poisson = precision, poisson
     o.poisson_rtol, o.poisson_atol, o.poisson_maxit, o.device = rtol, atol, maxit, device
+    o.precond = precond
     return o
 
 
@@ -107,6 +114,25 @@ class Case:
         _check(lib().hf_case_stats(self.h, C.byref(s)))
         return s
 
+    def instances(self) -> int:
+        n = C.c_int32()
+        _check(lib().hf_case_instances(self.h, C.byref(n)))
+        return n.value
+
+    def instance_result(self, inst: int):
+        """Last step's Poisson result of one instance: (iters, outer, status, residual)."""
+        it, ou, st, res = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _check(lib().hf_case_instance_result(self.h, inst, C.byref(it), C.byref(ou), C.byref(st), C.byref(res)))
+        return it.value, ou.value, st.value, res.value
+
+    def get_instance(self, fid: int, comp: int, inst: int) -> np.ndarray:
+        """Field values of one instance of a batch program."""
+        a = self.get(fid, comp)
+        if self.prog.ninst == 0:
+            return a
+        off = self.prog.cell_off if fid not in (hp.FIELD_U, hp.FIELD_USTAR, hp.FIELD_FU) else self.prog.facet_off[comp]
+        return a[off[inst]:off[inst + 1]]
+
     def stream(self) -> int:
         """Handle of the cudaStream_t all of this case's kernels run on."""
         p = C.c_void_p()
@@ -116,6 +142,15 @@ class Case:
     def profile(self, enable: bool = True) -> None:
         """Turn per-phase CUDA-event timing on/off (resets the counters)."""
         _check(lib().hf_case_profile(self.h, 1 if enable else 0))
+
+    def solver_info(self):
+        """{'method', 'levels': [(rows, nnz_A, nnz_P, nnz_R), ...]} of the Poisson solver."""
+        m, nl = C.c_int32(), C.c_int32()
+        k = 32
+        rows, na, npp, nr = (C.c_int64 * k)(), (C.c_int64 * k)(), (C.c_int64 * k)(), (C.c_int64 * k)()
+        _check(lib().hf_case_solver_info(self.h, C.byref(m), C.byref(nl), rows, na, npp, nr, k))
+        method = {hp.PRECOND_AMG: "amg-cg", hp.PRECOND_JACOBI: "jacobi-cg", -1: "bicgstab"}[m.value]
+        return {"method": method, "levels": [(rows[i], na[i], npp[i], nr[i]) for i in range(nl.value)]}
 
     PHASES = ("ve_cell", "velocity", "poisson_init", "poisson_iter", "final")
 

@@ -27,6 +27,7 @@ CELL_CENTRAL, CELL_CUBISTA = 0, 1
 KERNEL_IDENTITY, KERNEL_LOG, KERNEL_SQRT = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 POISSON_AUTO, POISSON_CG, POISSON_BICGSTAB = 0, 1, 2
+PRECOND_AUTO, PRECOND_JACOBI, PRECOND_AMG = 0, 1, 2
 
 FIELD_U, FIELD_USTAR, FIELD_P, FIELD_DP, FIELD_F, FIELD_FU, FIELD_KERNEL, FIELD_S, FIELD_DU = range(9)
 
@@ -46,6 +47,29 @@ def v_nslot(dim: int, ve: bool) -> int:
 
 def c_nslot(dim: int) -> int:
     return C_BLK0 + C_NB * dim + C_NQ * dim * (dim - 1)
+
+
+def vel_slot_grid(D: int, d: int, s: int) -> int:
+    """Field grid a velocity-stage slot reads: -1 cells, k >= 0 facets normal to k."""
+    if s == V_FU:
+        return d
+    if s <= V_FR:
+        return -1
+    if s < v_nslot(D, False):
+        d2, k = divmod(s - V_BLK0, V_NB)
+        return d2 if (k < 4 or k >= 8) else d
+    return -1
+
+
+def cell_slot_grid(D: int, s: int) -> int:
+    """Field grid a viscoelastic cell-stage slot reads."""
+    if s == C_SELF:
+        return -1
+    if s < C_BLK0 + C_NB * D:
+        dim, k = divmod(s - C_BLK0, C_NB)
+        return dim if k < 2 else -1
+    pair = (s - C_BLK0 - C_NB * D) // C_NQ
+    return pair // (D - 1)
 
 
 class HFParams(C.Structure):
@@ -86,6 +110,12 @@ class HFProgram(C.Structure):
         ("cell_nslot", C.c_int32),
         ("cell_slots", _P(C.c_int32)),
         ("cell_flags", _P(C.c_uint32)),
+        ("ninst", C.c_int32),
+        ("inst_par", _P(HFParams)),
+        ("cell_off", _P(C.c_int32)),
+        ("facet_off", _P(C.c_int32) * 3),
+        ("inst_pin", _P(C.c_int32)),
+        ("inst_pin_value", _P(C.c_double)),
     ]
 
 
@@ -93,7 +123,7 @@ class HFOptions(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("poisson", C.c_int32),
         ("poisson_rtol", C.c_double), ("poisson_atol", C.c_double),
-        ("poisson_maxit", C.c_int32), ("device", C.c_int32),
+        ("poisson_maxit", C.c_int32), ("device", C.c_int32), ("precond", C.c_int32),
     ]
 
 
@@ -145,7 +175,17 @@ class Program:
     pin_value: float
     cell_slots: Optional[np.ndarray] = None   # (nslot, ncell) int32
     cell_flags: Optional[np.ndarray] = None
+    # batches (see include/higflow_b200.h): per-instance parameters and offsets
+    inst_par: Optional[list] = None
+    cell_off: Optional[np.ndarray] = None
+    facet_off: Optional[list] = None
+    inst_pin: Optional[np.ndarray] = None
+    inst_pin_value: Optional[np.ndarray] = None
     _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def ninst(self) -> int:
+        return 0 if self.inst_par is None else len(self.inst_par)
 
     @property
     def dim(self) -> int:
@@ -240,8 +280,166 @@ class Program:
             p.cell_flags = a(self.cell_flags, np.uint32, C.c_uint32)
         else:
             p.cell_nslot = 0
+        if self.inst_par is not None:
+            n = len(self.inst_par)
+            pars = (HFParams * n)()
+            for i, ip in enumerate(self.inst_par):
+                for nm in _PARAM_NAMES:
+                    setattr(pars[i], nm, ip[nm])
+            keep.append(pars)
+            p.ninst = n
+            p.inst_par = C.cast(pars, C.POINTER(HFParams))
+            p.cell_off = a(self.cell_off, np.int32, C.c_int32)
+            for d in range(self.dim):
+                p.facet_off[d] = a(self.facet_off[d], np.int32, C.c_int32)
+            p.inst_pin = a(self.inst_pin, np.int32, C.c_int32)
+            p.inst_pin_value = a(self.inst_pin_value, np.float64, C.c_double)
+        else:
+            p.ninst = 0
         self._keep = keep
         return p
+
+    # ------------------------------------------------------------------
+    @staticmethod
+    def concatenate(progs) -> "Program":
+        """One batch program holding independent cases side by side."""
+        progs = list(progs)
+        p0 = progs[0]
+        D = p0.dim
+        ve = p0.viscoelastic
+        for q in progs:
+            if q.dim != D or q.viscoelastic != ve or q.ninst:
+                raise ValueError("batch members must share dim and flow type and not be batches")
+        ni = len(progs)
+        co = np.zeros(ni + 1, dtype=np.int64)
+        fo = [np.zeros(ni + 1, dtype=np.int64) for _ in range(D)]
+        for i, q in enumerate(progs):
+            co[i + 1] = co[i] + q.ncell
+            for d in range(D):
+                fo[d][i + 1] = fo[d][i] + q.nfacet[d]
+        if co[-1] > np.iinfo(np.int32).max or any(f[-1] > np.iinfo(np.int32).max for f in fo):
+            raise ValueError("batch too large for int32 ids")
+
+        def goff(i, g):
+            return int(co[i]) if g < 0 else int(fo[g][i])
+
+        # distinct deltas across the batch
+        dtab, dmap = [], {}
+        delta_remap = []
+        for q in progs:
+            m = np.empty(q.delta.shape[0], dtype=np.int64)
+            for k, row in enumerate(q.delta):
+                key = tuple(row.tolist())
+                if key not in dmap:
+                    dmap[key] = len(dtab)
+                    dtab.append(row)
+                m[k] = dmap[key]
+            delta_remap.append(m)
+        if len(dtab) > 65535:
+            raise ValueError("too many distinct cell sizes in the batch")
+
+        row_tmpl, row_base, row_rhs = [], [], []
+        tptr, tcol, tw = [np.zeros(1, dtype=np.int64)], [], []
+        nrow = ntm = nnz = 0
+        vel = [[] for _ in range(D)]
+        div, cells = [], []
+
+        for i, q in enumerate(progs):
+            # slot arrays of this instance with the field grid each slot reads
+            arrays = []   # (output array, grid per slot row)
+            for d in range(D):
+                s = q.vel_slots[d].astype(np.int64)
+                arrays.append((s, [vel_slot_grid(D, d, k) for k in range(s.shape[0])]))
+            arrays.append((q.div_slots.astype(np.int64), [k // 2 for k in range(q.div_slots.shape[0])]))
+            if ve:
+                arrays.append((q.cell_slots.astype(np.int64), [cell_slot_grid(D, k) for k in range(q.cell_slots.shape[0])]))
+            # rows keep their order; a row read through slots of two different field
+            # grids (possible when recorded rows were merged by content) gets a copy
+            # per extra grid
+            nr = q.row_rhs.size
+            grid_of = np.full(nr, -9, dtype=np.int64)
+            extra = {}   # (row, grid) -> new index of the copy
+            for a, gs in arrays:
+                for k in range(len(gs)):
+                    r = -a[k][a[k] < 0] - 1
+                    g = gs[k]
+                    unset = grid_of[r] == -9
+                    grid_of[r[unset]] = g
+                    clash = np.unique(r[grid_of[r] != g])
+                    for rr in clash.tolist():
+                        extra.setdefault((rr, g), None)
+            base_off = np.array([goff(i, int(g)) if g != -9 else 0 for g in range(-1, D)], dtype=np.int64)
+            gidx = np.where(grid_of == -9, -1, grid_of) + 1
+            row_tmpl.append(q.row_tmpl.astype(np.int64) + ntm)
+            row_base.append(q.row_base.astype(np.int64) + base_off[gidx] * (grid_of != -9))
+            row_rhs.append(q.row_rhs)
+            first_new = nrow
+            nrow += nr
+            for key in list(extra):
+                rr, g = key
+                extra[key] = nrow
+                row_tmpl.append(np.array([int(q.row_tmpl[rr]) + ntm]))
+                row_base.append(np.array([int(q.row_base[rr]) + goff(i, g)]))
+                row_rhs.append(np.array([q.row_rhs[rr]]))
+                nrow += 1
+            for a, gs in arrays:
+                for k in range(len(gs)):
+                    row = a[k]
+                    g = gs[k]
+                    gen = row < 0
+                    r = -row[gen] - 1
+                    new = r + first_new
+                    if extra:
+                        for j in np.nonzero(grid_of[r] != g)[0].tolist():
+                            new[j] = extra[(int(r[j]), g)]
+                    row[gen] = -(new + 1)
+                    row[~gen] += goff(i, g)
+            for d in range(D):
+                vel[d].append(arrays[d][0].astype(np.int32))
+            div.append(arrays[D][0].astype(np.int32))
+            if ve:
+                cells.append(arrays[D + 1][0].astype(np.int32))
+            tptr.append(q.tmpl_ptr[1:] + nnz)
+            tcol.append(q.tmpl_col)
+            tw.append(q.tmpl_w)
+            ntm += q.tmpl_ptr.size - 1
+            nnz += q.tmpl_col.size
+
+        p_ptr = [np.zeros(1, dtype=np.int64)]
+        p_col, p_val, p_brhs = [], [], []
+        pn = 0
+        for i, q in enumerate(progs):
+            p_ptr.append(q.p_ptr[1:] + pn)
+            p_col.append(q.p_col.astype(np.int64) + co[i])
+            p_val.append(q.p_val)
+            p_brhs.append(q.p_brhs)
+            pn += q.p_col.size
+        par = dict(p0.par)
+        return Program(
+            par=par, ncell=int(co[-1]), nfacet=[int(f[-1]) for f in fo] + [0] * (3 - D),
+            delta=np.array(dtab, dtype=np.float64).reshape(-1, D),
+            row_tmpl=np.concatenate(row_tmpl).astype(np.int32) if row_tmpl else np.zeros(0, np.int32),
+            row_base=np.concatenate(row_base).astype(np.int32) if row_base else np.zeros(0, np.int32),
+            row_rhs=np.concatenate(row_rhs).astype(np.float64) if row_rhs else np.zeros(0),
+            tmpl_ptr=np.concatenate(tptr),
+            tmpl_col=np.concatenate(tcol).astype(np.int32), tmpl_w=np.concatenate(tw),
+            vel_slots=[np.concatenate(v, axis=1) for v in vel],
+            vel_flags=[np.concatenate([q.vel_flags[d] for q in progs]) for d in range(D)],
+            vel_delta=[np.concatenate([delta_remap[i][q.vel_delta[d]] for i, q in enumerate(progs)]).astype(np.uint16)
+                       for d in range(D)],
+            div_slots=np.concatenate(div, axis=1),
+            cell_delta=np.concatenate([delta_remap[i][q.cell_delta] for i, q in enumerate(progs)]).astype(np.uint16),
+            p_ptr=np.concatenate(p_ptr), p_col=np.concatenate(p_col).astype(np.int32),
+            p_val=np.concatenate(p_val), p_brhs=np.concatenate(p_brhs),
+            pin_row=-1, pin_value=0.0,
+            cell_slots=np.concatenate(cells, axis=1) if ve else None,
+            cell_flags=np.concatenate([q.cell_flags for q in progs]) if ve else None,
+            inst_par=[dict(q.par) for q in progs],
+            cell_off=co.astype(np.int32), facet_off=[f.astype(np.int32) for f in fo],
+            inst_pin=np.array([(q.pin_row + int(co[i])) if q.pin_row >= 0 else -1 for i, q in enumerate(progs)],
+                              dtype=np.int32),
+            inst_pin_value=np.array([q.pin_value for q in progs], dtype=np.float64),
+        )
 
     # ------------------------------------------------------------------
     def save(self, path: str) -> None:

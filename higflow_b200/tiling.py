@@ -1,15 +1,21 @@
 """Step programs for large uniform meshes, tiled from a small recorded seed.
 
 On a uniform single-level box mesh every stencil HigTree builds for an element
-depends only on where the element sits relative to the walls: once an element is
-``R`` or more cells from a wall along an axis, moving it along that axis just
+depends on where the element sits relative to the walls: once an element is
+``R`` or more cells from a wall along an axis, moving it along that axis
 translates its stencil.  A seed program recorded by the flattener on a mesh of
-``2R+2`` cells per axis therefore contains every distinct stencil class, and a
-program for any larger mesh of the same box, boundary conditions and cell
-aspect ratio follows by mapping each element to its class in the seed and
-translating ids.  Translated general rows reuse the seed row as a template with
-a base offset (row-major ids make a translation a constant index shift), so
-interior interpolation weights are stored once however large the mesh is.
+``2R+2`` cells per axis contains every stencil class, and a program for a
+larger mesh of the same box, boundary conditions and cell aspect ratio follows
+by mapping each element to its class in the seed and translating ids.
+Translated general rows reuse the seed row as a template with a base offset
+(row-major ids make a translation a constant index shift).
+
+One caveat is inherited from HigTree itself: its interpolation stencils keep
+the nearest candidates by distances computed in absolute coordinates, so where
+several candidates are equidistant the reference's choice can differ with the
+element's position.  A tiled program uses the seed's choice for every element
+of a class, which gives the same discretisation up to that tie-break.  Programs
+that must match the reference bit for bit are recorded, not tiled.
 
 The id layouts are HigTree's for a single uniform tree: cells row-major with
 the last axis fastest (higtree/src/higtree.c:23-37); interior facets normal to
@@ -58,93 +64,6 @@ def _grid_ext(n: Sequence[int], g: int) -> List[int]:
     return e
 
 
-def _vel_slot_grid(D: int, d: int, s: int) -> int:
-    if s == hp.V_FU:
-        return d
-    if s <= hp.V_FR:
-        return -1
-    if s < hp.v_nslot(D, False):
-        d2, k = divmod(s - hp.V_BLK0, hp.V_NB)
-        return d2 if (k < 4 or k >= 8) else d
-    return -1
-
-
-def _cell_slot_grid(D: int, s: int) -> int:
-    if s == hp.C_SELF:
-        return -1
-    if s < hp.C_BLK0 + hp.C_NB * D:
-        dim, k = divmod(s - hp.C_BLK0, hp.C_NB)
-        return dim if k < 2 else -1
-    pair = (s - hp.C_BLK0 - hp.C_NB * D) // hp.C_NQ
-    return pair // (D - 1)
-
-
-class _Rows:
-    """Collects (seed row, grid, offset) references and emits target rows."""
-
-    def __init__(self, seed: hp.Program, sn, tn):
-        self.seed, self.sn, self.tn = seed, sn, tn
-        self.keys = []      # arrays (M, 2 + D): seed row, grid, offset...
-        self.where = []     # (array to write, flat positions)
-
-    def add(self, rows: np.ndarray, grid: int, off: np.ndarray, out: np.ndarray, pos: np.ndarray):
-        if rows.size == 0:
-            return
-        k = np.empty((rows.size, 2 + off.shape[1]), dtype=np.int64)
-        k[:, 0] = rows
-        k[:, 1] = grid
-        k[:, 2:] = off
-        self.keys.append(k)
-        self.where.append((out, pos))
-
-    def emit(self, prog_kw: dict):
-        seed, D = self.seed, self.seed.dim
-        if not self.keys:
-            prog_kw.update(row_tmpl=np.zeros(0, np.int32), row_base=np.zeros(0, np.int32),
-                           row_rhs=np.zeros(0), tmpl_ptr=np.zeros(1, np.int64),
-                           tmpl_col=np.zeros(0, np.int32), tmpl_w=np.zeros(0))
-            return
-        K = np.concatenate(self.keys)
-        # one int64 key per reference: ((row * 4 + grid + 1) * cells + linear offset);
-        # offsets are non-negative and smaller than the target extent on every axis
-        P = int(np.prod(self.tn))
-        key = (K[:, 0] * 4 + (K[:, 1] + 1)) * P + (K[:, 2:] * _strides(self.tn)).sum(axis=1)
-        ukey, first, inv = np.unique(key, return_index=True, return_inverse=True)
-        uniq = K[first]
-        inv = inv.reshape(-1)
-        # write the new codes back
-        start = 0
-        for (out, pos), k in zip(self.where, self.keys):
-            out.reshape(-1)[pos] = -(inv[start:start + len(k)] + 1)
-            start += len(k)
-        # one template per distinct (seed row, grid)
-        tkeys, tinv = np.unique(uniq[:, :2], axis=0, return_inverse=True)
-        tinv = tinv.reshape(-1)
-        tptr = [0]
-        tcol, tw = [], []
-        for sr, g in tkeys:
-            st = seed.row_tmpl[sr]
-            a, b = seed.tmpl_ptr[st], seed.tmpl_ptr[st + 1]
-            sc = seed.tmpl_col[a:b].astype(np.int64) + seed.row_base[sr]
-            se, te = _grid_ext(self.sn, int(g)), _grid_ext(self.tn, int(g))
-            tcol.append(_lin(_coords(sc, se), te))
-            tw.append(seed.tmpl_w[a:b])
-            tptr.append(tptr[-1] + (b - a))
-        base = np.empty(len(uniq), dtype=np.int64)
-        for g in np.unique(uniq[:, 1]):
-            m = uniq[:, 1] == g
-            base[m] = (uniq[m, 2:] * _strides(_grid_ext(self.tn, int(g)))).sum(axis=1)
-        if base.max(initial=0) > np.iinfo(np.int32).max:
-            raise ValueError("mesh too large for int32 row bases")
-        prog_kw.update(
-            row_tmpl=tinv.astype(np.int32), row_base=base.astype(np.int32),
-            row_rhs=seed.row_rhs[uniq[:, 0]].astype(np.float64),
-            tmpl_ptr=np.array(tptr, dtype=np.int64),
-            tmpl_col=(np.concatenate(tcol) if tcol else np.zeros(0)).astype(np.int32),
-            tmpl_w=(np.concatenate(tw) if tw else np.zeros(0)).astype(np.float64),
-        )
-
-
 def _classify(tc: np.ndarray, te: Sequence[int], se: Sequence[int], R: int):
     """Seed element coords and translation for target element coords tc."""
     te = np.asarray(te)
@@ -155,17 +74,96 @@ def _classify(tc: np.ndarray, te: Sequence[int], se: Sequence[int], R: int):
     return sc, tc - sc
 
 
-def _remap_codes(codes, grid, off, sn, tn, rows: _Rows, out, pos_base):
-    """Direct codes translate; general codes become (row, grid, offset) refs."""
-    direct = codes >= 0
-    res = out.reshape(-1)
-    if direct.any():
-        se, te = _grid_ext(sn, grid), _grid_ext(tn, grid)
-        c = _coords(codes[direct], se) + off[direct]
-        res[pos_base[direct]] = _lin(c, te)
-    gen = ~direct
-    if gen.any():
-        rows.add(-codes[gen].astype(np.int64) - 1, grid, off[gen], out, pos_base[gen])
+class _Remap:
+    """Seed id -> target id for translation zero, per field grid, and the
+    linear shift of each element's translation, per grid."""
+
+    def __init__(self, D, sn, tn):
+        self.D, self.sn, self.tn = D, sn, tn
+        self.map = {}
+        self.strides = {}
+        for g in range(-1, D):
+            se, te = _grid_ext(sn, g), _grid_ext(tn, g)
+            self.map[g] = _lin(_coords(np.arange(int(np.prod(se))), se), te)
+            self.strides[g] = _strides(te)
+
+    def shifts(self, off: np.ndarray):
+        return {g: off @ self.strides[g] for g in range(-1, self.D)}
+
+
+class _Rows:
+    """General-row references: (seed row, grid, linear shift) -> target rows."""
+
+    def __init__(self, seed: hp.Program, remap: _Remap):
+        self.seed, self.remap = seed, remap
+        self.rows, self.grids, self.shifts = [], [], []
+        self.count = 0
+
+    def add(self, seed_rows: np.ndarray, grid: int, shift: np.ndarray) -> np.ndarray:
+        """Register references; returns their new (negative) codes."""
+        n = seed_rows.size
+        self.rows.append(seed_rows)
+        self.grids.append(np.full(n, grid + 1, dtype=np.int64))
+        self.shifts.append(shift)
+        codes = -(np.arange(self.count, self.count + n, dtype=np.int64) + 1)
+        self.count += n
+        return codes
+
+    def emit(self, kw: dict):
+        seed = self.seed
+        if not self.rows:
+            kw.update(row_tmpl=np.zeros(0, np.int32), row_base=np.zeros(0, np.int32), row_rhs=np.zeros(0),
+                      tmpl_ptr=np.zeros(1, np.int64), tmpl_col=np.zeros(0, np.int32), tmpl_w=np.zeros(0))
+            return
+        r = np.concatenate(self.rows)
+        g1 = np.concatenate(self.grids)
+        base = np.concatenate(self.shifts)
+        # one template per distinct (seed row, grid); small key range -> table
+        tk = r * 4 + g1
+        present = np.zeros(int(tk.max()) + 1, dtype=bool)
+        present[tk] = True
+        keys = np.nonzero(present)[0]
+        table = np.full(present.size, -1, dtype=np.int64)
+        table[keys] = np.arange(keys.size)
+        tptr = [0]
+        tcol, tw = [], []
+        for key in keys.tolist():
+            sr, g = key // 4, key % 4 - 1
+            st = seed.row_tmpl[sr]
+            a, b = seed.tmpl_ptr[st], seed.tmpl_ptr[st + 1]
+            sc = seed.tmpl_col[a:b].astype(np.int64) + seed.row_base[sr]
+            tcol.append(self.remap.map[g][sc])
+            tw.append(seed.tmpl_w[a:b])
+            tptr.append(tptr[-1] + (b - a))
+        if base.max(initial=0) > np.iinfo(np.int32).max:
+            raise ValueError("mesh too large for int32 row bases")
+        kw.update(
+            row_tmpl=table[tk].astype(np.int32), row_base=base.astype(np.int32),
+            row_rhs=seed.row_rhs[r].astype(np.float64),
+            tmpl_ptr=np.array(tptr, dtype=np.int64),
+            tmpl_col=np.concatenate(tcol).astype(np.int32), tmpl_w=np.concatenate(tw).astype(np.float64),
+        )
+
+
+def _remap_slots(seed_slots, sel, grid_of_slot, shifts, remap: _Remap, rows: _Rows, skip=()):
+    """Translate a (nslot, seed elements) slot table to target elements."""
+    ns = seed_slots.shape[0]
+    ne = sel.size
+    out = np.empty((ns, ne), dtype=np.int32)
+    for s in range(ns):
+        if s in skip:
+            out[s] = 0
+            continue
+        g = grid_of_slot(s)
+        codes = seed_slots[s][sel].astype(np.int64)
+        direct = codes >= 0
+        res = np.empty(ne, dtype=np.int64)
+        res[direct] = remap.map[g][codes[direct]] + shifts[g][direct]
+        gen = ~direct
+        if gen.any():
+            res[gen] = rows.add(-codes[gen] - 1, g, shifts[g][gen])
+        out[s] = res
+    return out
 
 
 def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], lengths: Sequence[float],
@@ -184,7 +182,8 @@ def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], leng
         raise ValueError("cell aspect ratio differs from the seed's")
     scale = float(ratio[0]) ** 2
     ve = seed.viscoelastic and not newtonian
-    rows = _Rows(seed, sn, tn)
+    remap = _Remap(D, sn, tn)
+    rows = _Rows(seed, remap)
     kw = {}
 
     # velocity stage
@@ -196,15 +195,9 @@ def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], leng
         tc = _coords(np.arange(nf), te)
         sc, off = _classify(tc, te, se, R)
         sel = _lin(sc, se)
-        out = np.empty((nsv, nf), dtype=np.int32)
-        for s in range(nsv):
-            b0 = hp.V_BLK0 + hp.V_NB * d
-            if b0 <= s < b0 + 4:
-                out[s] = 0          # the tangential-average slots are unused for d2 == d
-                continue
-            codes = seed.vel_slots[d][s][sel]
-            _remap_codes(codes, _vel_slot_grid(D, d, s), off, sn, tn, rows, out, s * nf + np.arange(nf))
-        vel_slots.append(out)
+        b0 = hp.V_BLK0 + hp.V_NB * d
+        vel_slots.append(_remap_slots(seed.vel_slots[d][:nsv], sel, lambda s, d=d: hp.vel_slot_grid(D, d, s),
+                                      remap.shifts(off), remap, rows, skip=set(range(b0, b0 + 4))))
         vel_flags.append(seed.vel_flags[d][sel].copy())
         vel_delta.append(np.zeros(nf, dtype=np.uint16))
 
@@ -213,16 +206,11 @@ def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], leng
     tc = _coords(np.arange(nc), tn)
     sc, off = _classify(tc, tn, sn, R)
     sel = _lin(sc, sn)
-    div = np.empty((2 * D, nc), dtype=np.int32)
-    for s in range(2 * D):
-        _remap_codes(seed.div_slots[s][sel], s // 2, off, sn, tn, rows, div, s * nc + np.arange(nc))
+    sh = remap.shifts(off)
+    div = _remap_slots(seed.div_slots, sel, lambda s: s // 2, sh, remap, rows)
     cell_slots = cell_flags = None
     if ve:
-        ncs = hp.c_nslot(D)
-        cell_slots = np.empty((ncs, nc), dtype=np.int32)
-        for s in range(ncs):
-            _remap_codes(seed.cell_slots[s][sel], _cell_slot_grid(D, s), off, sn, tn, rows, cell_slots,
-                         s * nc + np.arange(nc))
+        cell_slots = _remap_slots(seed.cell_slots, sel, lambda s: hp.cell_slot_grid(D, s), sh, remap, rows)
         cell_flags = seed.cell_flags[sel].copy()
     rows.emit(kw)
 
@@ -241,8 +229,7 @@ def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], leng
     psc, poff = sc.copy(), off.copy()
     hit = sel == seed.pin_row
     if hit.any():
-        mid = (psc[hit] == R)
-        psc[hit] = np.where(mid, R + 1, psc[hit])
+        psc[hit] = np.where(psc[hit] == R, R + 1, psc[hit])
         poff[hit] = tc[hit] - psc[hit]
     psel = _lin(psc, sn)
     if np.any(psel == seed.pin_row):
@@ -255,8 +242,8 @@ def tile(seed: hp.Program, seed_n: Sequence[int], R: int, n: Sequence[int], leng
     rep = np.repeat(np.arange(nc), lens)
     first = np.repeat(seed.p_ptr[:-1][psel], lens)
     k = first + (np.arange(p_ptr[-1]) - np.repeat(p_ptr[:-1], lens))
-    scol = seed.p_col[k].astype(np.int64)
-    p_col = _lin(_coords(scol, sn) + poff[rep], tn).astype(np.int32)
+    pshift = poff @ remap.strides[-1]
+    p_col = (remap.map[-1][seed.p_col[k].astype(np.int64)] + pshift[rep]).astype(np.int32)
     p_val = seed.p_val[k] * scale
     p_brhs = seed.p_brhs[psel] * scale
 
@@ -280,10 +267,16 @@ def load_seed(name: str):
     return prog, [int(x) for x in z["n"]], int(z["R"]), [float(x) for x in z["lengths"]]
 
 
+_seed_cache = {}
+
+
 def cavity(dim: int, n: int, viscoelastic: bool = False, **par) -> hp.Program:
     """Lid-driven cavity program on the unit square/cube with n cells per axis
     (lid u_0 = 1 on the top face, no-slip walls, pinned Neumann pressure)."""
-    seed, sn, R, sl = load_seed(f"cavity{dim}d")
+    name = f"cavity{dim}d"
+    if name not in _seed_cache:
+        _seed_cache[name] = load_seed(name)
+    seed, sn, R, sl = _seed_cache[name]
     prog = tile(seed, sn, R, [n] * dim, [1.0] * dim, sl, newtonian=not viscoelastic)
     for k, v in par.items():
         if k not in prog.par:

@@ -1,0 +1,106 @@
+"""Synthetic case populations for the batched and served benchmark configurations.
+
+Seeded draws in a fixed order (numpy.random.default_rng(seed)); every case is a
+lid-driven cavity on the unit square, its program tiled from the recorded seed
+(higflow_b200/tiling.py).  The explicit time step of each case is a fixed
+fraction of its explicit stability bound, recorded with the case.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Dict, List
+
+import numpy as np
+
+from . import program as hp
+from . import tiling
+
+
+@dataclass
+class CaseDraw:
+    n: int                 # cells per side
+    model: int             # hp.OLDROYD_B / hp.GIESEKUS (viscoelastic) or -1 (Newtonian)
+    De: float              # Weissenberg number (De in HigFlow's parameters)
+    alpha: float           # Giesekus mobility
+    beta: float
+    Re: float
+    dt: float
+    steps: int
+
+    @property
+    def cells(self) -> int:
+        return self.n * self.n
+
+
+def explicit_dt(n: int, Re: float, frac: float = 0.2) -> float:
+    """frac times the explicit bound min(Re h^2 / 4, h) of a unit-lid cavity."""
+    h = 1.0 / n
+    return frac * min(Re * h * h / 4.0, h)
+
+
+def batched_giesekus(count: int = 256, seed: int = 0) -> List[CaseDraw]:
+    """256 cavities, side N log-uniform in [32, 256], Wi uniform [0.1, 2.0],
+    Giesekus alpha uniform [0, 0.5], beta 0.1, Re 1, 2000 steps each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(32), math.log(256)))))
+        wi = float(rng.uniform(0.1, 2.0))
+        alpha = float(rng.uniform(0.0, 0.5))
+        out.append(CaseDraw(n=n, model=hp.GIESEKUS, De=wi, alpha=alpha, beta=0.1, Re=1.0,
+                            dt=explicit_dt(n, 1.0), steps=2000))
+    return out
+
+
+def served_stream(seed: int = 0, rate: float = 50.0, window_s: float = 60.0):
+    """Poisson arrivals at ``rate`` per second over ``window_s``: 40% Newtonian
+    cavities, 40% Oldroyd-B cavities (Wi uniform [0.1, 1.5]), 20% Giesekus
+    (alpha uniform [0, 0.5], Wi uniform [0.1, 1.5]); side N log-uniform in
+    [64, 512]; 500-5000 steps.  Inter-arrival times are drawn first."""
+    rng = np.random.default_rng(seed)
+    t, times = 0.0, []
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > window_s:
+            break
+        times.append(t)
+    cases = []
+    for _ in times:
+        kind = float(rng.uniform())
+        n = int(round(math.exp(rng.uniform(math.log(64), math.log(512)))))
+        steps = int(rng.integers(500, 5001))
+        if kind < 0.4:
+            cases.append(CaseDraw(n=n, model=-1, De=0.0, alpha=0.0, beta=1.0, Re=100.0,
+                                  dt=explicit_dt(n, 100.0), steps=steps))
+        elif kind < 0.8:
+            cases.append(CaseDraw(n=n, model=hp.OLDROYD_B, De=float(rng.uniform(0.1, 1.5)), alpha=0.0,
+                                  beta=0.1, Re=1.0, dt=explicit_dt(n, 1.0), steps=steps))
+        else:
+            cases.append(CaseDraw(n=n, model=hp.GIESEKUS, De=float(rng.uniform(0.1, 1.5)),
+                                  alpha=float(rng.uniform(0.0, 0.5)), beta=0.1, Re=1.0,
+                                  dt=explicit_dt(n, 1.0), steps=steps))
+    return times, cases
+
+
+_cache: Dict[tuple, hp.Program] = {}
+
+
+def program(c: CaseDraw) -> hp.Program:
+    """The tiled cavity program of one draw, with its parameters."""
+    ve = c.model >= 0
+    key = (c.n, ve)
+    if key not in _cache:
+        _cache[key] = tiling.cavity(2, c.n, viscoelastic=ve)
+    base = _cache[key]
+    prog = hp.Program(**{k: v for k, v in base.__dict__.items() if k != "_keep"})
+    prog.par = dict(base.par)
+    prog.par.update(Re=c.Re, dt=c.dt)
+    if ve:
+        prog.par.update(ve_model=c.model, De=c.De, alpha=c.alpha, beta=c.beta, kernel=hp.KERNEL_LOG,
+                        kernel_tol=1e-2, ve_convecdiscrtype=hp.CELL_CUBISTA)
+    return prog
+
+
+def batch(draws: List[CaseDraw]) -> hp.Program:
+    return hp.Program.concatenate([program(c) for c in draws])

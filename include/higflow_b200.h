@@ -66,6 +66,13 @@ enum {
                            outer residual and time accumulation              */
 };
 
+/* Poisson preconditioner (CG path) */
+enum {
+    HF_PRECOND_AUTO = 0,    /* smoothed-aggregation AMG V-cycle                 */
+    HF_PRECOND_JACOBI = 1,  /* diagonal scaling                                  */
+    HF_PRECOND_AMG = 2
+};
+
 /* Poisson solver choice */
 enum {
     HF_POISSON_AUTO = 0,    /* CG when the reduced matrix is symmetric, else BiCGStab */
@@ -222,6 +229,19 @@ typedef struct hf_program {
     int32_t cell_nslot;            /* HF_C_NSLOT(dim) or 0                     */
     const int32_t  *cell_slots;    /* cell_nslot * ncell                       */
     const uint32_t *cell_flags;    /* ncell                                    */
+
+    /* Batches.  ninst > 0 concatenates ninst independent cases of the same
+     * dim and flow type: instance i owns cells [cell_off[i], cell_off[i+1])
+     * and facets [facet_off[d][i], facet_off[d][i+1]); every slot code, row
+     * base and Poisson column is already a global index; each instance has its
+     * own parameters and pressure pin.  ninst == 0 is one case described by
+     * par, pin_row and pin_value. */
+    int32_t ninst;
+    const hf_params *inst_par;     /* ninst                                    */
+    const int32_t *cell_off;       /* ninst + 1                                */
+    const int32_t *facet_off[3];   /* ninst + 1 per direction                  */
+    const int32_t *inst_pin;       /* ninst: pinned cell (global id) or -1     */
+    const double  *inst_pin_value; /* ninst                                    */
 } hf_program;
 
 /* ------------------------------------------------------------------ */
@@ -236,6 +256,7 @@ typedef struct hf_options {
     double  poisson_atol;     /* absolute residual target (reference: 1e-10)  */
     int32_t poisson_maxit;    /* iteration cap; 0 = 20000                      */
     int32_t device;           /* CUDA device ordinal                          */
+    int32_t precond;          /* HF_PRECOND_*                                 */
 } hf_options;
 
 typedef struct hf_stats {
@@ -259,6 +280,19 @@ int  hf_case_step(hf_case *c, int32_t nsteps);
 int  hf_case_stats(hf_case *c, hf_stats *out);
 int  hf_case_synchronize(hf_case *c);
 void hf_case_destroy(hf_case *c);
+
+/* Poisson solver of a case: method (HF_PRECOND_AMG / HF_PRECOND_JACOBI for CG,
+ * -1 for BiCGStab), number of levels (1 without AMG) and, per level up to
+ * max_levels, rows and non-zeros of A, P and R (the coarsest level is dense:
+ * nnz_a = rows^2, no P, R). */
+int  hf_case_solver_info(hf_case *c, int32_t *method, int32_t *nlev, int64_t *rows, int64_t *nnz_a,
+                         int64_t *nnz_p, int64_t *nnz_r, int32_t max_levels);
+
+/* Batches: number of instances, and the last step's Poisson result of one
+ * instance (iterations, refinement sweeps, status, relative residual). */
+int  hf_case_instances(hf_case *c, int32_t *ninst);
+int  hf_case_instance_result(hf_case *c, int32_t inst, int32_t *iters, int32_t *outer, int32_t *status,
+                             double *residual);
 
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);

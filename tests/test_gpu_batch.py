@@ -1,0 +1,76 @@
+"""Batched cases on one GPU: each instance's result is the same alone and in a
+batch, and the mixed-precision form agrees with the plain FP64 form.
+
+Tolerances: plain FP64 alone vs in a batch 1e-10 relative L2 (both solve each
+instance to its own 1e-13 Poisson residual); mixed vs plain 1e-6 relative L2
+(the FP32 inner solve is refined in FP64 to the same residual test).
+"""
+import numpy as np
+import pytest
+
+from higflow_b200 import engine
+from higflow_b200 import program as hp
+from tests.helpers import compare, field_keys, load_golden, load_init
+
+pytestmark = pytest.mark.gpu
+
+VE_NAMES = ["ve2d_oldroyd_log", "ve2d_giesekus_log", "ve2d_lptt_sqrt", "ve2d_oldroyd_central"]
+NEWT_NAMES = ["cav2d_cubista", "cav2d_quick", "cav2d_central", "chan2d_cubista", "cav2d_lid"]
+
+
+def _run_alone(name, steps, **kw):
+    prog, data = load_golden(name)
+    case = engine.Case(prog, engine.options(rtol=1e-13, atol=1e-300, **kw))
+    load_init(case, prog, data)
+    case.step(steps)
+    out = {k: case.get(fid, comp) for k, fid, comp in field_keys(prog)}
+    case.close()
+    return out
+
+
+def _keys(prog):
+    return [k for k, _, _ in field_keys(prog) if k != "dp"]
+
+
+@pytest.mark.parametrize("names", [VE_NAMES, NEWT_NAMES])
+def test_instances_same_alone_and_in_batch(names):
+    steps = 3
+    progs, datas = zip(*[load_golden(n) for n in names])
+    batch = hp.Program.concatenate(progs)
+    case = engine.Case(batch, engine.options(rtol=1e-13, atol=1e-300))
+    assert case.instances() == len(names)
+    # initial fields, instance by instance, in the concatenated arrays
+    for key, fid, comp in field_keys(progs[0]):
+        whole = np.concatenate([d["init_" + key] for d in datas])
+        case.set(fid, comp, whole)
+    case.step(steps)
+    for i, (name, prog) in enumerate(zip(names, progs)):
+        alone = _run_alone(name, steps)
+        got = {k: case.get_instance(fid, comp, i) for k, fid, comp in field_keys(prog)}
+        err = compare(got, alone, _keys(prog))
+        assert max(err.values()) < 1e-10, (name, err)
+        # CG accepts a breakdown once ||r|| <= 100 rtol ||b|| (the recurrence has
+        # lost its last digits there); that is the bound on the reported residual
+        it, outer, status, res = case.instance_result(i)
+        assert status == 0 and res < 1e-11
+    case.close()
+
+
+@pytest.mark.parametrize("name", ["cav2d_cubista", "ve2d_oldroyd_log", "cav3d_cubista"])
+def test_mixed_precision_matches_plain(name):
+    prog, data = load_golden(name)
+    steps = int(data["steps"])
+    plain = _run_alone(name, steps)
+    mixed = _run_alone(name, steps, precision=hp.PREC_MIXED)
+    err = compare(mixed, plain, _keys(prog))
+    assert max(err.values()) < 1e-6, err
+
+
+def test_mixed_precision_reaches_the_same_residual():
+    prog, data = load_golden("cav2d_lid")
+    case = engine.Case(prog, engine.options(rtol=1e-10, atol=1e-300, precision=hp.PREC_MIXED))
+    load_init(case, prog, data)
+    case.step(5)
+    it, outer, status, res = case.instance_result(0)
+    assert status == 0 and res <= 1e-10 and outer >= 1
+    case.close()

@@ -20,7 +20,7 @@ TOL = 1e-10
 
 
 def _opts(**kw):
-    kw.setdefault("rtol", 1e-14)
+    kw.setdefault("rtol", 1e-13)
     kw.setdefault("atol", 1e-300)
     return engine.options(**kw)
 
@@ -73,6 +73,34 @@ def test_velocity_stage_bit_exact(name):
         b = st.get(hp.FIELD_USTAR, d)
         assert np.array_equal(a, b), (d, np.abs(a - b).max())
     case.close()
+
+
+@pytest.mark.parametrize("name", ["cav2d_cubista", "cav3d_cubista", "ve2d_oldroyd_log"])
+def test_amg_and_jacobi_preconditioners_agree(name):
+    prog, data = load_golden(name)
+    out = []
+    for pc in (hp.PRECOND_AMG, hp.PRECOND_JACOBI):
+        case = engine.Case(prog, _opts(precond=pc))
+        load_init(case, prog, data)
+        case.step(int(data["steps"]))
+        out.append(case.get(hp.FIELD_P))
+        case.close()
+    assert np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[0]) < 1e-10
+
+
+def test_amg_iteration_count_is_small():
+    """On a 256x256 cavity the AMG-preconditioned CG converges in far fewer
+    iterations than diagonal scaling."""
+    from higflow_b200 import tiling
+    prog = tiling.cavity(2, 256)
+    iters = {}
+    for pc in (hp.PRECOND_AMG, hp.PRECOND_JACOBI):
+        case = engine.Case(prog, engine.options(precond=pc))
+        u = np.zeros(prog.nfacet[0])
+        case.step(2)
+        iters[pc] = case.stats().last_iters
+        case.close()
+    assert iters[hp.PRECOND_AMG] * 10 < iters[hp.PRECOND_JACOBI], iters
 
 
 def test_bicgstab_path_matches_cg():
