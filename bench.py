@@ -38,7 +38,7 @@ WORKLOADS = {
         name="batched 2D Giesekus lid-driven cavities: 256 instances, side N log-uniform in [32,256] "
              "(seed 0), Wi uniform [0.1,2.0], alpha uniform [0,0.5], beta 0.1, Re 1, log-conformation "
              "kernel from identity, explicit Euler at 0.2x the explicit bound, CUBISTA, AMG-CG Poisson "
-             "to 1e-10; one batch program, one persistent Poisson launch per step",
+             "to 1e-10; one batch program, one CUDA graph launch per step",
         batch="c4", precision="mixed", dim=2,
     ),
     "c1": dict(
@@ -148,29 +148,31 @@ def _row_bytes(prog, codes_list):
     return r.size * 16 + tm.size * 8 + nnz * 12
 
 
-def amg_iter_bytes(sinfo):
-    """(bytes, launches) of one preconditioned CG iteration of the multi-kernel
-    solver: the two CG launches on the finest operator plus one V-cycle."""
+def cg_iter_bytes(sinfo, mixed):
+    """Compulsory bytes of one preconditioned CG iteration over every instance of
+    the batch (each array a kernel reads or writes counted once per kernel):
+    direction + spmv and update on the FP64 finest operator, then the V-cycle
+    (hf_pcg.cuh) in FP32 (mixed) or FP64, or the Jacobi z."""
     lv = sinfo["levels"]
     n0, nnz0 = lv[0][0], lv[0][1]
-    b = (n0 * 4 + nnz0 * 12 + n0 * 8 * 4) + (n0 * 8 * 6)
-    launches = 2
-    if sinfo["method"] == "amg-cg":
-        for l in range(len(lv) - 1):
-            n, na, npp, nr = lv[l]
-            nn = lv[l + 1][0]
-            b += n * 8 * 3
-            b += n * 4 + na * 12 + n * 8 * 3
-            b += nn * 4 + nr * 12 + n * 8 + nn * 8
-            b += n * 4 + npp * 12 + nn * 8 + n * 16
-            b += n * 4 + na * 12 + n * 8 * 4
-            launches += 5
-        cn = lv[-1][0]
-        b += cn * cn * 8 + cn * 16
-        launches += 1
-    else:
-        b += n0 * 8 * 3
-    return b, launches
+    b = n0 * (4 + 8 * 4) + nnz0 * 12          # dir: ptr, col+val, z, p_old -> p, q
+    b += n0 * 8 * 6                            # update: p, q, r, x -> x, r
+    if sinfo["method"] != "amg-cg":
+        return b + n0 * 8 * 3                  # z = D^-1 r: r, dinv -> z
+    s = 4 if mixed else 8
+    nl = len(lv) - 1                           # concatenated levels; the last entry is the dense solves
+    for l in range(nl - 1):
+        n, na, npp, nr = lv[l]
+        nn = lv[l + 1][0]
+        b += n * 4 + na * (4 + s) + n * (s + (8 if l == 0 else s)) + n * s * 2      # down
+        b += nn * 4 + nr * (4 + s) + n * s + nn * s                                 # restrict
+        b += n * 4 + npp * (4 + s) + nn * s + n * s * 2                             # prolong
+        if l > 0:
+            b += n * 4 + na * (4 + s) + n * s * 4                                   # post
+    crows, cdense = lv[-1][0], lv[-1][1]
+    b += cdense * s + crows * s * 2                                                 # dense solves
+    b += n0 * (8 + 4 + 2 * s + 8) + nnz0 * (4 + s)                                  # finest post -> z
+    return b
 
 
 def phase_bytes(prog, sinfo=None):
@@ -190,9 +192,6 @@ def phase_bytes(prog, sinfo=None):
         # slots, flags, delta, instance; u faces; Du, S, K read; Du, S, Knew written
         b["ve_cell"] = cs.size * 4 + nc * (4 + 2 + 4) + nf * 8 + nc * 8 * D * D * 6 + _row_bytes(prog, [cs.ravel()])
     b["final"] = sum(s[1:3].size for s in prog.vel_slots) * 4 + nf * (8 * 2 + 2 + 4) + nc * 8 * 3
-    if sinfo is not None and sinfo["method"] in ("amg-cg", "jacobi-cg"):
-        ib, il = amg_iter_bytes(sinfo)
-        b["poisson_iter"] = ib / il
     return b
 
 
@@ -227,9 +226,10 @@ def timed_steps(case, steps, device, world, flush, stream, profile=True):
         with torch.cuda.stream(stream):
             flush.fill_(float(k))
             evs[k][0].record(stream)
-        case.step(1)
+        case.step(1, sync=False)       # one graph launch, queued behind the start event
         with torch.cuda.stream(stream):
             evs[k][1].record(stream)
+        case.synchronize()             # outside the events: reads the phase events, checks the solve
     case.synchronize()
     torch.cuda.synchronize(device)
     t_wall = time.perf_counter() - t_wall
@@ -268,9 +268,11 @@ def run_b200(args, rank, world, device):
         case.step(1)
     case.synchronize()
     st0 = case.stats()
+    it0 = case.instance_iters()
     with ClockSampler(device) as clk:
         dev_ms, t_wall = timed_steps(case, args.steps, device, world, flush, stream)
     st = case.stats()
+    dit = case.instance_iters() - it0
     launches = st.kernel_launches - st0.kernel_launches
     iters = st.total_iters - st0.total_iters
     phases = case.phase_times()
@@ -279,14 +281,20 @@ def run_b200(args, rank, world, device):
     cells = prog.ncell
     value = cells * args.steps * world / t_s
 
-    # roofline of the dominant phase (device time inside the timed region)
+    # roofline of the dominant phase (device time inside the timed region).
+    # Per phase: compulsory bytes of all its launches in the timed steps; the
+    # Poisson iterations weight each instance's rows by its own iteration count.
     sinfo = case.solver_info()
-    pb = phase_bytes(prog, sinfo)
+    pb = {p: v * phases[p][1] for p, v in phase_bytes(prog, sinfo).items() if p in phases}
+    if sinfo["method"] in ("amg-cg", "jacobi-cg"):
+        sizes = np.diff(prog.cell_off) if prog.ninst > 1 else np.array([prog.ncell])
+        equiv_iters = float((dit * sizes).sum()) / float(sizes.sum())
+        pb["poisson_iter"] = cg_iter_bytes(sinfo, mixed) * equiv_iters
     cand = [p for p in phases if phases[p][1] > 0 and p in pb]
     dom = max(cand, key=lambda p: phases[p][0])
     dom_ms, dom_launch = phases[dom]
     per_launch_s = dom_ms / 1e3 / dom_launch
-    achieved = pb[dom] / per_launch_s / 1e9
+    achieved = pb[dom] / (dom_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
     traffic = None
     tfile = os.path.join(REPO, "profiles", f"traffic_{args.workload}.json")
@@ -360,15 +368,18 @@ def run_b200(args, rank, world, device):
         "data": "synthetic",
         "config": {"workload": wl["name"], "instances": ninst, "cells": cells,
                    "facets": sum(prog.nfacet[:prog.dim]),
-                   "precision": "mixed (FP32 inner AMG-PCG in FP64 refinement; FP64 gathers, eigen, time update)"
-                   if mixed else "plain FP64",
+                   "precision": "mixed (FP32 AMG V-cycle preconditioner; FP64 CG recurrences, finest operator, "
+                                "gathers, eigen, time update)" if mixed else "plain FP64",
                    "poisson": f"{sinfo['method']}, rtol 1e-10 on ||b - A x|| per instance",
                    "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write, outside the step events)",
                    "parallelism": f"replicas x{world}",
                    "program": "tiled from recorded seeds" if (wl.get("tiled") or wl.get("batch")) else "recorded from the reference"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "bytes_per_launch": pb[dom], "launch_us": per_launch_s * 1e6, "peak_source": peak_kind},
+                     "bytes_per_launch": pb[dom] / dom_launch, "launch_us": per_launch_s * 1e6,
+                     "peak_source": peak_kind},
+        "phase_roofline": {p: {"GB/s": pb[p] / (phases[p][0] / 1e3) / 1e9, "launches": phases[p][1]}
+                           for p in cand},
         "e2e": e2e,
         "gpu_launches": int(launches),
         "poisson_iters_per_step": iters / args.steps,

@@ -33,11 +33,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "hf_amg.cuh"
@@ -576,308 +579,7 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
 // ---------------------------------------------------------------------------
 // Poisson: divergence rhs + first CG residual
 // ---------------------------------------------------------------------------
-struct CGVec {
-    double *x;    // solution (dp or p)
-    double *r, *z, *pa, *pb, *q;
-    double *partials;
-    Scal *sc;
-};
-
-template <int D>
-__global__ void __launch_bounds__(kBlock) k_cg_init(DevProg P, DevFields F, DevMat M, CGVec V, double rtol, double atol)
-{
-    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = P.ncell;
-    double part[3] = {0.0, 0.0, 0.0};  // r.z, r.r, b.b
-    if (cc < n) {
-        const double pinv = P.pin >= 0
-            ? (P.par.projtype == HF_INCREMENTAL ? P.pin_value - F.p[P.pin] : P.pin_value) : 0.0;
-        double borig;
-        if (cc == P.pin) {
-            borig = pinv;
-        } else {
-            const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
-            double sumdudx = 0.0;
-#pragma unroll
-            for (int dim = 0; dim < D; dim++) {
-                const double ustarl = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UL(dim) * n + cc), F.us[dim]);
-                const double ustarr = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UR(dim) * n + cc), F.us[dim]);
-                sumdudx += (ustarr - ustarl) / (2.0 * 0.5 * cd[dim]);
-            }
-            borig = sumdudx / P.par.dt + M.brhs[cc];
-        }
-        const double bred = cc == P.pin ? pinv : -(borig - M.apin[cc] * pinv);
-        double ax = 0.0;
-        for (int k = M.ptr[cc]; k < M.ptr[cc + 1]; k++) ax += M.val[k] * V.x[M.col[k]];
-        const double r = bred - ax;
-        const double z = M.dinv[cc] * r;
-        V.r[cc] = r;
-        V.z[cc] = z;
-        part[0] = r * z;
-        part[1] = r * r;
-        part[2] = borig * borig;
-    }
-    double tot[3];
-    if (grid_sum<3>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.rz = tot[0];
-        s.rr = tot[1];
-        s.bb = tot[2];
-        const double t = fmax(rtol * sqrt(tot[2]), atol);
-        s.tol2 = t * t;
-        s.beta = 0.0;
-        s.iters = 0;
-        s.status = 0;
-        s.done = !(tot[1] > s.tol2);
-        if (!finite(tot[0]) || !finite(tot[1]) || !finite(tot[2])) { s.status = HF_ERR_NAN; s.done = 1; }
-    }
-}
-
-// p_new = z + beta p_old ; q = M p_new ; alpha = rz / (p_new . q)
-__global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(DevMat M, CGVec V, const double *__restrict__ po, double *__restrict__ pn)
-{
-    if (V.sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const double beta = V.sc->beta;
-    const bool first = V.sc->iters == 0;
-    double part[1] = {0.0};
-    if (i < M.n) {
-        double q = 0.0;
-        if (first) {
-            for (int k = M.ptr[i]; k < M.ptr[i + 1]; k++) q += M.val[k] * V.z[M.col[k]];
-            pn[i] = V.z[i];
-        } else {
-            for (int k = M.ptr[i]; k < M.ptr[i + 1]; k++) {
-                const int j = M.col[k];
-                q += M.val[k] * (V.z[j] + beta * po[j]);
-            }
-            pn[i] = V.z[i] + beta * po[i];
-        }
-        V.q[i] = q;
-        part[0] = pn[i] * q;
-    }
-    double tot[1];
-    if (grid_sum<1>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.pq = tot[0];
-        if (!(tot[0] > 0.0) || !finite(tot[0])) {
-            // p.q <= 0: the recurrence has reached rounding level.  Accept when
-            // the residual is within 100x of the target, else report it.
-            s.status = !finite(tot[0]) ? HF_ERR_NAN : (s.rr <= 1e4 * s.tol2 ? 0 : HF_ERR_NOT_CONVERGED);
-            s.done = 1;
-        } else {
-            s.alpha = s.rz / tot[0];
-        }
-    }
-}
-
-// x += alpha p ; r -= alpha q ; z = D^-1 r ; beta = rz_new / rz
-__global__ void __launch_bounds__(kBlock) k_cg_update(DevMat M, CGVec V, const double *__restrict__ pn)
-{
-    if (V.sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const double alpha = V.sc->alpha;
-    double part[2] = {0.0, 0.0};
-    if (i < M.n) {
-        V.x[i] += alpha * pn[i];
-        const double r = V.r[i] - alpha * V.q[i];
-        const double z = M.dinv[i] * r;
-        V.r[i] = r;
-        V.z[i] = z;
-        part[0] = r * z;
-        part[1] = r * r;
-    }
-    double tot[2];
-    if (grid_sum<2>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.beta = tot[0] / s.rz;
-        s.rz = tot[0];
-        s.rr = tot[1];
-        s.iters += 1;
-        if (!finite(tot[0]) || !finite(tot[1])) { s.status = HF_ERR_NAN; s.done = 1; }
-        else if (!(tot[1] > s.tol2)) s.done = 1;
-        else if (s.iters >= s.maxit) { s.status = HF_ERR_NOT_CONVERGED; s.done = 1; }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// CG preconditioned by an AMG V-cycle (hf_amg.cuh): the residual update and the
-// preconditioner are separate launches; the last V-cycle kernel on the finest
-// level finishes r.z and the CG beta.
-// ---------------------------------------------------------------------------
-constexpr int kMaxLevels = 20;
-
-struct DevCSR {
-    int n;
-    const int32_t *ptr;
-    const int32_t *col;
-    const double *val;
-};
-
-struct DevLevel {
-    DevCSR A, P, R;
-    const double *dinv;
-    double *b, *x, *r, *out;
-};
-
-struct DevAMG {
-    int nlev;        // levels with a smoother; the coarsest has a dense inverse
-    DevLevel lev[kMaxLevels];
-    int cn;
-    const double *cinv;
-    double *cb, *cx;
-};
-
-constexpr double kSmoothW = 2.0 / 3.0;
-
-__device__ __forceinline__ double csr_row(const DevCSR &A, int i, const double *__restrict__ x)
-{
-    double s = 0.0;
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; k++) s += A.val[k] * x[A.col[k]];
-    return s;
-}
-
-__global__ void __launch_bounds__(kBlock) k_vc_smooth0(DevLevel L, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < L.A.n) L.x[i] = kSmoothW * L.dinv[i] * L.b[i];
-}
-
-__global__ void __launch_bounds__(kBlock) k_vc_residual(DevLevel L, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < L.A.n) L.r[i] = L.b[i] - csr_row(L.A, i, L.x);
-}
-
-// b_next = R r
-__global__ void __launch_bounds__(kBlock) k_vc_restrict(DevCSR R, const double *__restrict__ r, double *bn, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < R.n) bn[i] = csr_row(R, i, r);
-}
-
-// x = inv b on the coarsest level (dense, row-major)
-__global__ void __launch_bounds__(kBlock) k_vc_coarse(int n, const double *__restrict__ inv, const double *__restrict__ b,
-                                                    double *x, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double s = 0.0;
-    for (int k = 0; k < n; k++) s += inv[(size_t)i * n + k] * b[k];
-    x[i] = s;
-}
-
-// x += P e
-__global__ void __launch_bounds__(kBlock) k_vc_prolong(DevLevel L, const double *__restrict__ e, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < L.P.n) L.x[i] += csr_row(L.P, i, e);
-}
-
-// out = x + w D^-1 (b - A x)
-__global__ void __launch_bounds__(kBlock) k_vc_post(DevLevel L, const Scal *sc)
-{
-    if (sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < L.A.n) L.out[i] = L.x[i] + kSmoothW * L.dinv[i] * (L.b[i] - csr_row(L.A, i, L.x));
-}
-
-// finest-level post-smoothing writes z and finishes r.z -> beta
-__global__ void __launch_bounds__(kBlock) k_vc_post_fine(DevLevel L, CGVec V)
-{
-    if (V.sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double part[1] = {0.0};
-    if (i < L.A.n) {
-        const double z = L.x[i] + kSmoothW * L.dinv[i] * (L.b[i] - csr_row(L.A, i, L.x));
-        V.z[i] = z;
-        part[0] = L.b[i] * z;   // b of the finest level is the CG residual
-    }
-    double tot[1];
-    if (grid_sum<1>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        if (s.iters == 0) s.beta = 0.0;
-        else s.beta = tot[0] / s.rz;
-        s.rz = tot[0];
-        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
-    }
-}
-
-// first residual of the AMG-preconditioned solve (z comes from the V-cycle)
-template <int D>
-__global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, DevMat M, CGVec V, double rtol, double atol)
-{
-    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = P.ncell;
-    double part[2] = {0.0, 0.0};  // r.r, b.b
-    if (cc < n) {
-        const double pinv = P.pin >= 0
-            ? (P.par.projtype == HF_INCREMENTAL ? P.pin_value - F.p[P.pin] : P.pin_value) : 0.0;
-        double borig;
-        if (cc == P.pin) {
-            borig = pinv;
-        } else {
-            const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
-            double sumdudx = 0.0;
-#pragma unroll
-            for (int dim = 0; dim < D; dim++) {
-                const double ustarl = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UL(dim) * n + cc), F.us[dim]);
-                const double ustarr = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UR(dim) * n + cc), F.us[dim]);
-                sumdudx += (ustarr - ustarl) / (2.0 * 0.5 * cd[dim]);
-            }
-            borig = sumdudx / P.par.dt + M.brhs[cc];
-        }
-        const double bred = cc == P.pin ? pinv : -(borig - M.apin[cc] * pinv);
-        double ax = 0.0;
-        for (int k = M.ptr[cc]; k < M.ptr[cc + 1]; k++) ax += M.val[k] * V.x[M.col[k]];
-        const double r = bred - ax;
-        V.r[cc] = r;
-        part[0] = r * r;
-        part[1] = borig * borig;
-    }
-    double tot[2];
-    if (grid_sum<2>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.rr = tot[0];
-        s.bb = tot[1];
-        const double t = fmax(rtol * sqrt(tot[1]), atol);
-        s.tol2 = t * t;
-        s.beta = 0.0;
-        s.iters = 0;
-        s.status = 0;
-        s.done = !(tot[0] > s.tol2);
-        if (!finite(tot[0]) || !finite(tot[1])) { s.status = HF_ERR_NAN; s.done = 1; }
-    }
-}
-
-// x += alpha p ; r -= alpha q ; convergence on ||r||
-__global__ void __launch_bounds__(kBlock) k_pcg_update(DevMat M, CGVec V, const double *__restrict__ pn)
-{
-    if (V.sc->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const double alpha = V.sc->alpha;
-    double part[1] = {0.0};
-    if (i < M.n) {
-        V.x[i] += alpha * pn[i];
-        const double r = V.r[i] - alpha * V.q[i];
-        V.r[i] = r;
-        part[0] = r * r;
-    }
-    double tot[1];
-    if (grid_sum<1>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.rr = tot[0];
-        s.iters += 1;
-        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
-        else if (!(tot[0] > s.tol2)) s.done = 1;
-        else if (s.iters >= s.maxit) { s.status = HF_ERR_NOT_CONVERGED; s.done = 1; }
-    }
-}
+#include "hf_pcg.cuh"
 
 // ---------------------------------------------------------------------------
 // BiCGStab on the same operator (non-symmetric rows, e.g. AMR interfaces)
@@ -1055,7 +757,6 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
     }
 }
 
-#include "hf_batch.cuh"
 
 // ---------------------------------------------------------------------------
 // host side
@@ -1084,25 +785,34 @@ struct hf_case {
     DevProg P;
     DevFields F;
     DevMat M;
-    CGVec cg;
     BiVec bi;
     bool use_cg;
-    bool use_amg = false;
-    DevAMG amg{};
-    int amg_levels = 0;
-    // instances and the persistent per-instance Poisson solver (hf_batch.cuh)
+    // instances
     int ninst = 1;
     std::vector<int> coff;          // ninst + 1
     std::vector<int> foff[3];       // ninst + 1 per direction
-    bool persistent = false;
-    InstSolve *d_inst = nullptr;
-    ILevel<double> *d_l64 = nullptr;
-    ILevel<float> *d_l32 = nullptr;
-    int *d_res_i = nullptr;         // iters, outer, status per instance (3 * ninst)
-    double *d_res_d = nullptr;      // residual per instance
-    int *h_res_i = nullptr;         // pinned mirrors
-    double *h_res_d = nullptr;
-    int64_t batch_levels = 0;
+    // batched AMG-PCG (hf_pcg.cuh) and the graphs that run one step each
+    bool amg = false;
+    bool mixed = false;
+    PcgFine G{};
+    double *pa = nullptr, *pb = nullptr;   // CG directions (alternating)
+    int nlev = 1;                   // multigrid levels including the finest
+    VLev<double> L64[kMaxLevels] = {};
+    VLev<float> L32[kMaxLevels] = {};
+    CoarseInst<double> *c64 = nullptr;
+    CoarseInst<float> *c32 = nullptr;
+    std::vector<int64_t> lrows, lnnz_a, lnnz_p, lnnz_r;
+    int body_kernels = 0;           // kernels of one loop body (two iterations)
+    int fixed_kernels = 0;          // kernels of a step outside the loop
+    IScal *h_S = nullptr;           // pinned mirrors
+    Ctl *h_ctl = nullptr;
+    cudaStream_t body_stream = nullptr;
+    cudaGraph_t graph[2] = {};
+    cudaGraphExec_t exec[2] = {};
+    bool graph_profile = false;     // graphs were captured with phase events
+    bool phase_pending = false;     // a profiled step's events are not read yet
+    int64_t bodies0 = 0;            // loop bodies before that step
+    int parity = 0;
     std::vector<void *> owned;
     cudaStream_t stream = nullptr;
     Scal *h_scal = nullptr;   // pinned host mirror
@@ -1336,183 +1046,580 @@ std::vector<T> cast_vec(const std::vector<double> &v)
     return std::vector<T>(v.begin(), v.end());
 }
 
-// Per-instance AMG hierarchies and work vectors for the persistent solver.
-int build_batch_solver(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<int32_t> &mcol,
-                       const std::vector<double> &mval, const double *apin_dev, const double *brhs_dev,
-                       const std::vector<int> &pins, bool mixed)
+// Host copy of one concatenated level of the batched hierarchy.
+struct LevelHost {
+    int n = 0;
+    std::vector<int32_t> Ap, Ac, Pp, Pc, Rp, Rc;
+    std::vector<double> Av, dinv, Pv, Rv;
+    std::vector<Blk> sblk, ablk;
+};
+
+struct LevelOff {
+    size_t Ap, Ac, Av, dinv, Pp, Pc, Pv, Rp, Rc, Rv, b, x, r, out, sblk, ablk;
+};
+
+// Blocks of kBlock rows over the instances present on level l (smooth_only:
+// instances that are smoothed there, i.e. whose coarsest level is deeper).
+std::vector<Blk> block_table(const std::vector<std::vector<int>> &off, const std::vector<int> &clev, int l,
+                             bool smooth_only)
+{
+    std::vector<Blk> t;
+    const int ni = (int)clev.size();
+    for (int i = 0; i < ni; i++) {
+        if (clev[i] < l || (smooth_only && clev[i] == l)) continue;
+        const int r0 = off[l][i], rows = off[l][i + 1] - r0;
+        const int nb = (rows + kBlock - 1) / kBlock, first = (int)t.size();
+        for (int b = 0; b < nb; b++)
+            t.push_back(Blk{r0 + b * kBlock, std::min(kBlock, rows - b * kBlock), i, first, nb, 0, 0, 0});
+    }
+    return t;
+}
+
+template <typename T>
+LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
+{
+    LevelOff o{};
+    if (!fine) {
+        o.Ap = ar.vec(h.Ap);
+        o.Ac = ar.vec(h.Ac);
+        o.b = ar.zeros<T>(h.n);
+    }
+    if (!fine || !std::is_same<T, double>::value) {
+        o.Av = ar.vec(cast_vec<T>(h.Av));
+        o.dinv = ar.vec(cast_vec<T>(h.dinv));
+    }
+    if (!h.Pp.empty()) {
+        o.Pp = ar.vec(h.Pp); o.Pc = ar.vec(h.Pc); o.Pv = ar.vec(cast_vec<T>(h.Pv));
+        o.Rp = ar.vec(h.Rp); o.Rc = ar.vec(h.Rc); o.Rv = ar.vec(cast_vec<T>(h.Rv));
+    }
+    o.x = ar.zeros<T>(h.n);
+    o.r = ar.zeros<T>(h.n);
+    o.out = ar.zeros<T>(h.n);
+    o.sblk = ar.vec(h.sblk);
+    o.ablk = ar.vec(h.ablk);
+    return o;
+}
+
+template <typename T>
+VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const DevMat &M, bool fine)
+{
+    VLev<T> v{};
+    v.n = h.n;
+    if (fine) {
+        v.Ap = M.ptr;
+        v.Ac = M.col;
+        if (std::is_same<T, double>::value) {
+            v.Av = (const T *)M.val;
+            v.dinv = (const T *)M.dinv;
+        }
+    } else {
+        v.Ap = (const int32_t *)(base + o.Ap);
+        v.Ac = (const int32_t *)(base + o.Ac);
+        v.b = (T *)(base + o.b);
+    }
+    if (o.Av) v.Av = (const T *)(base + o.Av);
+    if (o.dinv) v.dinv = (const T *)(base + o.dinv);
+    if (o.Pp) {
+        v.Pp = (const int32_t *)(base + o.Pp); v.Pc = (const int32_t *)(base + o.Pc); v.Pv = (const T *)(base + o.Pv);
+        v.Rp = (const int32_t *)(base + o.Rp); v.Rc = (const int32_t *)(base + o.Rc); v.Rv = (const T *)(base + o.Rv);
+    }
+    v.x = (T *)(base + o.x);
+    v.r = (T *)(base + o.r);
+    v.out = (T *)(base + o.out);
+    v.sblk = (const Blk *)(base + o.sblk);
+    v.ablk = (const Blk *)(base + o.ablk);
+    v.nsblk = (int)h.sblk.size();
+    v.nablk = (int)h.ablk.size();
+    return v;
+}
+
+// Per-instance smoothed-aggregation hierarchies (hf_amg.cuh), concatenated
+// level by level, the finest-level CG state and the loop control.
+int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<int32_t> &mcol,
+              const std::vector<double> &mval, const std::vector<int> &pins)
 {
     const int ni = C->ninst;
-    struct LvlOff { int n; size_t Ap, Ac, Av, Av32, Pp, Pc, Pv, Pv32, Rp, Rc, Rv, Rv32, d, d32, x, b, r, out, x32, b32, r32, out32; };
-    struct InstOff {
-        int n, coff, nlev, cn, pin;
-        size_t cinv, cinv32, cb, cx, cb32, cx32, b, r, z, p, q, r32a, e32, t32, z32, p32, q32;
-        std::vector<LvlOff> lv;
+    const bool amg = C->amg, mixed = C->mixed;
+    struct InstHier {
+        std::vector<hf::HostLevel> H;
+        std::vector<double> inv;   // column-major
+        std::string err;
     };
-    Arena ar;
-    std::vector<InstOff> io(ni);
-    for (int i = 0; i < ni; i++) {
-        InstOff &o = io[i];
-        const int c0 = C->coff[i], n = C->coff[i + 1] - C->coff[i];
-        o.n = n;
-        o.coff = c0;
-        o.pin = pins[i] >= 0 ? pins[i] - c0 : -1;
-        hf::HostCSR A;
-        A.n = A.m = n;
-        A.ptr.assign(n + 1, 0);
-        for (int r = 0; r < n; r++) {
-            for (int k = mptr[c0 + r]; k < mptr[c0 + r + 1]; k++) {
-                const int c = mcol[k] - c0;
-                if (c < 0 || c >= n) return fail(HF_ERR_INVALID, "Poisson row reaches another instance");
-                A.col.push_back(c);
-                A.val.push_back(mval[k]);
+    std::vector<InstHier> IH(ni);
+    std::vector<int> clev(ni, 0);
+    if (amg) {
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            for (int i; (i = next++) < ni;) {
+                InstHier &ih = IH[i];
+                const int c0 = C->coff[i], n = C->coff[i + 1] - c0;
+                hf::HostCSR A;
+                A.n = A.m = n;
+                A.ptr.assign(n + 1, 0);
+                for (int r = 0; r < n && ih.err.empty(); r++) {
+                    for (int k = mptr[c0 + r]; k < mptr[c0 + r + 1]; k++) {
+                        const int c = mcol[k] - c0;
+                        if (c < 0 || c >= n) { ih.err = "Poisson row reaches another instance"; break; }
+                        A.col.push_back(c);
+                        A.val.push_back(mval[k]);
+                    }
+                    A.ptr[r + 1] = (int)A.col.size();
+                }
+                if (!ih.err.empty()) continue;
+                ih.H = hf::build_hierarchy(std::move(A), kMaxCoarse, kMaxLevels);
+                const hf::HostLevel &last = ih.H.back();
+                if (!last.P.ptr.empty()) { ih.err = "AMG hierarchy deeper than the level limit"; continue; }
+                const int cn = last.A.n;
+                if (cn > kCoarseCap) { ih.err = "AMG coarsening stalled above the dense-solve limit"; continue; }
+                std::vector<double> inv;
+                if (!hf::dense_inverse(last.A, inv)) { ih.err = "singular coarsest AMG level"; continue; }
+                ih.inv.resize(inv.size());
+                for (int r = 0; r < cn; r++)
+                    for (int c = 0; c < cn; c++) ih.inv[(size_t)c * cn + r] = inv[(size_t)r * cn + c];
             }
-            A.ptr[r + 1] = (int)A.col.size();
+        };
+        const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t + 1 < nt && (int)t < ni; t++) th.emplace_back(work);
+        work();
+        for (auto &t : th) t.join();
+        for (int i = 0; i < ni; i++) {
+            if (!IH[i].err.empty()) return fail(HF_ERR_UNSUPPORTED, IH[i].err + " (instance " + std::to_string(i) + ")");
+            clev[i] = (int)IH[i].H.size() - 1;
         }
-        std::vector<hf::HostLevel> H = hf::build_hierarchy(A, 64);
-        const hf::HostCSR &Cc = H.back().A;
-        if (Cc.n > 2048) return fail(HF_ERR_UNSUPPORTED, "AMG coarsening stalled above 2048 rows");
-        std::vector<double> inv;
-        if (!hf::dense_inverse(Cc, inv)) return fail(HF_ERR_INVALID, "singular coarsest AMG level");
-        o.nlev = (int)H.size() - 1;
-        o.cn = Cc.n;
-        o.cinv = ar.vec(inv);
-        o.cinv32 = mixed ? ar.vec(cast_vec<float>(inv)) : 0;
-        o.cb = ar.zeros<double>(o.cn);
-        o.cx = ar.zeros<double>(o.cn);
-        o.cb32 = mixed ? ar.zeros<float>(o.cn) : 0;
-        o.cx32 = mixed ? ar.zeros<float>(o.cn) : 0;
-        const int nl = std::max(o.nlev, 1);
-        for (int l = 0; l < nl; l++) {
-            const hf::HostLevel &h = H[l];
-            LvlOff L{};
-            L.n = h.A.n;
-            L.Ap = ar.vec(h.A.ptr);
-            L.Ac = ar.vec(h.A.col);
-            L.Av = ar.vec(h.A.val);
-            L.d = ar.vec(h.dinv);
-            if (l < o.nlev) {
-                L.Pp = ar.vec(h.P.ptr); L.Pc = ar.vec(h.P.col); L.Pv = ar.vec(h.P.val);
-                L.Rp = ar.vec(h.R.ptr); L.Rc = ar.vec(h.R.col); L.Rv = ar.vec(h.R.val);
-            }
-            L.x = ar.zeros<double>(L.n); L.b = ar.zeros<double>(L.n);
-            L.r = ar.zeros<double>(L.n); L.out = ar.zeros<double>(L.n);
-            if (mixed) {
-                L.Av32 = ar.vec(cast_vec<float>(h.A.val));
-                L.d32 = ar.vec(cast_vec<float>(h.dinv));
-                if (l < o.nlev) { L.Pv32 = ar.vec(cast_vec<float>(h.P.val)); L.Rv32 = ar.vec(cast_vec<float>(h.R.val)); }
-                L.x32 = ar.zeros<float>(L.n); L.b32 = ar.zeros<float>(L.n);
-                L.r32 = ar.zeros<float>(L.n); L.out32 = ar.zeros<float>(L.n);
-            }
-            o.lv.push_back(L);
-        }
-        o.b = ar.zeros<double>(n); o.r = ar.zeros<double>(n); o.z = ar.zeros<double>(n);
-        o.p = ar.zeros<double>(n); o.q = ar.zeros<double>(n);
-        if (mixed) {
-            o.r32a = ar.zeros<float>(n); o.e32 = ar.zeros<float>(n); o.t32 = ar.zeros<float>(n);
-            o.z32 = ar.zeros<float>(n); o.p32 = ar.zeros<float>(n); o.q32 = ar.zeros<float>(n);
-        }
-        C->batch_levels += nl;
     }
+    int nlev = 1;
+    for (int i = 0; i < ni; i++) nlev = std::max(nlev, clev[i] + 1);
+    C->nlev = nlev;
+    // row offsets of every instance on every level
+    std::vector<std::vector<int>> off(nlev, std::vector<int>(ni + 1, 0));
+    for (int l = 0; l < nlev; l++)
+        for (int i = 0; i < ni; i++) {
+            const int rows = l == 0 ? C->coff[i + 1] - C->coff[i] : (clev[i] >= l ? IH[i].H[l].A.n : 0);
+            off[l][i + 1] = off[l][i] + rows;
+        }
+    std::vector<LevelHost> LH(nlev);
+    C->lrows.assign(nlev, 0);
+    C->lnnz_a.assign(nlev, 0);
+    C->lnnz_p.assign(nlev, 0);
+    C->lnnz_r.assign(nlev, 0);
+    for (int l = 0; l < nlev; l++) {
+        LevelHost &h = LH[l];
+        h.n = off[l][ni];
+        C->lrows[l] = h.n;
+        if (l == 0) {
+            C->lnnz_a[0] = (int64_t)mcol.size();
+            if (amg) {
+                h.dinv.resize(h.n);
+                for (int i = 0; i < ni; i++)
+                    std::copy(IH[i].H[0].dinv.begin(), IH[i].H[0].dinv.end(), h.dinv.begin() + off[0][i]);
+                h.Av = mval;
+            }
+        } else {
+            h.Ap.assign(1, 0);
+            for (int i = 0; i < ni; i++) {
+                if (clev[i] < l) continue;
+                const hf::HostLevel &hl = IH[i].H[l];
+                for (int r = 0; r < hl.A.n; r++) {
+                    for (int k = hl.A.ptr[r]; k < hl.A.ptr[r + 1]; k++) {
+                        h.Ac.push_back(hl.A.col[k] + off[l][i]);
+                        h.Av.push_back(hl.A.val[k]);
+                    }
+                    h.Ap.push_back((int32_t)h.Ac.size());
+                }
+                h.dinv.insert(h.dinv.end(), hl.dinv.begin(), hl.dinv.end());
+            }
+            C->lnnz_a[l] = (int64_t)h.Ac.size();
+        }
+        if (l + 1 < nlev) {
+            // P: rows of this level -> next level; R: rows of the next level -> this level
+            h.Pp.assign(1, 0);
+            h.Rp.assign(1, 0);
+            for (int i = 0; i < ni; i++) {
+                if (clev[i] < l) continue;
+                const int rows = off[l][i + 1] - off[l][i];
+                if (clev[i] == l) {   // coarsest here: no transfer rows
+                    for (int r = 0; r < rows; r++) h.Pp.push_back((int32_t)h.Pc.size());
+                    continue;
+                }
+                const hf::HostLevel &hl = IH[i].H[l];
+                for (int r = 0; r < hl.P.n; r++) {
+                    for (int k = hl.P.ptr[r]; k < hl.P.ptr[r + 1]; k++) {
+                        h.Pc.push_back(hl.P.col[k] + off[l + 1][i]);
+                        h.Pv.push_back(hl.P.val[k]);
+                    }
+                    h.Pp.push_back((int32_t)h.Pc.size());
+                }
+                for (int r = 0; r < hl.R.n; r++) {
+                    for (int k = hl.R.ptr[r]; k < hl.R.ptr[r + 1]; k++) {
+                        h.Rc.push_back(hl.R.col[k] + off[l][i]);
+                        h.Rv.push_back(hl.R.val[k]);
+                    }
+                    h.Rp.push_back((int32_t)h.Rc.size());
+                }
+            }
+            C->lnnz_p[l] = (int64_t)h.Pc.size();
+            C->lnnz_r[l] = (int64_t)h.Rc.size();
+        }
+        h.sblk = block_table(off, clev, l, true);
+        h.ablk = block_table(off, clev, l, false);
+    }
+
+    // every index the kernels follow must stay inside its array
+    for (int l = 0; l < nlev; l++) {
+        const LevelHost &h = LH[l];
+        const int nn = l + 1 < nlev ? LH[l + 1].n : 0;
+        auto cols_ok = [](const std::vector<int32_t> &p, const std::vector<int32_t> &c, size_t rows, int ncol) {
+            if (p.size() != rows + 1 || p.back() != (int32_t)c.size()) return false;
+            for (int32_t v : c)
+                if (v < 0 || v >= ncol) return false;
+            return true;
+        };
+        bool ok = l == 0 || cols_ok(h.Ap, h.Ac, h.n, h.n);
+        if (ok && l + 1 < nlev) ok = cols_ok(h.Pp, h.Pc, h.n, nn) && cols_ok(h.Rp, h.Rc, nn, h.n);
+        for (const std::vector<Blk> *t : {&h.sblk, &h.ablk})
+            for (const Blk &b : *t)
+                if (b.row0 < 0 || b.cnt <= 0 || b.cnt > kBlock || b.row0 + b.cnt > h.n) ok = false;
+        if (!ok) return fail(HF_ERR_INVALID, "inconsistent multigrid level " + std::to_string(l));
+    }
+    for (int i = 0; i < ni && amg; i++)
+        if (off[clev[i]][i + 1] > LH[clev[i]].n || off[clev[i]][i + 1] - off[clev[i]][i] > kCoarseCap)
+            return fail(HF_ERR_INVALID, "inconsistent coarsest level");
+
+    // device arena: hierarchy (in the V-cycle's precision), dense inverses,
+    // CG vectors, partial sums, instance scalars and loop control
+    Arena ar;
+    ar.add(nullptr, 8);   // offset 0 stays unused: a zero offset means "absent"
+    std::vector<LevelOff> LO(nlev);
+    if (amg)
+        for (int l = 0; l < nlev; l++)
+            LO[l] = mixed ? place_level<float>(ar, LH[l], l == 0) : place_level<double>(ar, LH[l], l == 0);
+    std::vector<size_t> inv_off(ni, 0);
+    if (amg)
+        for (int i = 0; i < ni; i++)
+            inv_off[i] = mixed ? ar.vec(cast_vec<float>(IH[i].inv)) : ar.vec(IH[i].inv);
+    const int n = C->P.ncell;
+    const size_t o_r = ar.zeros<double>(n), o_z = ar.zeros<double>(n), o_q = ar.zeros<double>(n);
+    const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n);
+    const size_t o_part = ar.zeros<double>((size_t)LH[0].ablk.size() * 2);
+    std::vector<IScal> S(ni);
+    for (int i = 0; i < ni; i++) {
+        memset(&S[i], 0, sizeof(IScal));
+        S[i].clev = clev[i];
+        S[i].done = 1;
+    }
+    const size_t o_S = ar.vec(S);
+    Ctl ctl{};
+    ctl.maxbodies = C->opt.poisson_maxit / 2 + 2;
+    const size_t o_ctl = ar.add(&ctl, sizeof ctl);
+    std::vector<int32_t> ipin(pins.begin(), pins.end());
+    const size_t o_pin = ar.vec(ipin);
+    const size_t o_fblk = ar.vec(LH[0].ablk);
+
     char *base = nullptr;
     HF_CK(cudaMalloc((void **)&base, ar.host.size()));
     C->owned.push_back(base);
     C->bytes += (double)ar.host.size();
     HF_CK(cudaMemcpy(base, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice));
-    auto I = [&](size_t off) { return (int32_t *)(base + off); };
-    auto Dp = [&](size_t off) { return (double *)(base + off); };
-    auto Fp = [&](size_t off) { return mixed ? (float *)(base + off) : (float *)nullptr; };
-    std::vector<ILevel<double>> l64;
-    std::vector<ILevel<float>> l32;
-    std::vector<InstSolve> is(ni);
-    // largest instance first, so the longest solves start in the first wave
-    std::vector<int> order(ni);
-    for (int i = 0; i < ni; i++) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return io[a].n > io[b].n; });
-    for (int k = 0; k < ni; k++) {
-        const int i = order[k];
-        const InstOff &o = io[i];
-        InstSolve &s = is[k];
-        s.inst = i;
-        s.n = o.n;
-        s.coff = o.coff;
-        s.nlev = o.nlev;
-        s.lev = (int)l64.size();
-        s.cn = o.cn;
-        s.cinv64 = Dp(o.cinv);
-        s.cinv32 = mixed ? (const float *)(base + o.cinv32) : nullptr;
-        s.cb64 = Dp(o.cb); s.cx64 = Dp(o.cx);
-        s.cb32 = Fp(o.cb32); s.cx32 = Fp(o.cx32);
-        s.Mp = I(o.lv[0].Ap); s.Mc = I(o.lv[0].Ac); s.Mv = Dp(o.lv[0].Av);
-        s.apin = apin_dev + o.coff;
-        s.brhs = brhs_dev + o.coff;
-        s.pin = o.pin;
-        s.b = Dp(o.b); s.r = Dp(o.r); s.z = Dp(o.z); s.p = Dp(o.p); s.q = Dp(o.q);
-        s.r32 = Fp(o.r32a); s.e32 = Fp(o.e32); s.t32 = Fp(o.t32);
-        s.z32 = Fp(o.z32); s.p32 = Fp(o.p32); s.q32 = Fp(o.q32);
-        s.iters = C->d_res_i + 3 * i;
-        s.outer = C->d_res_i + 3 * i + 1;
-        s.status = C->d_res_i + 3 * i + 2;
-        s.res = C->d_res_d + i;
-        for (const LvlOff &L : o.lv) {
-            ILevel<double> a{};
-            a.n = L.n;
-            a.Ap = I(L.Ap); a.Ac = I(L.Ac); a.Av = Dp(L.Av);
-            a.Pp = L.Pp ? I(L.Pp) : nullptr; a.Pc = L.Pc ? I(L.Pc) : nullptr; a.Pv = L.Pv ? Dp(L.Pv) : nullptr;
-            a.Rp = L.Rp ? I(L.Rp) : nullptr; a.Rc = L.Rc ? I(L.Rc) : nullptr; a.Rv = L.Rv ? Dp(L.Rv) : nullptr;
-            a.dinv = Dp(L.d);
-            a.x = Dp(L.x); a.b = Dp(L.b); a.r = Dp(L.r); a.out = Dp(L.out);
-            l64.push_back(a);
-            ILevel<float> f{};
-            if (mixed) {
-                f.n = L.n;
-                f.Ap = a.Ap; f.Ac = a.Ac; f.Av = Fp(L.Av32);
-                f.Pp = a.Pp; f.Pc = a.Pc; f.Pv = L.Pv32 ? Fp(L.Pv32) : nullptr;
-                f.Rp = a.Rp; f.Rc = a.Rc; f.Rv = L.Rv32 ? Fp(L.Rv32) : nullptr;
-                f.dinv = Fp(L.d32);
-                f.x = Fp(L.x32); f.b = Fp(L.b32); f.r = Fp(L.r32); f.out = Fp(L.out32);
-            }
-            l32.push_back(f);
+
+    PcgFine &G = C->G;
+    G.n = n;
+    G.ptr = C->M.ptr;
+    G.col = C->M.col;
+    G.val = C->M.val;
+    G.dinv = C->M.dinv;
+    G.apin = C->M.apin;
+    G.brhs = C->M.brhs;
+    G.ipin = (const int32_t *)(base + o_pin);
+    G.ipar = C->P.ipar;
+    G.p = C->F.p;
+    G.dp = C->F.dp;
+    G.r = (double *)(base + o_r);
+    G.z = (double *)(base + o_z);
+    G.q = (double *)(base + o_q);
+    G.partials = (double *)(base + o_part);
+    G.S = (IScal *)(base + o_S);
+    G.ctl = (Ctl *)(base + o_ctl);
+    G.blk = (const Blk *)(base + o_fblk);
+    G.nblk = (int)LH[0].ablk.size();
+    G.ninst = ni;
+    G.rtol = C->opt.poisson_rtol;
+    G.atol = C->opt.poisson_atol;
+    G.maxit = C->opt.poisson_maxit;
+    C->pa = (double *)(base + o_pa);
+    C->pb = (double *)(base + o_pb);
+    if (amg) {
+        for (int l = 0; l < nlev; l++) {
+            if (mixed) C->L32[l] = make_level<float>(base, LO[l], LH[l], C->M, l == 0);
+            else C->L64[l] = make_level<double>(base, LO[l], LH[l], C->M, l == 0);
         }
+        std::vector<CoarseInst<double>> c64(ni);
+        std::vector<CoarseInst<float>> c32(ni);
+        for (int i = 0; i < ni; i++) {
+            const int l = clev[i], r0 = off[l][i], cn = off[l][i + 1] - r0;
+            CoarseInst<double> &a = c64[i];
+            CoarseInst<float> &b = c32[i];
+            a.inst = b.inst = i;
+            a.cn = b.cn = cn;
+            a.b64 = b.b64 = l == 0 ? G.r + r0 : nullptr;
+            if (mixed) {
+                b.b = l == 0 ? nullptr : C->L32[l].b + r0;
+                b.out = C->L32[l].out + r0;
+                b.inv = (const float *)(base + inv_off[i]);
+            } else {
+                a.b = l == 0 ? nullptr : C->L64[l].b + r0;
+                a.out = C->L64[l].out + r0;
+                a.inv = (const double *)(base + inv_off[i]);
+            }
+        }
+        double bytes = 0;
+        int rc;
+        if (mixed) {
+            if ((rc = upload(C->owned, &C->c32, c32.data(), c32.size(), bytes))) return rc;
+        } else if ((rc = upload(C->owned, &C->c64, c64.data(), c64.size(), bytes))) {
+            return rc;
+        }
+        C->bytes += bytes;
     }
-    double bytes = 0;
-    int rc;
-    if ((rc = upload(C->owned, &C->d_inst, is.data(), is.size(), bytes))) return rc;
-    if ((rc = upload(C->owned, &C->d_l64, l64.data(), l64.size(), bytes))) return rc;
-    if ((rc = upload(C->owned, &C->d_l32, l32.data(), l32.size(), bytes))) return rc;
-    C->bytes += bytes;
+    HF_CK(cudaMallocHost((void **)&C->h_S, sizeof(IScal) * ni));
+    HF_CK(cudaMallocHost((void **)&C->h_ctl, sizeof(Ctl)));
     return HF_OK;
 }
 
-// one V-cycle z = V(r) on the case stream (hf_amg.cuh)
-int64_t launch_vcycle(hf_case *C)
+// ---------------------------------------------------------------------------
+// one time step as a CUDA graph
+// ---------------------------------------------------------------------------
+template <typename T>
+void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const CoarseInst<T> *ci, int &kernels)
 {
-    const DevAMG &A = C->amg;
+    const IScal *S = C->G.S;
+    const double *r0 = C->G.r;
+    for (int l = 0; l + 1 < C->nlev; l++) {
+        if (L[l].nsblk) {
+            if (l == 0) k_vc_down<T, true><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
+            else k_vc_down<T, false><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
+            kernels++;
+        }
+        if (L[l + 1].nablk) {
+            k_vc_restrict<T><<<L[l + 1].nablk, kBlock, 0, st>>>(L[l], L[l + 1], S);
+            kernels++;
+        }
+    }
+    k_vc_coarse<T><<<C->ninst, kCoarseThreads, 0, st>>>(ci, S);
+    kernels++;
+    for (int l = C->nlev - 2; l >= 0; l--) {
+        if (!L[l].nsblk) continue;
+        k_vc_prolong<T><<<L[l].nsblk, kBlock, 0, st>>>(L[l], L[l + 1].out, S);
+        kernels++;
+        if (l > 0) {
+            k_vc_post<T><<<L[l].nsblk, kBlock, 0, st>>>(L[l], S);
+            kernels++;
+        }
+    }
+    k_pcg_z<T, false><<<C->G.nblk, kBlock, 0, st>>>(C->G, L[0]);
+    kernels++;
+}
+
+// two CG iterations (the direction vectors alternate, so two keep the graph static)
+void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, int &kernels)
+{
+    for (int it = 0; it < 2; it++) {
+        if (!C->amg) {
+            k_pcg_z<double, true><<<C->G.nblk, kBlock, 0, st>>>(C->G, VLev<double>{});
+            kernels++;
+        } else if (C->mixed) {
+            enqueue_vcycle<float>(C, st, C->L32, C->c32, kernels);
+        } else {
+            enqueue_vcycle<double>(C, st, C->L64, C->c64, kernels);
+        }
+        double *po = it == 0 ? C->pa : C->pb, *pn = it == 0 ? C->pb : C->pa;
+        k_pcg_dir<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
+        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, it == 1);
+        kernels += 2;
+    }
+}
+
+// a timing event recorded by the graph itself (an event-record node)
+void record(hf_case *C, int phase, int end)
+{
+    if (C->profile) cudaEventRecordWithFlags(C->ev[2 * phase + end], C->stream, cudaEventRecordExternal);
+}
+
+// Capture one step with the fields F (K/Knew as they are before the step).
+template <int D>
+int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
+{
     cudaStream_t st = C->stream;
-    const Scal *sc = C->cg.sc;
-    int64_t launches = 0;
-    for (int l = 0; l < A.nlev; l++) {
-        const DevLevel &L = A.lev[l];
-        k_vc_smooth0<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
-        k_vc_residual<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
-        double *bn = l + 1 < A.nlev ? A.lev[l + 1].b : A.cb;
-        k_vc_restrict<<<blocks(L.R.n), kBlock, 0, st>>>(L.R, L.r, bn, sc);
-        launches += 3;
+    const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    int fixed = 0, body = 0;
+    HF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    if (ve) {
+        record(C, HF_PHASE_VE_CELL, 0);
+        k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
+        record(C, HF_PHASE_VE_CELL, 1);
+        for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
+        fixed++;
     }
-    k_vc_coarse<<<blocks(A.cn), kBlock, 0, st>>>(A.cn, A.cinv, A.cb, A.cx, sc);
-    launches++;
-    for (int l = A.nlev - 1; l >= 0; l--) {
-        const DevLevel &L = A.lev[l];
-        const double *e = l + 1 < A.nlev ? A.lev[l + 1].out : A.cx;
-        k_vc_prolong<<<blocks(L.P.n), kBlock, 0, st>>>(L, e, sc);
-        if (l == 0) k_vc_post_fine<<<blocks(L.A.n), kBlock, 0, st>>>(L, C->cg);
-        else k_vc_post<<<blocks(L.A.n), kBlock, 0, st>>>(L, sc);
-        launches += 2;
+    record(C, HF_PHASE_VELOCITY, 0);
+    if (ve) k_velocity<D, true><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, F);
+    else k_velocity<D, false><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, F);
+    record(C, HF_PHASE_VELOCITY, 1);
+    record(C, HF_PHASE_POISSON_INIT, 0);
+    k_pcg_init<D><<<C->G.nblk, kBlock, 0, st>>>(C->P, F, C->G);
+    record(C, HF_PHASE_POISSON_INIT, 1);
+    record(C, HF_PHASE_POISSON_ITER, 0);
+    fixed += 2;
+
+    // the iterations: a conditional WHILE node after everything captured so far
+    cudaGraph_t g = nullptr;
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+    cudaGraphConditionalHandle cond = 0;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
     }
-    return launches;
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        cudaGraph_t bg = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(C->body_stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_body(C, C->body_stream, cond, body);
+            e = cudaStreamEndCapture(C->body_stream, &bg);
+        }
+    }
+    record(C, HF_PHASE_POISSON_ITER, 1);
+    record(C, HF_PHASE_FINAL, 0);
+    k_step_end<<<1, kBlock, 0, st>>>(C->G);
+    k_final<D><<<blocks(C->nfacet_total + C->P.ncell), kBlock, 0, st>>>(C->P, F);
+    record(C, HF_PHASE_FINAL, 1);
+    fixed += 2;
+    cudaGraph_t done = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &done);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (done) cudaGraphDestroy(done);
+        cudaGetLastError();
+        return fail(HF_ERR_CUDA, std::string("step graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    HF_CK(cudaGetLastError());
+    *gout = done;
+    C->fixed_kernels = fixed;
+    C->body_kernels = body;
+    return HF_OK;
+}
+
+void destroy_graphs(hf_case *C)
+{
+    for (int q = 0; q < 2; q++) {
+        if (C->exec[q]) cudaGraphExecDestroy(C->exec[q]);
+        if (C->graph[q]) cudaGraphDestroy(C->graph[q]);
+        C->exec[q] = nullptr;
+        C->graph[q] = nullptr;
+    }
+}
+
+// graph q runs a step that starts at parity q (K/Knew swapped for odd parity)
+template <int D>
+int ensure_graphs(hf_case *C)
+{
+    if (C->exec[0] && C->graph_profile == C->profile) return HF_OK;
+    destroy_graphs(C);
+    const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    for (int q = 0; q < (ve ? 2 : 1); q++) {
+        DevFields F = C->F;
+        if (ve && q != C->parity)
+            for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
+        int rc = capture_step<D>(C, F, &C->graph[q]);
+        if (rc) return rc;
+        HF_CK(cudaGraphInstantiate(&C->exec[q], C->graph[q], 0));
+    }
+    C->graph_profile = C->profile;
+    return HF_OK;
+}
+
+// device -> host copies of the instance scalars and the loop control
+int pull_state(hf_case *C)
+{
+    HF_CK(cudaMemcpyAsync(C->h_S, C->G.S, sizeof(IScal) * C->ninst, cudaMemcpyDeviceToHost, C->stream));
+    HF_CK(cudaMemcpyAsync(C->h_ctl, C->G.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, C->stream));
+    HF_CK(cudaStreamSynchronize(C->stream));
+    return HF_OK;
+}
+
+// the first failed solve since the last check, as a status (then cleared)
+int take_error(hf_case *C)
+{
+    const Ctl &c = *C->h_ctl;
+    if (!c.err_status) return HF_OK;
+    const int code = c.err_status;
+    std::string msg = "Poisson solve failed (" + std::to_string(code) + ") in instance " + std::to_string(c.err_inst) +
+                      " at step " + std::to_string(c.err_step);
+    HF_CK(cudaMemsetAsync(&C->G.ctl->err_status, 0, sizeof(int32_t), C->stream));
+    HF_CK(cudaStreamSynchronize(C->stream));
+    return fail(code, msg);
+}
+
+// Phase times of the last profiled step (its graph recorded the phase events);
+// waits for it.
+int collect_phases(hf_case *C)
+{
+    if (!C->phase_pending) return HF_OK;
+    C->phase_pending = false;
+    int rc = pull_state(C);
+    if (rc) return rc;
+    const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    for (int p = 0; p < HF_NPHASE; p++) {
+        if (p == HF_PHASE_VE_CELL && !ve) continue;
+        float ms = 0.f;
+        HF_CK(cudaEventElapsedTime(&ms, C->ev[2 * p], C->ev[2 * p + 1]));
+        C->phase_ms[p] += ms;
+    }
+    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 1;
+    C->phase_launches[HF_PHASE_VELOCITY] += 1;
+    C->phase_launches[HF_PHASE_POISSON_INIT] += 1;
+    C->phase_launches[HF_PHASE_POISSON_ITER] += (C->h_ctl->total_bodies - C->bodies0) * C->body_kernels;
+    C->phase_launches[HF_PHASE_FINAL] += 2;
+    return HF_OK;
 }
 
 template <int D>
-int launch_step(hf_case *C)
+int graph_steps(hf_case *C, int nsteps, bool sync)
+{
+    int rc = ensure_graphs<D>(C);
+    if (rc) return rc;
+    const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    for (int s = 0; s < nsteps; s++) {
+        if (C->profile) {
+            // one profiled step in flight at a time: its events are reused
+            if ((rc = C->phase_pending ? collect_phases(C) : pull_state(C))) return rc;
+            C->bodies0 = C->h_ctl->total_bodies;
+            HF_CK(cudaGraphLaunch(C->exec[ve ? C->parity : 0], C->stream));
+            C->phase_pending = true;
+        } else {
+            HF_CK(cudaGraphLaunch(C->exec[ve ? C->parity : 0], C->stream));
+        }
+        if (ve) {
+            for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
+            C->parity ^= 1;
+        }
+        C->stats.steps += 1;
+    }
+    if (!sync) return HF_OK;
+    if ((rc = collect_phases(C)) || (rc = pull_state(C))) return rc;
+    return take_error(C);
+}
+
+// BiCGStab (non-symmetric Poisson rows): one instance, host-driven loop
+template <int D>
+int bicg_step(hf_case *C)
 {
     cudaStream_t st = C->stream;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
@@ -1535,120 +1642,37 @@ int launch_step(hf_case *C)
     const double rtol = C->opt.poisson_rtol, atol = C->opt.poisson_atol;
     const int n = C->P.ncell;
     int rc = HF_OK;
-    if (C->persistent) {
-        {
-            PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
-            k_batch_poisson<D><<<C->ninst, kPB, 0, st>>>(C->P, C->F, C->d_inst, C->d_l64, C->d_l32,
-                                                          C->opt.precision == HF_PREC_MIXED, rtol, atol,
-                                                          C->opt.poisson_maxit);
-            launches++;
-            t.stop(launches);
-        }
-        HF_CK(cudaGetLastError());
-        HF_CK(cudaMemcpyAsync(C->h_res_i, C->d_res_i, sizeof(int) * 3 * C->ninst, cudaMemcpyDeviceToHost, st));
-        HF_CK(cudaMemcpyAsync(C->h_res_d, C->d_res_d, sizeof(double) * C->ninst, cudaMemcpyDeviceToHost, st));
-        HF_CK(cudaStreamSynchronize(st));
-        int it_max = 0, out_max = 0;
-        int64_t it_sum = 0;
-        double res_max = 0.0;
-        for (int i = 0; i < C->ninst; i++) {
-            it_max = std::max(it_max, C->h_res_i[3 * i]);
-            out_max = std::max(out_max, C->h_res_i[3 * i + 1]);
-            it_sum += C->h_res_i[3 * i];
-            res_max = std::max(res_max, C->h_res_d[i]);
-            if (C->h_res_i[3 * i + 2] && rc == HF_OK)
-                rc = fail(C->h_res_i[3 * i + 2], "Poisson solve failed in instance " + std::to_string(i));
-        }
-        C->h_scal->iters = it_max;
-        C->h_scal->rr = res_max * res_max;
-        C->h_scal->bb = 1.0;
-        C->stats.last_outer = out_max;
-        C->stats.total_iters += it_sum - it_max;   // the common update below adds it_max
-    } else if (C->use_cg && C->use_amg) {
+    int restarts = 0;
+    int from_step = 1;
+    for (;;) {
         {
             PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
-            k_pcg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
+            k_bi_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->bi, rtol, atol, from_step);
             launches++;
-            launches += launch_vcycle(C);
             t.stop(launches);
         }
-        double *pa = C->cg.pa, *pb = C->cg.pb;
         int chunk = 4;
         for (;;) {
             PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
             for (int k = 0; k < chunk; k++) {
-                k_cg_dir_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pa, pb);
-                k_pcg_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pb);
-                launches += 2 + launch_vcycle(C);
-                std::swap(pa, pb);
+                k_bi_p<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.ph, C->bi.v, 0);
+                k_bi_s<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.sh, C->bi.t, 1);
+                k_bi_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
+                launches += 5;
             }
             t.stop(launches);
-            HF_CK(cudaMemcpyAsync(C->h_scal, C->cg.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+            HF_CK(cudaMemcpyAsync(C->h_scal, C->bi.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
             HF_CK(cudaStreamSynchronize(st));
             if (C->h_scal->done) break;
-            chunk = std::min(chunk * 2, 16);
+            chunk = std::min(chunk * 2, 32);
         }
-        C->cg.pa = pa;
-        C->cg.pb = pb;
-        if (C->h_scal->status) rc = fail(C->h_scal->status, "Poisson AMG-CG failed");
-    } else if (C->use_cg) {
-        {
-            PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
-            k_cg_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->cg, rtol, atol);
-            launches++;
-            t.stop(launches);
-        }
-        double *pa = C->cg.pa, *pb = C->cg.pb;
-        int chunk = 8;
-        for (;;) {
-            PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
-            for (int k = 0; k < chunk; k++) {
-                k_cg_dir_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pa, pb);
-                k_cg_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->cg, pb);
-                std::swap(pa, pb);
-                launches += 2;
-            }
-            t.stop(launches);
-            HF_CK(cudaMemcpyAsync(C->h_scal, C->cg.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-            HF_CK(cudaStreamSynchronize(st));
-            if (C->h_scal->done) break;
-            chunk = std::min(chunk * 2, 64);
-        }
-        C->cg.pa = pa;
-        C->cg.pb = pb;
-        if (C->h_scal->status) rc = fail(C->h_scal->status, "Poisson CG failed");
-    } else {
-        int restarts = 0;
-        int from_step = 1;
-        for (;;) {
-            {
-                PhaseTimer t(C, HF_PHASE_POISSON_INIT, launches);
-                k_bi_init<D><<<blocks(n), kBlock, 0, st>>>(C->P, C->F, C->M, C->bi, rtol, atol, from_step);
-                launches++;
-                t.stop(launches);
-            }
-            int chunk = 4;
-            for (;;) {
-                PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
-                for (int k = 0; k < chunk; k++) {
-                    k_bi_p<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
-                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.ph, C->bi.v, 0);
-                    k_bi_s<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
-                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.sh, C->bi.t, 1);
-                    k_bi_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
-                    launches += 5;
-                }
-                t.stop(launches);
-                HF_CK(cudaMemcpyAsync(C->h_scal, C->bi.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-                HF_CK(cudaStreamSynchronize(st));
-                if (C->h_scal->done) break;
-                chunk = std::min(chunk * 2, 32);
-            }
-            if (C->h_scal->status == 1 && restarts++ < 50) { from_step = 0; continue; }
-            break;
-        }
-        if (C->h_scal->status) rc = fail(C->h_scal->status == 1 ? HF_ERR_NOT_CONVERGED : C->h_scal->status, "Poisson BiCGStab failed");
+        if (C->h_scal->status == 1 && restarts++ < 50) { from_step = 0; continue; }
+        break;
     }
+    if (C->h_scal->status)
+        rc = fail(C->h_scal->status == 1 ? HF_ERR_NOT_CONVERGED : C->h_scal->status, "Poisson BiCGStab failed");
     {
         PhaseTimer t(C, HF_PHASE_FINAL, launches);
         k_final<D><<<blocks(C->nfacet_total + n), kBlock, 0, st>>>(C->P, C->F);
@@ -1662,6 +1686,18 @@ int launch_step(hf_case *C)
     C->stats.kernel_launches += launches;
     C->stats.steps += 1;
     return rc;
+}
+
+int run_steps(hf_case *C, int nsteps, bool sync)
+{
+    if (!C->use_cg) {
+        for (int s = 0; s < nsteps; s++) {
+            int rc = C->D == 2 ? bicg_step<2>(C) : bicg_step<3>(C);
+            if (rc) return rc;
+        }
+        return HF_OK;
+    }
+    return C->D == 2 ? graph_steps<2>(C, nsteps, sync) : graph_steps<3>(C, nsteps, sync);
 }
 
 }  // namespace
@@ -1719,7 +1755,9 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         hf_case_destroy(C);
         return code;
     };
-    if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "stream"));
+    if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&C->body_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(HF_ERR_CUDA, "stream"));
     if (cudaMallocHost((void **)&C->h_scal, sizeof(Scal)) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "pinned scalars"));
 
     DevProg &P = C->P;
@@ -1832,14 +1870,11 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     if ((rc = build_matrix(pg, pins, mptr, mcol, mval, dinv, apin, sym))) return cleanup(rc);
     C->use_cg = opt.poisson == HF_POISSON_CG || (opt.poisson == HF_POISSON_AUTO && sym);
     if (opt.poisson == HF_POISSON_CG && !sym) return cleanup(fail(HF_ERR_UNSUPPORTED, "CG requested on a non-symmetric Poisson matrix"));
-    // the persistent per-instance solver serves batches and small single cases;
-    // one large case keeps the multi-kernel solver
-    int maxn = 0;
-    for (int i = 0; i < ni; i++) maxn = std::max(maxn, C->coff[i + 1] - C->coff[i]);
-    C->persistent = C->use_cg && opt.precond != HF_PRECOND_JACOBI && (ni > 1 || maxn <= 131072);
-    if (ni > 1 && !C->persistent) return cleanup(fail(HF_ERR_UNSUPPORTED, "batches need the AMG-CG Poisson solver"));
-    if (opt.precision == HF_PREC_MIXED && !C->persistent)
-        return cleanup(fail(HF_ERR_UNSUPPORTED, "the mixed form runs on the persistent per-instance solver"));
+    if (ni > 1 && !C->use_cg) return cleanup(fail(HF_ERR_UNSUPPORTED, "batches need symmetric Poisson rows (CG)"));
+    if (opt.precision == HF_PREC_MIXED && !C->use_cg)
+        return cleanup(fail(HF_ERR_UNSUPPORTED, "the mixed form needs the CG solver"));
+    C->amg = C->use_cg && opt.precond != HF_PRECOND_JACOBI;
+    C->mixed = C->amg && opt.precision == HF_PREC_MIXED;
     DevMat &M = C->M;
     M.n = pg->ncell;
     UP((int32_t **)&M.ptr, mptr.data(), mptr.size());
@@ -1860,69 +1895,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     UP(&partials, (const double *)nullptr, (size_t)nb * 4);
     const int n = pg->ncell;
     if (C->use_cg) {
-        C->cg.x = pg->par.projtype == HF_INCREMENTAL ? F.dp : F.p;
-        UP(&C->cg.r, (const double *)nullptr, n);
-        UP(&C->cg.z, (const double *)nullptr, n);
-        UP(&C->cg.pa, (const double *)nullptr, n);
-        UP(&C->cg.pb, (const double *)nullptr, n);
-        UP(&C->cg.q, (const double *)nullptr, n);
-        C->cg.partials = partials;
-        C->cg.sc = sc;
-        C->use_amg = opt.precond != HF_PRECOND_JACOBI && !C->persistent;
-        if (C->persistent) {
-            UP(&C->d_res_i, (const int *)nullptr, (size_t)3 * ni);
-            UP(&C->d_res_d, (const double *)nullptr, (size_t)ni);
-            if (cudaMallocHost((void **)&C->h_res_i, sizeof(int) * 3 * ni) != cudaSuccess ||
-                cudaMallocHost((void **)&C->h_res_d, sizeof(double) * ni) != cudaSuccess)
-                return cleanup(fail(HF_ERR_CUDA, "pinned results"));
-            if ((rc = build_batch_solver(C, mptr, mcol, mval, M.apin, M.brhs, pins, opt.precision == HF_PREC_MIXED)))
-                return cleanup(rc);
-        }
-        if (C->use_amg) {
-            hf::HostCSR M0;
-            M0.n = M0.m = n;
-            M0.ptr.assign(mptr.begin(), mptr.end());
-            M0.col.assign(mcol.begin(), mcol.end());
-            M0.val = mval;
-            std::vector<hf::HostLevel> H = hf::build_hierarchy(std::move(M0));
-            if ((int)H.size() - 1 > kMaxLevels) return cleanup(fail(HF_ERR_UNSUPPORTED, "AMG hierarchy too deep"));
-            DevAMG &A = C->amg;
-            A.nlev = (int)H.size() - 1;
-            C->amg_levels = (int)H.size();
-            for (int l = 0; l < A.nlev; l++) {
-                DevLevel &L = A.lev[l];
-                const hf::HostLevel &h = H[l];
-                auto up_csr = [&](DevCSR &d, const hf::HostCSR &s) {
-                    d.n = s.n;
-                    int r2;
-                    if ((r2 = upload(own, (int32_t **)&d.ptr, s.ptr.data(), s.ptr.size(), B))) return r2;
-                    if ((r2 = upload(own, (int32_t **)&d.col, s.col.data(), s.col.size(), B))) return r2;
-                    return upload(own, (double **)&d.val, s.val.data(), s.val.size(), B);
-                };
-                if (l == 0) {
-                    L.A = DevCSR{n, M.ptr, M.col, M.val};
-                } else if ((rc = up_csr(L.A, h.A))) {
-                    return cleanup(rc);
-                }
-                if ((rc = up_csr(L.P, h.P)) || (rc = up_csr(L.R, h.R))) return cleanup(rc);
-                UP((double **)&L.dinv, h.dinv.data(), h.dinv.size());
-                if (l == 0) {
-                    L.b = C->cg.r;
-                    L.out = C->cg.z;
-                } else {
-                    UP(&L.b, (const double *)nullptr, h.A.n);
-                    UP(&L.out, (const double *)nullptr, h.A.n);
-                }
-                UP(&L.x, (const double *)nullptr, h.A.n);
-                UP(&L.r, (const double *)nullptr, h.A.n);
-            }
-            std::vector<double> inv;
-            if (!hf::dense_inverse(H.back().A, inv)) return cleanup(fail(HF_ERR_INVALID, "singular coarsest AMG level"));
-            A.cn = H.back().A.n;
-            UP((double **)&A.cinv, inv.data(), inv.size());
-            UP(&A.cb, (const double *)nullptr, A.cn);
-            UP(&A.cx, (const double *)nullptr, A.cn);
-        }
+        if ((rc = build_pcg(C, mptr, mcol, mval, pins))) return cleanup(rc);
     } else {
         BiVec &V = C->bi;
         V.x = pg->par.projtype == HF_INCREMENTAL ? F.dp : F.p;
@@ -1998,26 +1971,46 @@ extern "C" int hf_case_get_field(hf_case *C, int32_t field, int32_t comp, double
 
 extern "C" int hf_case_step(hf_case *C, int32_t nsteps)
 {
-    if (!C) return fail(HF_ERR_INVALID, "null case");
-    for (int s = 0; s < nsteps; s++) {
-        int rc = C->D == 2 ? launch_step<2>(C) : launch_step<3>(C);
-        if (rc) return rc;
-    }
-    return HF_OK;
+    if (!C || nsteps < 0) return fail(HF_ERR_INVALID, "bad argument");
+    return run_steps(C, nsteps, true);
+}
+
+extern "C" int hf_case_step_async(hf_case *C, int32_t nsteps)
+{
+    if (!C || nsteps < 0) return fail(HF_ERR_INVALID, "bad argument");
+    return run_steps(C, nsteps, false);
 }
 
 extern "C" int hf_case_synchronize(hf_case *C)
 {
     if (!C) return fail(HF_ERR_INVALID, "null case");
     HF_CK(cudaStreamSynchronize(C->stream));
-    return HF_OK;
+    if (!C->use_cg) return HF_OK;
+    int rc = collect_phases(C);
+    if (!rc) rc = pull_state(C);
+    return rc ? rc : take_error(C);
 }
 
 extern "C" int hf_case_stats(hf_case *C, hf_stats *out)
 {
     if (!C || !out) return fail(HF_ERR_INVALID, "null argument");
+    if (C->use_cg) {
+        int rc = pull_state(C);
+        if (rc) return rc;
+        hf_stats &s = C->stats;
+        s.last_iters = 0;
+        s.last_residual = 0.0;
+        s.total_iters = 0;
+        for (int i = 0; i < C->ninst; i++) {
+            const IScal &q = C->h_S[i];
+            s.last_iters = std::max(s.last_iters, q.iters);
+            s.last_residual = std::max(s.last_residual, q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr));
+            s.total_iters += q.total_iters;
+        }
+        s.kernel_launches = s.steps * C->fixed_kernels + C->h_ctl->total_bodies * C->body_kernels;
+    }
     *out = C->stats;
-    if (!C->persistent) out->last_outer = 1;
+    out->last_outer = 1;
     return HF_OK;
 }
 
@@ -2032,17 +2025,32 @@ extern "C" int hf_case_instance_result(hf_case *C, int32_t inst, int32_t *iters,
                                        double *residual)
 {
     if (!C || inst < 0 || inst >= C->ninst) return fail(HF_ERR_INVALID, "bad instance");
-    if (!C->persistent) {
+    if (outer) *outer = 1;
+    if (!C->use_cg) {
         if (iters) *iters = C->stats.last_iters;
-        if (outer) *outer = 1;
-        if (status) *status = 0;
+        if (status) *status = C->h_scal->status == 1 ? HF_ERR_NOT_CONVERGED : C->h_scal->status;
         if (residual) *residual = C->stats.last_residual;
         return HF_OK;
     }
-    if (iters) *iters = C->h_res_i[3 * inst];
-    if (outer) *outer = C->h_res_i[3 * inst + 1];
-    if (status) *status = C->h_res_i[3 * inst + 2];
-    if (residual) *residual = C->h_res_d[inst];
+    int rc = pull_state(C);
+    if (rc) return rc;
+    const IScal &q = C->h_S[inst];
+    if (iters) *iters = q.iters;
+    if (status) *status = q.status;
+    if (residual) *residual = q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr);
+    return HF_OK;
+}
+
+extern "C" int hf_case_instance_iters(hf_case *C, int64_t *total_iters, int32_t n)
+{
+    if (!C || !total_iters || n != C->ninst) return fail(HF_ERR_INVALID, "bad argument");
+    if (!C->use_cg) {
+        total_iters[0] = C->stats.total_iters;
+        return HF_OK;
+    }
+    int rc = pull_state(C);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) total_iters[i] = C->h_S[i].total_iters;
     return HF_OK;
 }
 
@@ -2050,25 +2058,46 @@ extern "C" int hf_case_solver_info(hf_case *C, int32_t *method, int32_t *nlev, i
                                    int64_t *nnz_p, int64_t *nnz_r, int32_t max_levels)
 {
     if (!C || !method || !nlev) return fail(HF_ERR_INVALID, "null argument");
-    *method = C->use_cg ? (C->use_amg ? HF_PRECOND_AMG : HF_PRECOND_JACOBI) : -1;
-    *nlev = C->use_amg ? C->amg.nlev + 1 : 1;
-    for (int l = 0; l < *nlev && l < max_levels; l++) {
-        if (!C->use_amg) {
-            if (rows) rows[l] = C->M.n;
-            continue;
+    *method = C->use_cg ? (C->amg ? HF_PRECOND_AMG : HF_PRECOND_JACOBI) : -1;
+    if (!C->amg) {
+        *nlev = 1;
+        if (max_levels > 0) {
+            if (rows) rows[0] = C->M.n;
+            if (nnz_a) nnz_a[0] = C->use_cg ? C->lnnz_a[0] : 0;
+            if (nnz_p) nnz_p[0] = 0;
+            if (nnz_r) nnz_r[0] = 0;
         }
-        const bool coarse = l == C->amg.nlev;
-        std::vector<int32_t> hp(2);
-        auto nnz = [&](const DevCSR &d) -> int64_t {
-            int32_t last = 0;
-            if (d.ptr && cudaMemcpy(&last, d.ptr + d.n, sizeof last, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-            return last;
-        };
-        if (rows) rows[l] = coarse ? C->amg.cn : C->amg.lev[l].A.n;
-        if (nnz_a) nnz_a[l] = coarse ? (int64_t)C->amg.cn * C->amg.cn : nnz(C->amg.lev[l].A);
-        if (nnz_p) nnz_p[l] = coarse ? 0 : nnz(C->amg.lev[l].P);
-        if (nnz_r) nnz_r[l] = coarse ? 0 : nnz(C->amg.lev[l].R);
+        return HF_OK;
     }
+    // the concatenated levels, then one entry for the dense coarsest solves
+    *nlev = C->nlev + 1;
+    int64_t crows = 0, cdense = 0;
+    std::vector<CoarseInst<double>> c64;
+    std::vector<CoarseInst<float>> c32;
+    if (C->mixed) {
+        c32.resize(C->ninst);
+        HF_CK(cudaMemcpy(c32.data(), C->c32, sizeof(CoarseInst<float>) * C->ninst, cudaMemcpyDeviceToHost));
+        for (auto &c : c32) { crows += c.cn; cdense += (int64_t)c.cn * c.cn; }
+    } else {
+        c64.resize(C->ninst);
+        HF_CK(cudaMemcpy(c64.data(), C->c64, sizeof(CoarseInst<double>) * C->ninst, cudaMemcpyDeviceToHost));
+        for (auto &c : c64) { crows += c.cn; cdense += (int64_t)c.cn * c.cn; }
+    }
+    for (int l = 0; l < *nlev && l < max_levels; l++) {
+        const bool dense = l == C->nlev;
+        if (rows) rows[l] = dense ? crows : C->lrows[l];
+        if (nnz_a) nnz_a[l] = dense ? cdense : C->lnnz_a[l];
+        if (nnz_p) nnz_p[l] = dense ? 0 : C->lnnz_p[l];
+        if (nnz_r) nnz_r[l] = dense ? 0 : C->lnnz_r[l];
+    }
+    return HF_OK;
+}
+
+extern "C" int hf_case_launch_counts(hf_case *C, int32_t *per_step, int32_t *per_body)
+{
+    if (!C || !per_step || !per_body) return fail(HF_ERR_INVALID, "null argument");
+    *per_step = C->fixed_kernels;
+    *per_body = C->body_kernels;
     return HF_OK;
 }
 
@@ -2082,6 +2111,8 @@ extern "C" int hf_case_stream(hf_case *C, void **stream)
 extern "C" int hf_case_profile(hf_case *C, int32_t enable)
 {
     if (!C) return fail(HF_ERR_INVALID, "null case");
+    int rc = collect_phases(C);
+    if (rc) return rc;
     if (enable && !C->ev[0])
         for (int k = 0; k < 2 * HF_NPHASE; k++) HF_CK(cudaEventCreate(&C->ev[k]));
     C->profile = enable != 0;
@@ -2092,6 +2123,8 @@ extern "C" int hf_case_profile(hf_case *C, int32_t enable)
 extern "C" int hf_case_phase_times(hf_case *C, double *ms, int64_t *launches, int32_t n)
 {
     if (!C || n < 0) return fail(HF_ERR_INVALID, "bad argument");
+    int rc = collect_phases(C);
+    if (rc) return rc;
     for (int k = 0; k < n && k < HF_NPHASE; k++) {
         if (ms) ms[k] = C->phase_ms[k];
         if (launches) launches[k] = C->phase_launches[k];
@@ -2103,12 +2136,14 @@ extern "C" void hf_case_destroy(hf_case *C)
 {
     if (!C) return;
     if (C->stream) cudaStreamSynchronize(C->stream);
+    destroy_graphs(C);
     for (int k = 0; k < 2 * HF_NPHASE; k++)
         if (C->ev[k]) cudaEventDestroy(C->ev[k]);
     for (void *p : C->owned) cudaFree(p);
     if (C->h_scal) cudaFreeHost(C->h_scal);
-    if (C->h_res_i) cudaFreeHost(C->h_res_i);
-    if (C->h_res_d) cudaFreeHost(C->h_res_d);
+    if (C->h_S) cudaFreeHost(C->h_S);
+    if (C->h_ctl) cudaFreeHost(C->h_ctl);
+    if (C->body_stream) cudaStreamDestroy(C->body_stream);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;
 }

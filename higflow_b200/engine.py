@@ -40,6 +40,9 @@ def lib() -> C.CDLL:
         L.hf_case_set_field.argtypes = [V, C.c_int32, C.c_int32, P(C.c_double), C.c_int64]
         L.hf_case_get_field.argtypes = [V, C.c_int32, C.c_int32, P(C.c_double), C.c_int64]
         L.hf_case_step.argtypes = [V, C.c_int32]
+        L.hf_case_step_async.argtypes = [V, C.c_int32]
+        L.hf_case_launch_counts.argtypes = [V, P(C.c_int32), P(C.c_int32)]
+        L.hf_case_instance_iters.argtypes = [V, P(C.c_int64), C.c_int32]
         L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
         L.hf_case_synchronize.argtypes = [V]
         L.hf_case_destroy.argtypes = [V]
@@ -103,8 +106,23 @@ class Case:
         _check(lib().hf_case_get_field(self.h, fid, comp, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
         return out
 
-    def step(self, n: int = 1) -> None:
-        _check(lib().hf_case_step(self.h, n))
+    def step(self, n: int = 1, sync: bool = True) -> None:
+        """Advance n steps; with sync=False they are only queued on the case
+        stream and a failure surfaces at the next synchronize()."""
+        _check((lib().hf_case_step if sync else lib().hf_case_step_async)(self.h, n))
+
+    def instance_iters(self) -> np.ndarray:
+        """Poisson iterations of every instance summed over all steps so far."""
+        n = self.instances()
+        out = np.zeros(n, dtype=np.int64)
+        _check(lib().hf_case_instance_iters(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), n))
+        return out
+
+    def launch_counts(self):
+        """(kernels per step outside the Poisson loop, kernels per loop body)."""
+        a, b = C.c_int32(), C.c_int32()
+        _check(lib().hf_case_launch_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def synchronize(self) -> None:
         _check(lib().hf_case_synchronize(self.h))

@@ -61,9 +61,10 @@ enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
 /* precision forms */
 enum {
     HF_PREC_FP64 = 0,   /* plain: every gather, update and Poisson iterate in FP64 */
-    HF_PREC_MIXED = 1   /* FP32 stencil gathers + FP32 inner PCG inside FP64
-                           iterative refinement; FP64 eigen/kernel transform,
-                           outer residual and time accumulation              */
+    HF_PREC_MIXED = 1   /* the AMG V-cycle preconditioner in FP32; the CG
+                           recurrences, the finest Poisson operator, stencil
+                           gathers, eigen/kernel transform and time update
+                           stay FP64 (same residual test as the plain form) */
 };
 
 /* Poisson preconditioner (CG path) */
@@ -275,24 +276,39 @@ typedef struct hf_stats {
 int  hf_case_create(const hf_program *prog, const hf_options *opt, hf_case **out);
 int  hf_case_set_field(hf_case *c, int32_t field, int32_t comp, const double *host, int64_t n);
 int  hf_case_get_field(hf_case *c, int32_t field, int32_t comp, double *host, int64_t n);
-/* Advance nsteps time steps (each one the full reference sub-step order). */
+/* Advance nsteps time steps (each one the full reference sub-step order) and
+ * wait for them; returns the first failed Poisson solve among them.  With the
+ * CG solver each step is one CUDA graph launch on the case stream (the first
+ * call captures the graphs). */
 int  hf_case_step(hf_case *c, int32_t nsteps);
+/* The same without waiting: the steps are queued on the case stream and a
+ * failure is reported by the next hf_case_synchronize (or hf_case_step). */
+int  hf_case_step_async(hf_case *c, int32_t nsteps);
 int  hf_case_stats(hf_case *c, hf_stats *out);
 int  hf_case_synchronize(hf_case *c);
 void hf_case_destroy(hf_case *c);
 
 /* Poisson solver of a case: method (HF_PRECOND_AMG / HF_PRECOND_JACOBI for CG,
- * -1 for BiCGStab), number of levels (1 without AMG) and, per level up to
- * max_levels, rows and non-zeros of A, P and R (the coarsest level is dense:
- * nnz_a = rows^2, no P, R). */
+ * -1 for BiCGStab), number of levels and, per level up to max_levels, rows and
+ * non-zeros of A, P and R summed over the instances.  With AMG the levels are
+ * the concatenated multigrid levels followed by one entry for the dense
+ * coarsest solves of all instances (rows = sum cn, nnz_a = sum cn^2). */
 int  hf_case_solver_info(hf_case *c, int32_t *method, int32_t *nlev, int64_t *rows, int64_t *nnz_a,
                          int64_t *nnz_p, int64_t *nnz_r, int32_t max_levels);
 
+/* Kernels per step outside the Poisson iterations, and per loop body of the
+ * iterations (one body = two CG iterations). */
+int  hf_case_launch_counts(hf_case *c, int32_t *per_step, int32_t *per_body);
+
 /* Batches: number of instances, and the last step's Poisson result of one
- * instance (iterations, refinement sweeps, status, relative residual). */
+ * instance (iterations, refinement sweeps (always 1), status, relative
+ * residual ||r|| / ||b||). */
 int  hf_case_instances(hf_case *c, int32_t *ninst);
 int  hf_case_instance_result(hf_case *c, int32_t inst, int32_t *iters, int32_t *outer, int32_t *status,
                              double *residual);
+
+/* Poisson iterations of every instance summed over all steps so far (n = ninst). */
+int  hf_case_instance_iters(hf_case *c, int64_t *total_iters, int32_t n);
 
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);

@@ -104,15 +104,23 @@ def test_amg_iteration_count_is_small():
 
 
 def test_bicgstab_path_matches_cg():
-    prog, data = load_golden("cav2d_cubista")
+    """Both Poisson solvers against the reference's fields after the golden
+    steps.  BiCGStab stops on its recursive residual, which drifts from the true
+    one near 1e-13, so the two agree to ~1e-9 rather than to the CG's 1e-10."""
+    name = "cav2d_cubista"
+    prog, data = load_golden(name)
+    steps = int(data["steps"])
     out = []
     for solver in (hp.POISSON_CG, hp.POISSON_BICGSTAB):
         case = engine.Case(prog, _opts(poisson=solver))
         load_init(case, prog, data)
-        case.step(3)
-        out.append(case.get(hp.FIELD_P))
+        case.step(steps)
+        got = {k: case.get(fid, comp) for k, fid, comp in field_keys(prog)}
+        err = compare(got, {k: data["ref_" + k] for k, _, _ in field_keys(prog)}, ["u0", "u1", "p"])
+        assert max(err.values()) < 1e-9, (solver, err)
+        out.append(got["p"])
         case.close()
-    assert np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[0]) < 1e-10
+    assert np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[0]) < 1e-9
 
 
 def test_invalid_program_rejected_on_host():
