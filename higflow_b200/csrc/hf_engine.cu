@@ -38,6 +38,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -2443,4 +2444,126 @@ extern "C" void hf_slv_destroy(hf_slv *s)
     if (s->h_scal) cudaFreeHost(s->h_scal);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab without allocation: the hf_slv_solve iteration on a CSR system the
+// caller already holds in device memory, with every work vector in one static
+// device buffer.  For callers that cannot allocate once they run: a host code
+// that sizes its whole HBM budget at start-up, or one that solves on a stream
+// while other streams of the same device are busy, where cudaMalloc/cudaFree
+// would synchronise the device and stall them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNaMaxRows = 1 << 16;                            // 65536 rows
+constexpr int kNaMaxBlocks = (kNaMaxRows + kBlock - 1) / kBlock;
+constexpr size_t kNaScalDoubles = (sizeof(Scal) + 7) / 8;
+// dinv, r, rh, p, v, s, t, ph, sh; partial sums; scalars (about 4.7 MB)
+constexpr size_t kNaDoubles = 9 * (size_t)kNaMaxRows + 4 * (size_t)kNaMaxBlocks + kNaScalDoubles;
+static __device__ __align__(256) double g_noalloc_scratch[kNaDoubles];
+
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mutex;
+double *g_na_ptr[kNaMaxDevices] = {};
+
+// dinv = 1 / a_ii (1 where the diagonal is missing or zero), as slv_upload_matrix
+__global__ void __launch_bounds__(kBlock) k_na_dinv(DevMat M, double *dinv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M.n) return;
+    double d = 1.0;
+    for (int k = M.ptr[i]; k < M.ptr[i + 1]; k++)
+        if (M.col[k] == i && M.val[k] != 0.0) d = 1.0 / M.val[k];
+    dinv[i] = d;
+}
+
+// fresh scalars: zero, iteration cap set; the reduction counter is left as it is
+__global__ void k_na_begin(Scal *sc, int maxit)
+{
+    const unsigned counter = sc->counter;
+    Scal z{};
+    z.maxit = maxit;
+    z.counter = counter;
+    *sc = z;
+}
+
+}  // namespace
+
+extern "C" int hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const int32_t *col, const double *val,
+                                           const double *b, double *x, double rtol, double atol, int32_t maxit,
+                                           void *stream, int32_t *iterations, double *residual)
+{
+    if (n <= 0 || !ptr || !col || !val || !b || !x || maxit <= 0) return fail(HF_ERR_INVALID, "bad argument");
+    if (n > kNaMaxRows)
+        return fail(HF_ERR_INVALID, "system of " + std::to_string(n) + " rows exceeds the static scratch of " +
+                                        std::to_string(kNaMaxRows) + " rows");
+    int dev = 0;
+    HF_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNaMaxDevices) return fail(HF_ERR_INVALID, "device ordinal beyond the scratch table");
+    double *base;
+    {
+        // once per device, with that device current: the scratch's address
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        if (!g_na_ptr[dev]) {
+            double *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p)
+                return fail(HF_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+            g_na_ptr[dev] = p;
+        }
+        base = g_na_ptr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    DevMat M{};
+    M.n = n;
+    M.ptr = ptr;
+    M.col = col;
+    M.val = val;
+    double *dinv = base;
+    M.dinv = dinv;
+    BiVec V{};
+    double *v = base + kNaMaxRows;
+    V.x = x;
+    V.b = const_cast<double *>(b);   // k_slv_init and k_bi_* only read b
+    V.r = v; v += kNaMaxRows;
+    V.rh = v; v += kNaMaxRows;
+    V.p = v; v += kNaMaxRows;
+    V.v = v; v += kNaMaxRows;
+    V.s = v; v += kNaMaxRows;
+    V.t = v; v += kNaMaxRows;
+    V.ph = v; v += kNaMaxRows;
+    V.sh = v; v += kNaMaxRows;
+    V.partials = v; v += 4 * (size_t)kNaMaxBlocks;
+    V.sc = (Scal *)v;
+    k_na_dinv<<<blocks(n), kBlock, 0, st>>>(M, dinv);
+    k_na_begin<<<1, 1, 0, st>>>(V.sc, maxit);
+    Scal h{};
+    int restarts = 0, first = 1;
+    for (;;) {
+        k_slv_init<<<blocks(n), kBlock, 0, st>>>(M, V, rtol, atol, first);
+        first = 0;
+        int chunk = 4;
+        for (;;) {
+            for (int k = 0; k < chunk; k++) {
+                k_bi_p<<<blocks(n), kBlock, 0, st>>>(M, V);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(M, V, V.ph, V.v, 0);
+                k_bi_s<<<blocks(n), kBlock, 0, st>>>(M, V);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(M, V, V.sh, V.t, 1);
+                k_bi_update<<<blocks(n), kBlock, 0, st>>>(M, V);
+            }
+            HF_CK(cudaGetLastError());
+            HF_CK(cudaMemcpyAsync(&h, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+            HF_CK(cudaStreamSynchronize(st));
+            if (h.done) break;
+            chunk = std::min(chunk * 2, 32);
+        }
+        if (h.status == 1 && restarts++ < 50) continue;
+        break;
+    }
+    if (iterations) *iterations = h.iters;
+    if (residual) *residual = h.bb > 0 ? sqrt(h.rr / h.bb) : sqrt(h.rr);
+    if (h.status == HF_ERR_NAN) return fail(HF_ERR_NAN, "NaN in BiCGStab");
+    if (h.status) return fail(HF_ERR_NOT_CONVERGED, "BiCGStab did not converge");
+    return HF_OK;
 }

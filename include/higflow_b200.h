@@ -358,6 +358,24 @@ int  hf_slv_solve(hf_slv *s);                                                  /
 int  hf_slv_result(hf_slv *s, int32_t *iterations, double *residual, int32_t *converged);
 void hf_slv_destroy(hf_slv *s);                                                /* destroy           */
 
+/* No counterpart in the reference.  The hf_slv_solve iteration (Jacobi-
+ * preconditioned BiCGStab from the given x until ||b - A x|| <= max(rtol ||b||,
+ * atol)) on an n-row CSR system whose arrays (ptr: n+1, col/val: ptr[n], b, x:
+ * n) already live in device memory of the current device, queued on `stream`
+ * and waited for.  It allocates nothing: every work vector sits in one static
+ * device buffer of 65536 rows (about 4.7 MB), for callers that cannot allocate
+ * once running (an HBM budget fixed at start-up, or solves on one stream while
+ * other streams of the device are busy, which cudaMalloc/cudaFree would stall).
+ * Larger systems are rejected with HF_ERR_INVALID.  The first call on each
+ * device looks the buffer up (cudaGetSymbolAddress, which may load the module)
+ * and should come before any stream capture.  The buffer's reduction counter
+ * must be zero when a call starts: it is zero at load and every call that
+ * returns leaves it zero.  Calls that overlap (other threads or streams on the
+ * same device) share the buffer and race: serialise them. */
+int  hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const int32_t *col, const double *val,
+                                 const double *b, double *x, double rtol, double atol, int32_t maxit,
+                                 void *stream, int32_t *iterations, double *residual);
+
 #ifdef __cplusplus
 }
 #endif
