@@ -41,6 +41,11 @@ WORKLOADS = {
              "to 1e-10; one batch program, one CUDA graph launch per step",
         batch="c4", precision="mixed", dim=2,
     ),
+    "c4_64": dict(
+        name="the first 64 cavities of the batched Giesekus population (seed 0), otherwise as c4; a smaller "
+             "case of the same kernels for profiling",
+        batch="c4", count=64, precision="mixed", dim=2,
+    ),
     "c1": dict(
         name="2D Newtonian lid-driven cavity 64x64 (uniform quadtree, unit square), Re=100, lid u=1, "
              "explicit Euler dt=1e-4, CUBISTA, incremental projection, Poisson CG to 1e-10 relative residual, "
@@ -60,7 +65,7 @@ def load_program(wl):
     from higflow_b200 import program as hp
     from higflow_b200 import tiling, workloads
     if wl.get("batch") == "c4":
-        return workloads.batch(workloads.batched_giesekus())
+        return workloads.batch(workloads.batched_giesekus()[:wl.get("count", 256)])
     if wl.get("tiled"):
         prog = tiling.cavity(wl["dim"], wl["n"])
     else:
@@ -259,7 +264,8 @@ def run_b200(args, rank, world, device):
     mixed = wl["precision"] == "mixed"
     prec = hp.PREC_MIXED if mixed else hp.PREC_FP64
     t0 = time.perf_counter()
-    case = engine.Case(prog, engine.options(rtol=1e-10, atol=1e-300, device=device, precision=prec))
+    case = engine.Case(prog, engine.options(rtol=1e-10, atol=1e-300, device=device, precision=prec,
+                                            eager=args.eager))
     t_create = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(case.stream(), device=device)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
@@ -306,7 +312,7 @@ def run_b200(args, rank, world, device):
 
     # mixed vs plain: the same batch from the same state, both forms, K steps
     extra = {}
-    if mixed:
+    if mixed and not args.no_extras:
         state = {k: v.copy() for k, v in fields_of(case, prog).items()}
         m_case = case
         plain = engine.Case(prog, engine.options(rtol=1e-10, atol=1e-300, device=device, precision=hp.PREC_FP64))
@@ -333,32 +339,8 @@ def run_b200(args, rank, world, device):
         plain.close()
 
     # end to end through the C ABI with pinned host buffers, copies every step
-    import ctypes as C
-    pinned = {}
-    names = [(hp.FIELD_U, d) for d in range(prog.dim)] + [(hp.FIELD_P, 0)]
-    if prog.viscoelastic:
-        names += [(hp.FIELD_KERNEL, k) for k in range(prog.dim ** 2)]
-    for fid, comp in names:
-        n = prog.field_size(fid, comp)
-        pinned[(fid, comp)] = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        pinned[(fid, comp)].numpy()[:] = case.get(fid, comp)
-    h2d = sum(v.numel() * 8 for v in pinned.values())
-    L = engine.lib()
-    _barrier(world)
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        for (fid, comp), buf in pinned.items():
-            engine._check(L.hf_case_set_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
-                                              buf.numel()))
-        case.step(1)
-        for (fid, comp), buf in pinned.items():
-            engine._check(L.hf_case_get_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
-                                              buf.numel()))
-    t_e2e = _max_over_ranks(time.perf_counter() - t0, world, device)
-    e2e = {"value": cells * args.steps * world / t_e2e, "unit": UNIT,
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d}
     ninst = case.instances()
+    e2e = None if args.no_extras else end_to_end(case, prog, args, world, device)
     case.close()
 
     line = {
@@ -390,6 +372,41 @@ def run_b200(args, rank, world, device):
     }
     line.update(extra)
     return line
+
+
+def end_to_end(case, prog, args, world, device):
+    """The metric through the C ABI with pinned host buffers: every step copies
+    the state fields host -> device, steps, and copies them back."""
+    import ctypes as C
+    import torch
+    from higflow_b200 import engine
+    from higflow_b200 import program as hp
+    cells = prog.ncell
+    pinned = {}
+    names = [(hp.FIELD_U, d) for d in range(prog.dim)] + [(hp.FIELD_P, 0)]
+    if prog.viscoelastic:
+        names += [(hp.FIELD_KERNEL, k) for k in range(prog.dim ** 2)]
+    for fid, comp in names:
+        n = prog.field_size(fid, comp)
+        pinned[(fid, comp)] = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        pinned[(fid, comp)].numpy()[:] = case.get(fid, comp)
+    h2d = sum(v.numel() * 8 for v in pinned.values())
+    L = engine.lib()
+    _barrier(world)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        for (fid, comp), buf in pinned.items():
+            engine._check(L.hf_case_set_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
+                                              buf.numel()))
+        case.step(1)
+        for (fid, comp), buf in pinned.items():
+            engine._check(L.hf_case_get_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
+                                              buf.numel()))
+    t_e2e = _max_over_ranks(time.perf_counter() - t0, world, device)
+    e2e = {"value": cells * args.steps * world / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d}
+    return e2e
 
 
 # ---------------------------------------------------------------------------
@@ -475,6 +492,10 @@ def main():
     ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch kernels one by one instead of one CUDA graph per step (kernel profilers)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="warm-up and timed steps only (no plain-FP64 comparison, no end-to-end pass); for profiling")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -42,6 +42,7 @@
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "hf_amg.cuh"
@@ -79,6 +80,12 @@ struct DevProg {
     const uint32_t *vflags[3];
     const uint16_t *vdelta[3];
     int vns;
+    // general rows of the velocity stage, one per (row, field read) pair: the
+    // velocity slot codes index these pairs; k_vrows evaluates them into rowval
+    hf::Rows<double> vrow;
+    const uint8_t *vtag;
+    int nvrows;
+    double *rowval;
     const int32_t *dslots;
     const uint16_t *cdelta;
     const int32_t *cslots;
@@ -187,33 +194,115 @@ __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 // ---------------------------------------------------------------------------
 // velocity stage
 // ---------------------------------------------------------------------------
+// arr[d] for a small runtime d without indexing the parameter array
+// (a dynamic index would copy the kernel parameters to local memory)
+template <int N, typename T>
+__device__ __forceinline__ T pick(T const (&arr)[N], int d)
+{
+    T v = arr[0];
+#pragma unroll
+    for (int k = 1; k < N; k++)
+        if (d == k) v = arr[k];
+    return v;
+}
+
+// field read by velocity slot s of a facet normal to d (slot table in
+// include/higflow_b200.h)
+template <int D>
+__device__ __forceinline__ const double *vslot_field(const DevFields &F, int d, int s)
+{
+    if (s == HF_V_FU) return pick<3>(F.FU, d);
+    if (s == HF_V_PL || s == HF_V_PR) return F.p;
+    if (s == HF_V_FL || s == HF_V_FR) return F.F;
+    if (s < HF_V_NSLOT_NEWT(D)) {
+        const int d2 = (s - HF_V_BLK0) / HF_V_NB, k = (s - HF_V_BLK0) % HF_V_NB;
+        return (k < 4 || k >= 8) ? F.u[d2] : pick<3>(F.u, d);
+    }
+    const int d2 = (s - HF_V_NSLOT_NEWT(D)) / HF_V_NS;
+    return d == 0 ? F.S[d2] : d == 1 ? F.S[D + d2] : F.S[(D - 1) * D + d2];
+}
+
+// field of a velocity-stage general row by tag: 0-2 FU[d], 3 p, 4 F, 5-7 u[d],
+// 8-16 S[d * D + d2] (switches: a dynamic index would copy the parameters)
+
+__device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
+{
+    switch (tag) {
+    case 0: return F.FU[0];
+    case 1: return F.FU[1];
+    case 2: return F.FU[2];
+    case 3: return F.p;
+    case 4: return F.F;
+    case 5: return F.u[0];
+    case 6: return F.u[1];
+    case 7: return F.u[2];
+    case 8: return F.S[0];
+    case 9: return F.S[1];
+    case 10: return F.S[2];
+    case 11: return F.S[3];
+    case 12: return F.S[4];
+    case 13: return F.S[5];
+    case 14: return F.S[6];
+    case 15: return F.S[7];
+    default: return F.S[8];
+    }
+}
+
+// The general rows the velocity stage reads, one thread per row: the long
+// interpolation stencils (tens of entries) run here, coalesced and without
+// divergence, instead of inside the per-facet kernel.
+__global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= P.nvrows) return;
+    P.rowval[u] = hf::query(P.vrow, -u - 1, vtag_field(F, __ldg(P.vtag + u)));
+}
+
+// 128-thread blocks: the prefetched slots take ~170 registers per thread, and
+// three such blocks fit an SM where one 256-thread block would
+constexpr int kVelBlock = 128;
+
 template <int D, bool VE>
-__global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
+__global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= P.off[D]) return;
     int d = 0;
 #pragma unroll
     for (int k = 1; k < D; k++) d += (e >= P.off[k]);
-    const int f = e - P.off[d];
-    const int nf = P.nf[d];
-    const int32_t *__restrict__ sl = P.vslots[d];
-#define SL(s) __ldg(sl + (size_t)(s) * nf + f)
-    const double *fd = P.delta + (size_t)__ldg(P.vdelta[d] + f) * D;
-    const uint32_t fl = __ldg(P.vflags[d] + f);
-    const hf::Rows<double> &R = P.rows;
-    const hf_params &par = P.ipar[__ldg(P.finst[d] + f)];
+    const int f = e - pick<4>(P.off, d);
+    const int nf = pick<3>(P.nf, d);
+    const int32_t *__restrict__ sl = pick<3>(P.vslots, d);
+    // every slot code, then every slot value (a centre hit's field entry or a
+    // general row's value from k_vrows), as independent loads issued together
+    constexpr int NS = VE ? HF_V_NSLOT_VE(D) : HF_V_NSLOT_NEWT(D);
+    int32_t code[NS];
+    double val[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) code[s] = __ldg(sl + (size_t)s * nf + f);
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const bool unused = s >= HF_V_BLK0 && s < HF_V_NSLOT_NEWT(D) && (s - HF_V_BLK0) % HF_V_NB < 4 &&
+                            (s - HF_V_BLK0) / HF_V_NB == d;   // u[d] corners of the facet's own direction
+        const double *src = code[s] >= 0 ? vslot_field<D>(F, d, s) + code[s] : P.rowval + (-code[s] - 1);
+        val[s] = unused ? 0.0 : __ldg(src);
+    }
+#define SLQ(s, fld) (val[s])
+    const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
+    const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
+    const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
     const double a = 1.7500, b = 0.3750, c = 0.7500, dd = 0.1250, ee = 0.2500;
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
     double conv1 = 0.0, conv2 = 0.0;
-    const double ufacet = F.u[d][f];
-    double Fs = hf::query(R, SL(HF_V_FU), F.FU[d]);
-    const double pl = hf::query(R, SL(HF_V_PL), F.p);
-    const double pr = hf::query(R, SL(HF_V_PR), F.p);
+    const double *ud = pick<3>(F.u, d);
+    const double ufacet = __ldg(ud + f);
+    double Fs = SLQ(HF_V_FU, pick<3>(F.FU, d));
+    const double pl = SLQ(HF_V_PL, F.p);
+    const double pr = SLQ(HF_V_PR, F.p);
     const double dpdx = (pr - pl) / (2.0 * 0.5 * fd[d]);
-    const double Fl = hf::query(R, SL(HF_V_FL), F.F);
-    const double Fr = hf::query(R, SL(HF_V_FR), F.F);
+    const double Fl = SLQ(HF_V_FL, F.F);
+    const double Fr = SLQ(HF_V_FR, F.F);
     Fs += (Fr + Fl) / 2.0;
     double v[D], dudxc[D], dudxr[D], dudxl[D], dudxrr[D], dudxll[D], du2dx2[D], vc[D];
 #pragma unroll
@@ -225,31 +314,31 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
         if (d2 == d) {
             v[d2] = ufacet;
         } else {
-            const double vrr = hf::query(R, SL(B + HF_V_V4 + 0), F.u[d2]);
-            const double vlr = hf::query(R, SL(B + HF_V_V4 + 1), F.u[d2]);
-            const double vrl = hf::query(R, SL(B + HF_V_V4 + 2), F.u[d2]);
-            const double vll = hf::query(R, SL(B + HF_V_V4 + 3), F.u[d2]);
+            const double vrr = SLQ(B + HF_V_V4 + 0, F.u[d2]);
+            const double vlr = SLQ(B + HF_V_V4 + 1, F.u[d2]);
+            const double vrl = SLQ(B + HF_V_V4 + 2, F.u[d2]);
+            const double vll = SLQ(B + HF_V_V4 + 3, F.u[d2]);
             v[d2] = 0.25 * (vll + vlr + vrl + vrr);
         }
-        const double ul = hf::query(R, SL(B + HF_V_UL), F.u[d]);
+        const double ul = SLQ(B + HF_V_UL, ud);
         const int infl = (fl >> (4 * d2 + 0)) & 1;
         if (infl == 0 && convec == HF_SECOND_ORDER) convec = HF_FIRST_ORDER;
-        const double ur = hf::query(R, SL(B + HF_V_UR), F.u[d]);
+        const double ur = SLQ(B + HF_V_UR, ud);
         const int infr = (fl >> (4 * d2 + 1)) & 1;
         if (infr == 0 && convec == HF_SECOND_ORDER) convec = HF_FIRST_ORDER;
         dudxc[d2] = (ur - ul) / (2.0 * 1.0 * fd[d2]);
         dudxr[d2] = (ur - ufacet) / (1.0 * fd[d2]);
         dudxl[d2] = (ufacet - ul) / (1.0 * fd[d2]);
-        const double urr = hf::query(R, SL(B + HF_V_URR), F.u[d]);
+        const double urr = SLQ(B + HF_V_URR, ud);
         const int infrr = (fl >> (4 * d2 + 3)) & 1;
-        const double ull = hf::query(R, SL(B + HF_V_ULL), F.u[d]);
+        const double ull = SLQ(B + HF_V_ULL, ud);
         const int infll = (fl >> (4 * d2 + 2)) & 1;
         if (convec == HF_SECOND_ORDER) {
             if (second == HF_QUICK) {
                 dudxrr[d2] = (urr - ur) / (1.0 * fd[d2]);
                 dudxll[d2] = (ul - ull) / (1.0 * fd[d2]);
             } else if (second == HF_CUBISTA) {
-                const double vcr = hf::query(R, SL(B + HF_V_VCR), F.u[d2]);
+                const double vcr = SLQ(B + HF_V_VCR, F.u[d2]);
                 if (vcr > 0.0) {
                     if (HF_FLT_EQ(ur, ul)) {
                         conv1 = vcr * ufacet;
@@ -277,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
                         }
                     }
                 }
-                const double vcl = hf::query(R, SL(B + HF_V_VCL), F.u[d2]);
+                const double vcl = SLQ(B + HF_V_VCL, F.u[d2]);
                 if (vcl > 0.0) {
                     if (HF_FLT_EQ(ufacet, ull)) {
                         conv2 = vcl * ul;
@@ -316,17 +405,17 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
 #pragma unroll
         for (int d2 = 0; d2 < D; d2++) {
             const int B = HF_V_NSLOT_NEWT(D) + HF_V_NS * d2;
-            const double *Sf = F.S[d * D + d2];
+            const double *Sf = vslot_field<D>(F, d, HF_V_NSLOT_NEWT(D) + HF_V_NS * d2);
             if (d2 == d) {
-                const double Sl = hf::query(R, SL(B + 0), Sf);
-                const double Sr = hf::query(R, SL(B + 2), Sf);
+                const double Sl = SLQ(B + 0, Sf);
+                const double Sr = SLQ(B + 2, Sf);
                 dSdx[d2] = (Sr - Sl) / (2.0 * 0.5 * fd[d2]);
             } else {
-                const double l1 = hf::query(R, SL(B + 0), Sf);
-                const double l2 = hf::query(R, SL(B + 1), Sf);
+                const double l1 = SLQ(B + 0, Sf);
+                const double l2 = SLQ(B + 1, Sf);
                 const double Sl = 0.5 * (l1 + l2);
-                const double r1 = hf::query(R, SL(B + 2), Sf);
-                const double r2 = hf::query(R, SL(B + 3), Sf);
+                const double r1 = SLQ(B + 2, Sf);
+                const double r2 = SLQ(B + 3, Sf);
                 const double Sr = 0.5 * (r1 + r2);
                 dSdx[d2] = (Sr - Sl) / (2.0 * 1.0 * fd[d2]);
             }
@@ -334,7 +423,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
 #pragma unroll
         for (int d2 = 0; d2 < D; d2++) tens += dSdx[d2];
     }
-#undef SL
+#undef SLQ
     const double pterm = par.projtype == HF_INCREMENTAL ? dpdx : 0.0;
     double conv = 0.0;
     if (convec == HF_CENTRAL) {
@@ -388,7 +477,7 @@ __global__ void __launch_bounds__(kBlock) k_velocity(DevProg P, DevFields F)
         rhs -= conv;
         rhs += diff;
     }
-    F.us[d][f] = ufacet + par.dt * rhs;
+    pick<3>(F.us, d)[f] = ufacet + par.dt * rhs;
 }
 
 // ---------------------------------------------------------------------------
@@ -743,15 +832,17 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
         int d = 0;
 #pragma unroll
         for (int k = 1; k < D; k++) d += (e >= P.off[k]);
-        const int f = e - P.off[d];
-        const int nf = P.nf[d];
-        const hf_params &par = P.ipar[__ldg(P.finst[d] + f)];
+        const int f = e - pick<4>(P.off, d);
+        const int nf = pick<3>(P.nf, d);
+        const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
         const double *pp = par.projtype == HF_INCREMENTAL ? F.dp : F.p;
-        const double *fd = P.delta + (size_t)__ldg(P.vdelta[d] + f) * D;
-        const double pl = hf::query(P.rows, __ldg(P.vslots[d] + (size_t)HF_V_PL * nf + f), pp);
-        const double pr = hf::query(P.rows, __ldg(P.vslots[d] + (size_t)HF_V_PR * nf + f), pp);
+        const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
+        const int32_t *sl = pick<3>(P.vslots, d);
+        const int32_t cl = __ldg(sl + (size_t)HF_V_PL * nf + f), cr = __ldg(sl + (size_t)HF_V_PR * nf + f);
+        const double pl = hf::query(P.vrow, cl, pp);
+        const double pr = hf::query(P.vrow, cr, pp);
         const double dpdx = (pr - pl) / (2.0 * 0.5 * fd[d]);
-        F.u[d][f] = F.us[d][f] - par.dt * dpdx;
+        pick<3>(F.u, d)[f] = __ldg(pick<3>(F.us, d) + f) - par.dt * dpdx;
     } else {
         const int c = e - P.off[D];
         if (c < P.ncell && P.ipar[__ldg(P.cinst + c)].projtype == HF_INCREMENTAL) F.p[c] = F.p[c] + F.dp[c];
@@ -812,6 +903,7 @@ struct hf_case {
     cudaGraphExec_t exec[2] = {};
     bool graph_profile = false;     // graphs were captured with phase events
     bool phase_pending = false;     // a profiled step's events are not read yet
+    bool capturing = false;         // a step graph is being captured
     int64_t bodies0 = 0;            // loop bodies before that step
     int parity = 0;
     std::vector<void *> owned;
@@ -1421,7 +1513,8 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const CoarseI
     kernels++;
 }
 
-// two CG iterations (the direction vectors alternate, so two keep the graph static)
+// two CG iterations (the direction vectors alternate, so two keep the graph
+// static); cond == 0: eager launches, the body is only counted on the device
 void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, int &kernels)
 {
     for (int it = 0; it < 2; it++) {
@@ -1435,25 +1528,27 @@ void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, 
         }
         double *po = it == 0 ? C->pa : C->pb, *pn = it == 0 ? C->pb : C->pa;
         k_pcg_dir<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
-        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, it == 1);
+        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, it == 1 ? (cond ? 1 : 2) : 0);
         kernels += 2;
     }
 }
 
-// a timing event recorded by the graph itself (an event-record node)
+// a phase timing event; while a step graph is captured it becomes an
+// event-record node of the graph
 void record(hf_case *C, int phase, int end)
 {
-    if (C->profile) cudaEventRecordWithFlags(C->ev[2 * phase + end], C->stream, cudaEventRecordExternal);
+    if (!C->profile) return;
+    if (C->capturing) cudaEventRecordWithFlags(C->ev[2 * phase + end], C->stream, cudaEventRecordExternal);
+    else cudaEventRecord(C->ev[2 * phase + end], C->stream);
 }
 
-// Capture one step with the fields F (K/Knew as they are before the step).
+// The kernels of a step before the Poisson iterations: viscoelastic cell stage
+// (F's K/Knew swap after it), intermediate velocity, Poisson right-hand side.
 template <int D>
-int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
+void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
 {
     cudaStream_t st = C->stream;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
-    int fixed = 0, body = 0;
-    HF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     if (ve) {
         record(C, HF_PHASE_VE_CELL, 0);
         k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
@@ -1462,14 +1557,64 @@ int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
         fixed++;
     }
     record(C, HF_PHASE_VELOCITY, 0);
-    if (ve) k_velocity<D, true><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, F);
-    else k_velocity<D, false><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, F);
+    if (C->P.nvrows) {
+        k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
+        fixed++;
+    }
+    if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
     record(C, HF_PHASE_VELOCITY, 1);
     record(C, HF_PHASE_POISSON_INIT, 0);
     k_pcg_init<D><<<C->G.nblk, kBlock, 0, st>>>(C->P, F, C->G);
     record(C, HF_PHASE_POISSON_INIT, 1);
     record(C, HF_PHASE_POISSON_ITER, 0);
     fixed += 2;
+}
+
+// ... and after them: per-instance totals, final velocity and pressure
+template <int D>
+void enqueue_post(hf_case *C, const DevFields &F, int &fixed)
+{
+    cudaStream_t st = C->stream;
+    record(C, HF_PHASE_POISSON_ITER, 1);
+    record(C, HF_PHASE_FINAL, 0);
+    k_step_end<<<1, kBlock, 0, st>>>(C->G);
+    k_final<D><<<blocks(C->nfacet_total + C->P.ncell), kBlock, 0, st>>>(C->P, F);
+    record(C, HF_PHASE_FINAL, 1);
+    fixed += 2;
+}
+
+// One step with eager launches: the host reads the loop control after each body.
+template <int D>
+int eager_step(hf_case *C)
+{
+    DevFields F = C->F;
+    int fixed = 0, body = 0;
+    enqueue_pre<D>(C, F, fixed);
+    for (;;) {
+        body = 0;
+        enqueue_body(C, C->stream, 0, body);
+        HF_CK(cudaGetLastError());
+        HF_CK(cudaMemcpyAsync(C->h_ctl, C->G.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, C->stream));
+        HF_CK(cudaStreamSynchronize(C->stream));
+        if (!(C->h_ctl->active > 0 && C->h_ctl->bodies < C->h_ctl->maxbodies)) break;
+    }
+    enqueue_post<D>(C, F, fixed);
+    HF_CK(cudaGetLastError());
+    C->fixed_kernels = fixed;
+    C->body_kernels = body;
+    return HF_OK;
+}
+
+// Capture one step with the fields F (K/Knew as they are before the step).
+template <int D>
+int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
+{
+    cudaStream_t st = C->stream;
+    int fixed = 0, body = 0;
+    HF_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    C->capturing = true;
+    enqueue_pre<D>(C, F, fixed);
 
     // the iterations: a conditional WHILE node after everything captured so far
     cudaGraph_t g = nullptr;
@@ -1497,14 +1642,10 @@ int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
             e = cudaStreamEndCapture(C->body_stream, &bg);
         }
     }
-    record(C, HF_PHASE_POISSON_ITER, 1);
-    record(C, HF_PHASE_FINAL, 0);
-    k_step_end<<<1, kBlock, 0, st>>>(C->G);
-    k_final<D><<<blocks(C->nfacet_total + C->P.ncell), kBlock, 0, st>>>(C->P, F);
-    record(C, HF_PHASE_FINAL, 1);
-    fixed += 2;
+    enqueue_post<D>(C, F, fixed);
     cudaGraph_t done = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(st, &done);
+    C->capturing = false;
     if (e != cudaSuccess || e2 != cudaSuccess) {
         if (done) cudaGraphDestroy(done);
         cudaGetLastError();
@@ -1594,18 +1735,24 @@ int collect_phases(hf_case *C)
 template <int D>
 int graph_steps(hf_case *C, int nsteps, bool sync)
 {
-    int rc = ensure_graphs<D>(C);
+    const bool eager = C->opt.eager != 0;
+    int rc = eager ? HF_OK : ensure_graphs<D>(C);
     if (rc) return rc;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    auto one = [&]() -> int {
+        if (eager) return eager_step<D>(C);
+        HF_CK(cudaGraphLaunch(C->exec[ve ? C->parity : 0], C->stream));
+        return HF_OK;
+    };
     for (int s = 0; s < nsteps; s++) {
         if (C->profile) {
             // one profiled step in flight at a time: its events are reused
             if ((rc = C->phase_pending ? collect_phases(C) : pull_state(C))) return rc;
             C->bodies0 = C->h_ctl->total_bodies;
-            HF_CK(cudaGraphLaunch(C->exec[ve ? C->parity : 0], C->stream));
+            if ((rc = one())) return rc;
             C->phase_pending = true;
-        } else {
-            HF_CK(cudaGraphLaunch(C->exec[ve ? C->parity : 0], C->stream));
+        } else if ((rc = one())) {
+            return rc;
         }
         if (ve) {
             for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
@@ -1634,8 +1781,12 @@ int bicg_step(hf_case *C)
     }
     {
         PhaseTimer t(C, HF_PHASE_VELOCITY, launches);
-        if (ve) k_velocity<D, true><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
-        else k_velocity<D, false><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, C->F);
+        if (C->P.nvrows) {
+            k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, C->F);
+            launches++;
+        }
+        if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
+        else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
         launches++;
         t.stop(launches);
     }
@@ -1834,10 +1985,73 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     UP((int64_t **)&P.rows.tptr, pg->tmpl_ptr, pg->ntmpl + 1);
     UP((int32_t **)&P.rows.col, pg->tmpl_col, pg->nnz);
     UP((double **)&P.rows.w, pg->tmpl_w, pg->nnz);
-    for (int d = 0; d < D; d++) {
-        UP((int32_t **)&P.vslots[d], pg->vel_slots[d], (size_t)pg->vel_nslot * pg->nfacet[d]);
-        UP((uint32_t **)&P.vflags[d], pg->vel_flags[d], pg->nfacet[d]);
-        UP((uint16_t **)&P.vdelta[d], pg->vel_delta[d], pg->nfacet[d]);
+    {
+        // velocity slots: general codes renumbered to (row, field read) pairs,
+        // so that k_vrows can evaluate each pair once per step on its field
+        std::vector<int32_t> pair_first(pg->nrows, -1);
+        std::vector<uint8_t> tag_first(pg->nrows, 0);
+        std::unordered_map<uint64_t, int32_t> extra;   // pairs of rows read on a second field
+        std::vector<int32_t> ptmpl, pbase;
+        std::vector<double> prhs;
+        std::vector<uint8_t> ptag;
+        bool overflow = false;
+        auto pair_index = [&](int64_t r, int tag) -> int32_t {
+            auto add = [&]() {
+                if (ptmpl.size() >= (size_t)INT32_MAX) overflow = true;
+                ptmpl.push_back(pg->row_tmpl[r]);
+                pbase.push_back(pg->row_base[r]);
+                prhs.push_back(pg->row_rhs[r]);
+                ptag.push_back((uint8_t)tag);
+                return (int32_t)(ptmpl.size() - 1);
+            };
+            if (pair_first[r] < 0) {
+                tag_first[r] = (uint8_t)tag;
+                return pair_first[r] = add();
+            }
+            if (tag_first[r] == tag) return pair_first[r];
+            const uint64_t key = (uint64_t)r * 32 + (uint64_t)tag;
+            auto it = extra.find(key);
+            if (it != extra.end()) return it->second;
+            const int32_t u = add();
+            extra.emplace(key, u);
+            return u;
+        };
+        std::vector<int32_t> row;
+        for (int d = 0; d < D; d++) {
+            const int64_t nf = pg->nfacet[d];
+            UP((int32_t **)&P.vslots[d], (const int32_t *)nullptr, (size_t)pg->vel_nslot * nf);
+            for (int s = 0; s < pg->vel_nslot; s++) {
+                int tag;
+                if (s == HF_V_FU) tag = d;
+                else if (s == HF_V_PL || s == HF_V_PR) tag = 3;
+                else if (s == HF_V_FL || s == HF_V_FR) tag = 4;
+                else if (s < HF_V_NSLOT_NEWT(D)) {
+                    const int d2 = (s - HF_V_BLK0) / HF_V_NB, k = (s - HF_V_BLK0) % HF_V_NB;
+                    tag = 5 + ((k < 4 || k >= 8) ? d2 : d);
+                } else {
+                    tag = 8 + d * D + (s - HF_V_NSLOT_NEWT(D)) / HF_V_NS;
+                }
+                const int32_t *sl = pg->vel_slots[d] + (size_t)s * nf;
+                row.assign(sl, sl + nf);
+                for (int64_t f = 0; f < nf; f++)
+                    if (row[f] < 0) row[f] = -pair_index(-(int64_t)row[f] - 1, tag) - 1;
+                if (overflow) return cleanup(fail(HF_ERR_UNSUPPORTED, "too many velocity-stage rows"));
+                if (cudaMemcpy((int32_t *)P.vslots[d] + (size_t)s * nf, row.data(), sizeof(int32_t) * nf,
+                               cudaMemcpyHostToDevice) != cudaSuccess)
+                    return cleanup(fail(HF_ERR_CUDA, "velocity slots"));
+            }
+            UP((uint32_t **)&P.vflags[d], pg->vel_flags[d], pg->nfacet[d]);
+            UP((uint16_t **)&P.vdelta[d], pg->vel_delta[d], pg->nfacet[d]);
+        }
+        P.nvrows = (int)ptmpl.size();
+        P.vrow.tptr = P.rows.tptr;
+        P.vrow.col = P.rows.col;
+        P.vrow.w = P.rows.w;
+        UP((int32_t **)&P.vrow.tmpl, ptmpl.data(), ptmpl.size());
+        UP((int32_t **)&P.vrow.base, pbase.data(), pbase.size());
+        UP((double **)&P.vrow.rhs, prhs.data(), prhs.size());
+        UP((uint8_t **)&P.vtag, ptag.data(), ptag.size());
+        UP(&P.rowval, (const double *)nullptr, ptmpl.size());
     }
     UP((int32_t **)&P.dslots, pg->div_slots, (size_t)2 * D * pg->ncell);
     UP((uint16_t **)&P.cdelta, pg->cell_delta, pg->ncell);

@@ -396,8 +396,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
     }
 }
 
-// x += alpha p ; r -= alpha q ; convergence on ||r||.  With set_cond, the last
-// block of the grid sets the loop condition for the next body.
+// x += alpha p ; r -= alpha q ; convergence on ||r||.  set_cond != 0: the last
+// block of the grid counts the loop body and (set_cond == 1, inside the step
+// graph) sets the loop condition for the next body; with eager launches the
+// host reads the count and the active instances instead.
 __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *__restrict__ pn,
                                                        cudaGraphConditionalHandle cond, int set_cond)
 {
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *
             c.gcount = 0;
             c.bodies += 1;
             const int active = ((volatile Ctl *)G.ctl)->active;
-            cudaGraphSetConditional(cond, (active > 0 && c.bodies < c.maxbodies) ? 1u : 0u);
+            if (set_cond == 1) cudaGraphSetConditional(cond, (active > 0 && c.bodies < c.maxbodies) ? 1u : 0u);
         }
     }
 }

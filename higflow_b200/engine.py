@@ -67,11 +67,12 @@ def _check(rc: int) -> None:
 
 def options(precision: int = hp.PREC_FP64, poisson: int = hp.POISSON_AUTO, rtol: float = 1e-10,
             atol: float = 1e-10, maxit: int = 20000, device: int = 0,
-            precond: int = hp.PRECOND_AUTO) -> hp.HFOptions:
+            precond: int = hp.PRECOND_AUTO, eager: bool = False) -> hp.HFOptions:
     o = hp.HFOptions()
     o.precision, o.poisson = precision, poisson
     o.poisson_rtol, o.poisson_atol, o.poisson_maxit, o.device = rtol, atol, maxit, device
     o.precond = precond
+    o.eager = int(bool(eager))
     return o
 
 

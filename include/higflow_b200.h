@@ -258,6 +258,9 @@ typedef struct hf_options {
     int32_t poisson_maxit;    /* iteration cap; 0 = 20000                      */
     int32_t device;           /* CUDA device ordinal                          */
     int32_t precond;          /* HF_PRECOND_*                                 */
+    int32_t eager;            /* 0: each step is one CUDA graph launch; 1:    */
+                              /* kernels launched one by one with a host loop */
+                              /* over the iterations (kernel profilers)       */
 } hf_options;
 
 typedef struct hf_stats {

@@ -74,3 +74,22 @@ def test_mixed_precision_reaches_the_same_residual():
     it, outer, status, res = case.instance_result(0)
     assert status == 0 and res <= 1e-10 and outer >= 1
     case.close()
+
+
+def test_eager_launches_match_the_step_graph():
+    """The same kernels launched one by one (host-driven iteration loop) give
+    the graph's results bit for bit."""
+    names = VE_NAMES[:2]
+    progs, datas = zip(*[load_golden(n) for n in names])
+    batch = hp.Program.concatenate(progs)
+    out = []
+    for eager in (False, True):
+        case = engine.Case(batch, engine.options(rtol=1e-13, atol=1e-300, precision=hp.PREC_MIXED, eager=eager))
+        for key, fid, comp in field_keys(progs[0]):
+            case.set(fid, comp, np.concatenate([d["init_" + key] for d in datas]))
+        case.step(3)
+        out.append({k: case.get(fid, comp) for k, fid, comp in field_keys(progs[0])})
+        assert case.stats().total_iters > 0
+        case.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
