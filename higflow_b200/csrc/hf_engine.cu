@@ -901,6 +901,7 @@ struct hf_case {
     cudaStream_t body_stream = nullptr;
     cudaGraph_t graph[2] = {};
     cudaGraphExec_t exec[2] = {};
+    int64_t ntemplates = 0;         // row templates of the finest Poisson operator
     bool graph_profile = false;     // graphs were captured with phase events
     bool phase_pending = false;     // a profiled step's events are not read yet
     bool capturing = false;         // a step graph is being captured
@@ -1177,10 +1178,8 @@ LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
         o.Ac = ar.vec(h.Ac);
         o.b = ar.zeros<T>(h.n);
     }
-    if (!fine || !std::is_same<T, double>::value) {
-        o.Av = ar.vec(cast_vec<T>(h.Av));
-        o.dinv = ar.vec(cast_vec<T>(h.dinv));
-    }
+    if (!fine) o.Av = ar.vec(cast_vec<T>(h.Av));   // the finest level's operator is the row templates
+    if (!fine || !std::is_same<T, double>::value) o.dinv = ar.vec(cast_vec<T>(h.dinv));
     if (!h.Pp.empty()) {
         o.Pp = ar.vec(h.Pp); o.Pc = ar.vec(h.Pc); o.Pv = ar.vec(cast_vec<T>(h.Pv));
         o.Rp = ar.vec(h.Rp); o.Rc = ar.vec(h.Rc); o.Rv = ar.vec(cast_vec<T>(h.Rv));
@@ -1194,17 +1193,13 @@ LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
 }
 
 template <typename T>
-VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const DevMat &M, bool fine)
+VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const DevMat &M, const TRows<T> &At, bool fine)
 {
     VLev<T> v{};
     v.n = h.n;
     if (fine) {
-        v.Ap = M.ptr;
-        v.Ac = M.col;
-        if (std::is_same<T, double>::value) {
-            v.Av = (const T *)M.val;
-            v.dinv = (const T *)M.dinv;
-        }
+        v.At = At;
+        if (std::is_same<T, double>::value) v.dinv = (const T *)M.dinv;
     } else {
         v.Ap = (const int32_t *)(base + o.Ap);
         v.Ac = (const int32_t *)(base + o.Ac);
@@ -1235,7 +1230,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     const bool amg = C->amg, mixed = C->mixed;
     struct InstHier {
         std::vector<hf::HostLevel> H;
-        std::vector<double> inv;   // column-major
+        std::vector<double> inv;   // row-major
         std::string err;
     };
     std::vector<InstHier> IH(ni);
@@ -1266,9 +1261,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
                 if (cn > kCoarseCap) { ih.err = "AMG coarsening stalled above the dense-solve limit"; continue; }
                 std::vector<double> inv;
                 if (!hf::dense_inverse(last.A, inv)) { ih.err = "singular coarsest AMG level"; continue; }
-                ih.inv.resize(inv.size());
-                for (int r = 0; r < cn; r++)
-                    for (int c = 0; c < cn; c++) ih.inv[(size_t)c * cn + r] = inv[(size_t)r * cn + c];
+                ih.inv = std::move(inv);
             }
         };
         const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
@@ -1306,7 +1299,6 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
                 h.dinv.resize(h.n);
                 for (int i = 0; i < ni; i++)
                     std::copy(IH[i].H[0].dinv.begin(), IH[i].H[0].dinv.end(), h.dinv.begin() + off[0][i]);
-                h.Av = mval;
             }
         } else {
             h.Ap.assign(1, 0);
@@ -1408,6 +1400,38 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     std::vector<int32_t> ipin(pins.begin(), pins.end());
     const size_t o_pin = ar.vec(ipin);
     const size_t o_fblk = ar.vec(LH[0].ablk);
+    // the finest operator as row templates: rows with the same column offsets
+    // and values (in entry order) share one template
+    std::vector<int32_t> rt(n), tp(1, 0), toff;
+    std::vector<double> tval;
+    {
+        std::unordered_map<std::string, int32_t> seen;
+        std::string key;
+        for (int i = 0; i < n; i++) {
+            key.clear();
+            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
+                const int32_t o = mcol[k] - i;
+                key.append((const char *)&o, sizeof o);
+                key.append((const char *)&mval[k], sizeof(double));
+            }
+            auto it = seen.find(key);
+            if (it != seen.end()) {
+                rt[i] = it->second;
+                continue;
+            }
+            const int32_t t = (int32_t)tp.size() - 1;
+            seen.emplace(key, t);
+            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
+                toff.push_back(mcol[k] - i);
+                tval.push_back(mval[k]);
+            }
+            tp.push_back((int32_t)toff.size());
+            rt[i] = t;
+        }
+    }
+    const size_t o_rt = ar.vec(rt), o_tp = ar.vec(tp), o_toff = ar.vec(toff), o_tval = ar.vec(tval);
+    const size_t o_tval32 = mixed ? ar.vec(cast_vec<float>(tval)) : 0;
+    C->ntemplates = (int64_t)tp.size() - 1;
 
     char *base = nullptr;
     HF_CK(cudaMalloc((void **)&base, ar.host.size()));
@@ -1417,9 +1441,10 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
 
     PcgFine &G = C->G;
     G.n = n;
-    G.ptr = C->M.ptr;
-    G.col = C->M.col;
-    G.val = C->M.val;
+    G.A.rt = (const int32_t *)(base + o_rt);
+    G.A.tp = (const int32_t *)(base + o_tp);
+    G.A.toff = (const int32_t *)(base + o_toff);
+    G.A.tval = (const double *)(base + o_tval);
     G.dinv = C->M.dinv;
     G.apin = C->M.apin;
     G.brhs = C->M.brhs;
@@ -1443,8 +1468,12 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     C->pb = (double *)(base + o_pb);
     if (amg) {
         for (int l = 0; l < nlev; l++) {
-            if (mixed) C->L32[l] = make_level<float>(base, LO[l], LH[l], C->M, l == 0);
-            else C->L64[l] = make_level<double>(base, LO[l], LH[l], C->M, l == 0);
+            if (mixed) {
+                const TRows<float> At32{G.A.rt, G.A.tp, G.A.toff, (const float *)(base + o_tval32)};
+                C->L32[l] = make_level<float>(base, LO[l], LH[l], C->M, At32, l == 0);
+            } else {
+                C->L64[l] = make_level<double>(base, LO[l], LH[l], C->M, G.A, l == 0);
+            }
         }
         std::vector<CoarseInst<double>> c64(ni);
         std::vector<CoarseInst<float>> c32(ni);
@@ -2092,9 +2121,11 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     C->mixed = C->amg && opt.precision == HF_PREC_MIXED;
     DevMat &M = C->M;
     M.n = pg->ncell;
-    UP((int32_t **)&M.ptr, mptr.data(), mptr.size());
-    UP((int32_t **)&M.col, mcol.data(), mcol.size());
-    UP((double **)&M.val, mval.data(), mval.size());
+    if (!C->use_cg) {   // BiCGStab reads CSR; the CG path keeps the row templates
+        UP((int32_t **)&M.ptr, mptr.data(), mptr.size());
+        UP((int32_t **)&M.col, mcol.data(), mcol.size());
+        UP((double **)&M.val, mval.data(), mval.size());
+    }
     UP((double **)&M.dinv, dinv.data(), dinv.size());
     UP((double **)&M.apin, apin.data(), apin.size());
     UP((double **)&M.brhs, pg->p_brhs, pg->ncell);

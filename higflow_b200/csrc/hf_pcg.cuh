@@ -16,7 +16,7 @@
 // One CG iteration (hig-flow-step.c:48-131 solves the same system with PETSc's
 // KSP; the operator here is the reduced, negated SPD form built on the host):
 //   V-cycle  down: x = w D^-1 b, r = b - A x, b_next = R r     (per level)
-//            coarsest: x = inv b per instance (dense, column-major)
+//            coarsest: x = inv b per instance (dense)
 //            up:   x += P e, out = x + w D^-1 (b - A x)         (per level)
 //   z        finest post-smoothing writes z, r.z -> beta
 //   dir      p = z + beta p_old, q = A p, p.q -> alpha
@@ -64,11 +64,33 @@ struct Ctl {
     int64_t total_bodies;
 };
 
+// The finest operator as row templates: row i applies template rt[i], whose
+// entries k in [tp[t], tp[t+1]) are (column offset toff[k], value tval[k]).
+// On a uniform grid a handful of templates per instance cover every row, so a
+// row costs one 4-byte index instead of its CSR columns and values.
+template <typename T>
+struct TRows {
+    const int32_t *rt, *tp, *toff;
+    const T *tval;
+};
+
+// sum over row i of val_k * f(i + off_k), in the row's entry order
+template <typename T, typename Fn>
+__device__ __forceinline__ T trow(const TRows<T> &A, int i, Fn f)
+{
+    const int t = __ldg(A.rt + i);
+    const int e = __ldg(A.tp + t + 1);
+    T s = T(0);
+    for (int k = __ldg(A.tp + t); k < e; k++) s += __ldg(A.tval + k) * f(i + __ldg(A.toff + k));
+    return s;
+}
+
 template <typename T>
 struct VLev {
     int n;
-    const int32_t *Ap, *Ac;
+    const int32_t *Ap, *Ac;   // CSR on the coarse levels; the finest level uses At
     const T *Av, *dinv;
+    TRows<T> At;
     const int32_t *Pp, *Pc;   // rows: this level, columns: next level
     const T *Pv;
     const int32_t *Rp, *Rc;   // rows: next level, columns: this level
@@ -83,14 +105,14 @@ struct CoarseInst {
     const T *b;               // level b (nullptr on the finest level)
     const double *b64;        // the CG residual when the coarsest level is the finest
     T *out;
-    const T *inv;             // column-major cn x cn
+    const T *inv;             // row-major cn x cn
     int32_t inst, cn;
 };
 
 struct PcgFine {
     int n;
-    const int32_t *ptr, *col;
-    const double *val, *dinv, *apin, *brhs;
+    TRows<double> A;
+    const double *dinv, *apin, *brhs;
     const int32_t *ipin;      // per instance: pinned global row or -1
     const hf_params *ipar;
     double *p, *dp;           // unknown: dp (incremental projection) or p
@@ -223,8 +245,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
             borig = sumdudx / par.dt + G.brhs[cc];
         }
         const double bred = cc == pin ? pinv : -(borig - G.apin[cc] * pinv);
-        double ax = 0.0;
-        for (int k = G.ptr[cc]; k < G.ptr[cc + 1]; k++) ax += G.val[k] * x[G.col[k]];
+        const double ax = trow(G.A, cc, [&](int j) { return x[j]; });
         const double r = bred - ax;
         G.r[cc] = r;
         part[0] = r * r;
@@ -256,10 +277,13 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
     const T w = T(kSmoothW);
     const T bi = FINE ? T(r0[i]) : L.b[i];
     T s = T(0);
-    for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
-        const int j = L.Ac[k];
-        const T bj = FINE ? T(r0[j]) : L.b[j];
-        s += L.Av[k] * (w * L.dinv[j] * bj);
+    if (FINE) {
+        s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+    } else {
+        for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
+            const int j = L.Ac[k];
+            s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+        }
     }
     L.x[i] = w * L.dinv[i] * bi;
     L.r[i] = bi - s;
@@ -277,7 +301,9 @@ __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, c
     Ln.b[i] = s;
 }
 
-// out = inv b on each instance's coarsest level; one block per instance
+// out = inv b on each instance's coarsest level; one block per instance, one
+// warp per row at a time: the lanes split the row (row-major, coalesced) and
+// add their partial sums in a fixed shuffle order
 template <typename T>
 __global__ void __launch_bounds__(kCoarseThreads) k_vc_coarse(const CoarseInst<T> *ci, const IScal *S)
 {
@@ -292,10 +318,14 @@ __global__ void __launch_bounds__(kCoarseThreads) k_vc_coarse(const CoarseInst<T
     if (done) return;
     for (int i = threadIdx.x; i < c.cn; i += kCoarseThreads) sb[i] = c.b64 ? T(c.b64[i]) : c.b[i];
     __syncthreads();
-    for (int i = threadIdx.x; i < c.cn; i += kCoarseThreads) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < c.cn; i += kCoarseThreads / 32) {
+        const T *row = c.inv + (size_t)i * c.cn;
         T s = T(0);
-        for (int k = 0; k < c.cn; k++) s += c.inv[(size_t)k * c.cn + i] * sb[k];
-        c.out[i] = s;
+        for (int k = lane; k < c.cn; k += 32) s += row[k] * sb[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) c.out[i] = s;
     }
 }
 
@@ -340,8 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
         } else if (G.S[B.inst].clev == 0) {
             z = double(L0.out[i]);
         } else {
-            T s = T(0);
-            for (int k = L0.Ap[i]; k < L0.Ap[i + 1]; k++) s += L0.Av[k] * L0.x[L0.Ac[k]];
+            const T s = trow(L0.At, i, [&](int j) { return L0.x[j]; });
             z = double(L0.x[i] + T(kSmoothW) * L0.dinv[i] * (T(ri) - s));
         }
         G.z[i] = z;
@@ -367,15 +396,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
     double part[1] = {0.0};
     if ((int)threadIdx.x < B.cnt) {
         const int i = B.row0 + threadIdx.x;
-        double q = 0.0, p;
+        double q, p;
         if (first) {
-            for (int k = G.ptr[i]; k < G.ptr[i + 1]; k++) q += G.val[k] * G.z[G.col[k]];
+            q = trow(G.A, i, [&](int j) { return G.z[j]; });
             p = G.z[i];
         } else {
-            for (int k = G.ptr[i]; k < G.ptr[i + 1]; k++) {
-                const int j = G.col[k];
-                q += G.val[k] * (G.z[j] + beta * po[j]);
-            }
+            q = trow(G.A, i, [&](int j) { return G.z[j] + beta * po[j]; });
             p = G.z[i] + beta * po[i];
         }
         pn[i] = p;
