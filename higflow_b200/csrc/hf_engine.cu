@@ -891,8 +891,12 @@ struct hf_case {
     int nlev = 1;                   // multigrid levels including the finest
     VLev<double> L64[kMaxLevels] = {};
     VLev<float> L32[kMaxLevels] = {};
-    CoarseInst<double> *c64 = nullptr;
-    CoarseInst<float> *c32 = nullptr;
+    int nreg = 0;                   // levels run by level-synchronous kernels (above every tail)
+    VLev<double> *h64 = nullptr;    // the level tables in device memory (tail kernel)
+    VLev<float> *h32 = nullptr;
+    TailInst<double> *t64 = nullptr;
+    TailInst<float> *t32 = nullptr;
+    int64_t coarse_rows = 0, coarse_dense = 0;
     std::vector<int64_t> lrows, lnnz_a, lnnz_p, lnnz_r;
     int body_kernels = 0;           // kernels of one loop body (two iterations)
     int fixed_kernels = 0;          // kernels of a step outside the loop
@@ -1152,19 +1156,25 @@ struct LevelOff {
     size_t Ap, Ac, Av, dinv, Pp, Pc, Pv, Rp, Rc, Rv, b, x, r, out, sblk, ablk;
 };
 
-// Blocks of kBlock rows over the instances present on level l (smooth_only:
-// instances that are smoothed there, i.e. whose coarsest level is deeper).
-std::vector<Blk> block_table(const std::vector<std::vector<int>> &off, const std::vector<int> &clev, int l,
+// Blocks of kBlock rows over the instances a level-synchronous kernel of level
+// l covers: smooth_only, the instances smoothed there by those kernels (l below
+// the instance's tail level s); otherwise every instance on the finest level
+// and, on a coarser level, those whose rows the regular restriction fills
+// (l up to s).
+// Blocks hold kBlockRows rows (kRPT per thread) on levels large enough to
+// fill the device several times over, kBlock rows (one per thread) below that.
+std::vector<Blk> block_table(const std::vector<std::vector<int>> &off, const std::vector<int> &tail, int l,
                              bool smooth_only)
 {
     std::vector<Blk> t;
-    const int ni = (int)clev.size();
+    const int ni = (int)tail.size();
+    const int chunk = off[l][ni] >= (1 << 19) ? kBlockRows : kBlock;
     for (int i = 0; i < ni; i++) {
-        if (clev[i] < l || (smooth_only && clev[i] == l)) continue;
+        if (smooth_only ? l >= tail[i] : (l > 0 && l > tail[i])) continue;
         const int r0 = off[l][i], rows = off[l][i + 1] - r0;
-        const int nb = (rows + kBlock - 1) / kBlock, first = (int)t.size();
+        const int nb = (rows + chunk - 1) / chunk, first = (int)t.size();
         for (int b = 0; b < nb; b++)
-            t.push_back(Blk{r0 + b * kBlock, std::min(kBlock, rows - b * kBlock), i, first, nb, 0, 0, 0});
+            t.push_back(Blk{r0 + b * chunk, std::min(chunk, rows - b * chunk), i, first, nb, 0, 0, 0});
     }
     return t;
 }
@@ -1284,6 +1294,17 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
             const int rows = l == 0 ? C->coff[i + 1] - C->coff[i] : (clev[i] >= l ? IH[i].H[l].A.n : 0);
             off[l][i + 1] = off[l][i] + rows;
         }
+    // tail level of every instance: its first level with at most kTailRows rows
+    // (the coarsest level always qualifies); the levels above it are run by the
+    // level-synchronous kernels
+    std::vector<int> tail(ni, 0);
+    C->nreg = 0;
+    for (int i = 0; i < ni && amg; i++) {
+        int s = 0;
+        while (s < clev[i] && off[s][i + 1] - off[s][i] > kTailRows) s++;
+        tail[i] = s;
+        C->nreg = std::max(C->nreg, s);
+    }
     std::vector<LevelHost> LH(nlev);
     C->lrows.assign(nlev, 0);
     C->lnnz_a.assign(nlev, 0);
@@ -1346,8 +1367,8 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
             C->lnnz_p[l] = (int64_t)h.Pc.size();
             C->lnnz_r[l] = (int64_t)h.Rc.size();
         }
-        h.sblk = block_table(off, clev, l, true);
-        h.ablk = block_table(off, clev, l, false);
+        h.sblk = block_table(off, tail, l, true);
+        h.ablk = block_table(off, tail, l, false);
     }
 
     // every index the kernels follow must stay inside its array
@@ -1364,12 +1385,14 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         if (ok && l + 1 < nlev) ok = cols_ok(h.Pp, h.Pc, h.n, nn) && cols_ok(h.Rp, h.Rc, nn, h.n);
         for (const std::vector<Blk> *t : {&h.sblk, &h.ablk})
             for (const Blk &b : *t)
-                if (b.row0 < 0 || b.cnt <= 0 || b.cnt > kBlock || b.row0 + b.cnt > h.n) ok = false;
+                if (b.row0 < 0 || b.cnt <= 0 || b.cnt > kBlockRows || b.row0 + b.cnt > h.n) ok = false;
         if (!ok) return fail(HF_ERR_INVALID, "inconsistent multigrid level " + std::to_string(l));
     }
-    for (int i = 0; i < ni && amg; i++)
+    for (int i = 0; i < ni && amg; i++) {
         if (off[clev[i]][i + 1] > LH[clev[i]].n || off[clev[i]][i + 1] - off[clev[i]][i] > kCoarseCap)
             return fail(HF_ERR_INVALID, "inconsistent coarsest level");
+        if (tail[i] > clev[i] || clev[i] >= kMaxLevels) return fail(HF_ERR_INVALID, "inconsistent tail level");
+    }
 
     // device arena: hierarchy (in the V-cycle's precision), dense inverses,
     // CG vectors, partial sums, instance scalars and loop control
@@ -1390,7 +1413,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     std::vector<IScal> S(ni);
     for (int i = 0; i < ni; i++) {
         memset(&S[i], 0, sizeof(IScal));
-        S[i].clev = clev[i];
+        S[i].tail0 = amg && tail[i] == 0;
         S[i].done = 1;
     }
     const size_t o_S = ar.vec(S);
@@ -1402,13 +1425,16 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     const size_t o_fblk = ar.vec(LH[0].ablk);
     // the finest operator as row templates: rows with the same column offsets
     // and values (in entry order) share one template
-    std::vector<int32_t> rt(n), tp(1, 0), toff;
+    std::vector<uint32_t> rd(n);
+    std::vector<int32_t> tp(1, 0), toff;
     std::vector<double> tval;
     {
-        std::unordered_map<std::string, int32_t> seen;
+        std::unordered_map<std::string, uint32_t> seen;
         std::string key;
         for (int i = 0; i < n; i++) {
             key.clear();
+            const int len = mptr[i + 1] - mptr[i];
+            if (len >= (1 << kTLenBits)) return fail(HF_ERR_UNSUPPORTED, "Poisson row with more than 63 entries");
             for (int k = mptr[i]; k < mptr[i + 1]; k++) {
                 const int32_t o = mcol[k] - i;
                 key.append((const char *)&o, sizeof o);
@@ -1416,20 +1442,22 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
             }
             auto it = seen.find(key);
             if (it != seen.end()) {
-                rt[i] = it->second;
+                rd[i] = it->second;
                 continue;
             }
-            const int32_t t = (int32_t)tp.size() - 1;
-            seen.emplace(key, t);
+            if (toff.size() + len >= ((size_t)1 << (32 - kTLenBits)))
+                return fail(HF_ERR_UNSUPPORTED, "too many distinct Poisson rows for the template table");
+            const uint32_t d = ((uint32_t)toff.size() << kTLenBits) | (uint32_t)len;
+            seen.emplace(key, d);
             for (int k = mptr[i]; k < mptr[i + 1]; k++) {
                 toff.push_back(mcol[k] - i);
                 tval.push_back(mval[k]);
             }
             tp.push_back((int32_t)toff.size());
-            rt[i] = t;
+            rd[i] = d;
         }
     }
-    const size_t o_rt = ar.vec(rt), o_tp = ar.vec(tp), o_toff = ar.vec(toff), o_tval = ar.vec(tval);
+    const size_t o_rd = ar.vec(rd), o_toff = ar.vec(toff), o_tval = ar.vec(tval);
     const size_t o_tval32 = mixed ? ar.vec(cast_vec<float>(tval)) : 0;
     C->ntemplates = (int64_t)tp.size() - 1;
 
@@ -1441,8 +1469,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
 
     PcgFine &G = C->G;
     G.n = n;
-    G.A.rt = (const int32_t *)(base + o_rt);
-    G.A.tp = (const int32_t *)(base + o_tp);
+    G.A.rd = (const uint32_t *)(base + o_rd);
     G.A.toff = (const int32_t *)(base + o_toff);
     G.A.tval = (const double *)(base + o_tval);
     G.dinv = C->M.dinv;
@@ -1469,36 +1496,43 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     if (amg) {
         for (int l = 0; l < nlev; l++) {
             if (mixed) {
-                const TRows<float> At32{G.A.rt, G.A.tp, G.A.toff, (const float *)(base + o_tval32)};
+                const TRows<float> At32{G.A.rd, G.A.toff, (const float *)(base + o_tval32)};
                 C->L32[l] = make_level<float>(base, LO[l], LH[l], C->M, At32, l == 0);
             } else {
                 C->L64[l] = make_level<double>(base, LO[l], LH[l], C->M, G.A, l == 0);
             }
         }
-        std::vector<CoarseInst<double>> c64(ni);
-        std::vector<CoarseInst<float>> c32(ni);
+        // the per-instance tails: level table and row ranges
+        std::vector<TailInst<double>> t64(ni);
+        std::vector<TailInst<float>> t32(ni);
+        C->coarse_rows = 0;
+        C->coarse_dense = 0;
         for (int i = 0; i < ni; i++) {
-            const int l = clev[i], r0 = off[l][i], cn = off[l][i + 1] - r0;
-            CoarseInst<double> &a = c64[i];
-            CoarseInst<float> &b = c32[i];
+            TailInst<double> &a = t64[i];
+            TailInst<float> &b = t32[i];
+            memset(&a, 0, sizeof a);
+            memset(&b, 0, sizeof b);
             a.inst = b.inst = i;
-            a.cn = b.cn = cn;
-            a.b64 = b.b64 = l == 0 ? G.r + r0 : nullptr;
-            if (mixed) {
-                b.b = l == 0 ? nullptr : C->L32[l].b + r0;
-                b.out = C->L32[l].out + r0;
-                b.inv = (const float *)(base + inv_off[i]);
-            } else {
-                a.b = l == 0 ? nullptr : C->L64[l].b + r0;
-                a.out = C->L64[l].out + r0;
-                a.inv = (const double *)(base + inv_off[i]);
+            a.s = b.s = tail[i];
+            a.clev = b.clev = clev[i];
+            for (int l = 0; l <= clev[i]; l++) {
+                a.row0[l] = b.row0[l] = off[l][i];
+                a.nrow[l] = b.nrow[l] = off[l][i + 1] - off[l][i];
             }
+            a.inv = mixed ? nullptr : (const double *)(base + inv_off[i]);
+            b.inv = mixed ? (const float *)(base + inv_off[i]) : nullptr;
+            const int64_t cn = a.nrow[clev[i]];
+            C->coarse_rows += cn;
+            C->coarse_dense += cn * cn;
         }
         double bytes = 0;
         int rc;
         if (mixed) {
-            if ((rc = upload(C->owned, &C->c32, c32.data(), c32.size(), bytes))) return rc;
-        } else if ((rc = upload(C->owned, &C->c64, c64.data(), c64.size(), bytes))) {
+            if ((rc = upload(C->owned, &C->t32, t32.data(), t32.size(), bytes)) ||
+                (rc = upload(C->owned, &C->h32, C->L32, (size_t)nlev, bytes)))
+                return rc;
+        } else if ((rc = upload(C->owned, &C->t64, t64.data(), t64.size(), bytes)) ||
+                   (rc = upload(C->owned, &C->h64, C->L64, (size_t)nlev, bytes))) {
             return rc;
         }
         C->bytes += bytes;
@@ -1512,11 +1546,13 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
 // one time step as a CUDA graph
 // ---------------------------------------------------------------------------
 template <typename T>
-void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const CoarseInst<T> *ci, int &kernels)
+void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T> *H, const TailInst<T> *ti,
+                    int &kernels)
 {
     const IScal *S = C->G.S;
     const double *r0 = C->G.r;
-    for (int l = 0; l + 1 < C->nlev; l++) {
+    // the large levels, every instance at once, down to each instance's tail
+    for (int l = 0; l < C->nreg; l++) {
         if (L[l].nsblk) {
             if (l == 0) k_vc_down<T, true><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
             else k_vc_down<T, false><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
@@ -1527,9 +1563,10 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const CoarseI
             kernels++;
         }
     }
-    k_vc_coarse<T><<<C->ninst, kCoarseThreads, 0, st>>>(ci, S);
+    // the small levels: one CTA per instance
+    k_vc_tail<T><<<C->ninst, kTailThreads, 0, st>>>(H, ti, r0, S);
     kernels++;
-    for (int l = C->nlev - 2; l >= 0; l--) {
+    for (int l = C->nreg - 1; l >= 0; l--) {
         if (!L[l].nsblk) continue;
         k_vc_prolong<T><<<L[l].nsblk, kBlock, 0, st>>>(L[l], L[l + 1].out, S);
         kernels++;
@@ -1551,9 +1588,9 @@ void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, 
             k_pcg_z<double, true><<<C->G.nblk, kBlock, 0, st>>>(C->G, VLev<double>{});
             kernels++;
         } else if (C->mixed) {
-            enqueue_vcycle<float>(C, st, C->L32, C->c32, kernels);
+            enqueue_vcycle<float>(C, st, C->L32, C->h32, C->t32, kernels);
         } else {
-            enqueue_vcycle<double>(C, st, C->L64, C->c64, kernels);
+            enqueue_vcycle<double>(C, st, C->L64, C->h64, C->t64, kernels);
         }
         double *po = it == 0 ? C->pa : C->pb, *pn = it == 0 ? C->pb : C->pa;
         k_pcg_dir<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
@@ -2317,18 +2354,7 @@ extern "C" int hf_case_solver_info(hf_case *C, int32_t *method, int32_t *nlev, i
     }
     // the concatenated levels, then one entry for the dense coarsest solves
     *nlev = C->nlev + 1;
-    int64_t crows = 0, cdense = 0;
-    std::vector<CoarseInst<double>> c64;
-    std::vector<CoarseInst<float>> c32;
-    if (C->mixed) {
-        c32.resize(C->ninst);
-        HF_CK(cudaMemcpy(c32.data(), C->c32, sizeof(CoarseInst<float>) * C->ninst, cudaMemcpyDeviceToHost));
-        for (auto &c : c32) { crows += c.cn; cdense += (int64_t)c.cn * c.cn; }
-    } else {
-        c64.resize(C->ninst);
-        HF_CK(cudaMemcpy(c64.data(), C->c64, sizeof(CoarseInst<double>) * C->ninst, cudaMemcpyDeviceToHost));
-        for (auto &c : c64) { crows += c.cn; cdense += (int64_t)c.cn * c.cn; }
-    }
+    const int64_t crows = C->coarse_rows, cdense = C->coarse_dense;
     for (int l = 0; l < *nlev && l < max_levels; l++) {
         const bool dense = l == C->nlev;
         if (rows) rows[l] = dense ? crows : C->lrows[l];

@@ -36,10 +36,15 @@
 constexpr int kMaxLevels = 16;       // multigrid levels including the finest
 constexpr int kMaxCoarse = 128;      // rows of the coarsest level (dense inverse)
 constexpr int kCoarseCap = 1024;     // largest coarsest level accepted (stalled coarsening)
-constexpr int kCoarseThreads = 128;
 
-// rows [row0, row0 + cnt) of instance inst at one level; first/nblk: the
-// instance's block range in the same table (for reductions)
+// Every level-synchronous kernel gives each thread kRPT rows of its block
+// (rows row0 + threadIdx.x + q * kBlock): their independent load chains
+// overlap, and a block's fixed costs (descriptor, reduction) are shared.
+constexpr int kRPT = 4;
+constexpr int kBlockRows = kBlock * kRPT;
+
+// rows [row0, row0 + cnt) of instance inst at one level (cnt <= kBlockRows);
+// first/nblk: the instance's block range in the same table (for reductions)
 struct Blk {
     int32_t row0, cnt, inst, first, nblk, pad0, pad1, pad2;
 };
@@ -47,7 +52,7 @@ struct Blk {
 // Krylov state of one instance
 struct IScal {
     double rz, alpha, beta, rr, bb, tol2;
-    int32_t iters, status, done, clev;   // clev: the instance's coarsest level
+    int32_t iters, status, done, tail0;  // tail0: the whole V-cycle is the tail (s = 0)
     uint32_t counter, pad;
     int64_t total_iters;
 };
@@ -64,13 +69,18 @@ struct Ctl {
     int64_t total_bodies;
 };
 
-// The finest operator as row templates: row i applies template rt[i], whose
-// entries k in [tp[t], tp[t+1]) are (column offset toff[k], value tval[k]).
-// On a uniform grid a handful of templates per instance cover every row, so a
-// row costs one 4-byte index instead of its CSR columns and values.
+// The finest operator as row templates: row i applies the template described
+// by rd[i] = (first entry << kTLenBits) | entry count, whose entries are
+// (column offset toff[k], value tval[k]).  On a uniform grid a handful of
+// templates per instance cover every row, so a row costs one 4-byte word
+// instead of its CSR columns and values (and one dependent load less than a
+// template index would).
+constexpr int kTLenBits = 6;   // rows of up to 63 entries
+
 template <typename T>
 struct TRows {
-    const int32_t *rt, *tp, *toff;
+    const uint32_t *rd;
+    const int32_t *toff;
     const T *tval;
 };
 
@@ -78,10 +88,10 @@ struct TRows {
 template <typename T, typename Fn>
 __device__ __forceinline__ T trow(const TRows<T> &A, int i, Fn f)
 {
-    const int t = __ldg(A.rt + i);
-    const int e = __ldg(A.tp + t + 1);
+    const uint32_t d = __ldg(A.rd + i);
+    const int k0 = (int)(d >> kTLenBits), e = k0 + (int)(d & ((1u << kTLenBits) - 1));
     T s = T(0);
-    for (int k = __ldg(A.tp + t); k < e; k++) s += __ldg(A.tval + k) * f(i + __ldg(A.toff + k));
+    for (int k = k0; k < e; k++) s += __ldg(A.tval + k) * f(i + __ldg(A.toff + k));
     return s;
 }
 
@@ -100,13 +110,17 @@ struct VLev {
     int nsblk, nablk;
 };
 
+// The small levels of one instance, from the first level with at most
+// kTailRows rows (s) down to its coarsest (clev, dense inverse), run by one
+// CTA: phases separated by __syncthreads instead of kernel launches.
+constexpr int kTailRows = 1024;
+constexpr int kTailThreads = 512;
+
 template <typename T>
-struct CoarseInst {
-    const T *b;               // level b (nullptr on the finest level)
-    const double *b64;        // the CG residual when the coarsest level is the finest
-    T *out;
-    const T *inv;             // row-major cn x cn
-    int32_t inst, cn;
+struct TailInst {
+    const T *inv;             // row-major cn x cn, cn = nrow[clev]
+    int32_t inst, s, clev, pad;
+    int32_t row0[kMaxLevels], nrow[kMaxLevels];   // the instance's rows on each level
 };
 
 struct PcgFine {
@@ -228,8 +242,11 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
     const double pinv = pin >= 0 ? (incr ? P.ipinv[B.inst] - F.p[pin] : P.ipinv[B.inst]) : 0.0;
     const int n = P.ncell;
     double part[2] = {0.0, 0.0};   // r.r, b.b
-    if ((int)threadIdx.x < B.cnt) {
-        const int cc = B.row0 + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int cc = B.row0 + t;
         double borig;
         if (cc == pin) {
             borig = pinv;
@@ -248,8 +265,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
         const double ax = trow(G.A, cc, [&](int j) { return x[j]; });
         const double r = bred - ax;
         G.r[cc] = r;
-        part[0] = r * r;
-        part[1] = borig * borig;
+        part[0] += r * r;
+        part[1] += borig * borig;
     }
     double tot[2];
     if (pcg::inst_sum<2>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
@@ -272,21 +289,26 @@ template <typename T, bool FINE>
 __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__restrict__ r0, const IScal *S)
 {
     Blk B;
-    if (pcg::load_blk(L.sblk, S, B) || (int)threadIdx.x >= B.cnt) return;
-    const int i = B.row0 + threadIdx.x;
+    if (pcg::load_blk(L.sblk, S, B)) return;
     const T w = T(kSmoothW);
-    const T bi = FINE ? T(r0[i]) : L.b[i];
-    T s = T(0);
-    if (FINE) {
-        s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
-    } else {
-        for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
-            const int j = L.Ac[k];
-            s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        const T bi = FINE ? T(r0[i]) : L.b[i];
+        T s = T(0);
+        if (FINE) {
+            s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+        } else {
+            for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
+                const int j = L.Ac[k];
+                s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+            }
         }
+        L.x[i] = w * L.dinv[i] * bi;
+        L.r[i] = bi - s;
     }
-    L.x[i] = w * L.dinv[i] * bi;
-    L.r[i] = bi - s;
 }
 
 // b_next = R r on every row of the next level
@@ -294,38 +316,118 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, const IScal *S)
 {
     Blk B;
-    if (pcg::load_blk(Ln.ablk, S, B) || (int)threadIdx.x >= B.cnt) return;
-    const int i = B.row0 + threadIdx.x;
-    T s = T(0);
-    for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
-    Ln.b[i] = s;
+    if (pcg::load_blk(Ln.ablk, S, B)) return;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        T s = T(0);
+        for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
+        Ln.b[i] = s;
+    }
 }
 
-// out = inv b on each instance's coarsest level; one block per instance, one
-// warp per row at a time: the lanes split the row (row-major, coalesced) and
-// add their partial sums in a fixed shuffle order
+// The V-cycle of one instance from its tail level s down to its coarsest level
+// and back, one CTA per instance (H: the level table in device memory; levels
+// are copied to shared memory one at a time, a dynamic index into the kernel
+// parameters would spill them).  Level s's b is the regular restriction's
+// output (or the CG residual when s is the finest level); level s's out is the
+// correction the regular prolongation reads.  Same arithmetic as the
+// level-synchronous kernels; the dense solve splits each row over a warp.
 template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads) k_vc_coarse(const CoarseInst<T> *ci, const IScal *S)
+__global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, const TailInst<T> *TI,
+                                                        const double *__restrict__ r0, const IScal *S)
 {
-    __shared__ T sb[kCoarseCap];
-    __shared__ CoarseInst<T> c;
+    __shared__ TailInst<T> ti;
+    __shared__ VLev<T> L, Ln;
     __shared__ int done;
+    __shared__ T sb[kCoarseCap];
     if (threadIdx.x == 0) {
-        c = ci[blockIdx.x];
-        done = ((volatile const IScal *)S)[c.inst].done;
+        ti = TI[blockIdx.x];
+        done = ((volatile const IScal *)S)[ti.inst].done;
     }
     __syncthreads();
     if (done) return;
-    for (int i = threadIdx.x; i < c.cn; i += kCoarseThreads) sb[i] = c.b64 ? T(c.b64[i]) : c.b[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = warp; i < c.cn; i += kCoarseThreads / 32) {
-        const T *row = c.inv + (size_t)i * c.cn;
-        T s = T(0);
-        for (int k = lane; k < c.cn; k += 32) s += row[k] * sb[k];
+    const T w = T(kSmoothW);
+    const int tid = threadIdx.x;
+    // down: x = w D^-1 b, r = b - A x, b_next = R r
+    for (int l = ti.s; l < ti.clev; l++) {
+        if (tid == 0) {
+            L = H[l];
+            Ln = H[l + 1];
+        }
+        __syncthreads();
+        const int a = ti.row0[l], e = a + ti.nrow[l];
+        for (int i = a + tid; i < e; i += kTailThreads) {
+            T bi, s = T(0);
+            if (l == 0) {
+                bi = T(r0[i]);
+                s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+            } else {
+                bi = L.b[i];
+                for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
+                    const int j = L.Ac[k];
+                    s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+                }
+            }
+            L.x[i] = w * L.dinv[i] * bi;
+            L.r[i] = bi - s;
+        }
+        __syncthreads();
+        const int an = ti.row0[l + 1], en = an + ti.nrow[l + 1];
+        for (int i = an + tid; i < en; i += kTailThreads) {
+            T s = T(0);
+            for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
+            Ln.b[i] = s;
+        }
+        __syncthreads();
+    }
+    // coarsest: out = inv b, one warp per row, lanes over the row
+    {
+        if (tid == 0) L = H[ti.clev];
+        __syncthreads();
+        const int a = ti.row0[ti.clev], cn = ti.nrow[ti.clev];
+        for (int i = tid; i < cn; i += kTailThreads) sb[i] = ti.clev == 0 ? T(r0[a + i]) : L.b[a + i];
+        __syncthreads();
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int i = warp; i < cn; i += kTailThreads / 32) {
+            const T *row = ti.inv + (size_t)i * cn;
+            T s = T(0);
+            for (int k = lane; k < cn; k += 32) s += row[k] * sb[k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) c.out[i] = s;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) L.out[a + i] = s;
+        }
+        __syncthreads();
+    }
+    // up: x += P e, out = x + w D^-1 (b - A x)
+    for (int l = ti.clev - 1; l >= ti.s; l--) {
+        if (tid == 0) {
+            L = H[l];
+            Ln = H[l + 1];
+        }
+        __syncthreads();
+        const int a = ti.row0[l], e = a + ti.nrow[l];
+        for (int i = a + tid; i < e; i += kTailThreads) {
+            T s = T(0);
+            for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * Ln.out[L.Pc[k]];
+            L.x[i] += s;
+        }
+        __syncthreads();
+        for (int i = a + tid; i < e; i += kTailThreads) {
+            T bi, s;
+            if (l == 0) {
+                bi = T(r0[i]);
+                s = trow(L.At, i, [&](int j) { return L.x[j]; });
+            } else {
+                bi = L.b[i];
+                s = T(0);
+                for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
+            }
+            L.out[i] = L.x[i] + w * L.dinv[i] * (bi - s);
+        }
+        __syncthreads();
     }
 }
 
@@ -334,11 +436,16 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_prolong(VLev<T> L, const T *__restrict__ e, const IScal *S)
 {
     Blk B;
-    if (pcg::load_blk(L.sblk, S, B) || (int)threadIdx.x >= B.cnt) return;
-    const int i = B.row0 + threadIdx.x;
-    T s = T(0);
-    for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * e[L.Pc[k]];
-    L.x[i] += s;
+    if (pcg::load_blk(L.sblk, S, B)) return;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        T s = T(0);
+        for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * e[L.Pc[k]];
+        L.x[i] += s;
+    }
 }
 
 // out = x + w D^-1 (b - A x) on the smoothed rows of a coarse level
@@ -346,35 +453,44 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_post(VLev<T> L, const IScal *S)
 {
     Blk B;
-    if (pcg::load_blk(L.sblk, S, B) || (int)threadIdx.x >= B.cnt) return;
-    const int i = B.row0 + threadIdx.x;
-    T s = T(0);
-    for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
-    L.out[i] = L.x[i] + T(kSmoothW) * L.dinv[i] * (L.b[i] - s);
+    if (pcg::load_blk(L.sblk, S, B)) return;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        T s = T(0);
+        for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
+        L.out[i] = L.x[i] + T(kSmoothW) * L.dinv[i] * (L.b[i] - s);
+    }
 }
 
-// z on the finest level (post-smoothing, the dense solve's output, or D^-1 r),
-// then r.z -> beta per instance
+// z on the finest level (post-smoothing, the tail's output, or D^-1 r), then
+// r.z -> beta per instance
 template <typename T, bool JACOBI>
 __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
 {
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
+    const bool tail0 = G.S[B.inst].tail0;
     double part[1] = {0.0};
-    if ((int)threadIdx.x < B.cnt) {
-        const int i = B.row0 + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
         const double ri = G.r[i];
         double z;
         if (JACOBI) {
             z = G.dinv[i] * ri;
-        } else if (G.S[B.inst].clev == 0) {
+        } else if (tail0) {
             z = double(L0.out[i]);
         } else {
             const T s = trow(L0.At, i, [&](int j) { return L0.x[j]; });
             z = double(L0.x[i] + T(kSmoothW) * L0.dinv[i] * (T(ri) - s));
         }
         G.z[i] = z;
-        part[0] = ri * z;
+        part[0] += ri * z;
     }
     double tot[1];
     if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
@@ -394,19 +510,22 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
     const bool first = sc.iters == 0;
     const double beta = sc.beta;
     double part[1] = {0.0};
-    if ((int)threadIdx.x < B.cnt) {
-        const int i = B.row0 + threadIdx.x;
-        double q, p;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        double qi, p;
         if (first) {
-            q = trow(G.A, i, [&](int j) { return G.z[j]; });
+            qi = trow(G.A, i, [&](int j) { return G.z[j]; });
             p = G.z[i];
         } else {
-            q = trow(G.A, i, [&](int j) { return G.z[j] + beta * po[j]; });
+            qi = trow(G.A, i, [&](int j) { return G.z[j] + beta * po[j]; });
             p = G.z[i] + beta * po[i];
         }
         pn[i] = p;
-        G.q[i] = q;
-        part[0] = p * q;
+        G.q[i] = qi;
+        part[0] += p * qi;
     }
     double tot[1];
     if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
@@ -436,12 +555,15 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *
         double *x = incr ? G.dp : G.p;
         const double alpha = G.S[B.inst].alpha;
         double part[1] = {0.0};
-        if ((int)threadIdx.x < B.cnt) {
-            const int i = B.row0 + threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < kRPT; q++) {
+            const int t = threadIdx.x + q * kBlock;
+            if (t >= B.cnt) break;
+            const int i = B.row0 + t;
             x[i] += alpha * pn[i];
             const double r = G.r[i] - alpha * G.q[i];
             G.r[i] = r;
-            part[0] = r * r;
+            part[0] += r * r;
         }
         double tot[1];
         if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
