@@ -376,6 +376,9 @@ int hfref_solver_stats(hfref_case *C, int32_t *iters, double *residual)
 
 double hfref_time(hfref_case *C) { return C->ns->par.t; }
 
+/* the case's higflow_solver, for the drop-in binding (hf_attach & co.) */
+void *hfref_ns(hfref_case *C) { return C->ns; }
+
 /* flatten through the binding (hf_flatten) and hand the program to Python */
 int hfref_flatten(hfref_case *C, hf_program **out)
 {

@@ -68,6 +68,15 @@ def lib(dim: int) -> C.CDLL:
         L.hfref_last_system.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.hfref_last_system_copy.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.hfref_ns.argtypes = [C.c_void_p]
+        L.hfref_ns.restype = C.c_void_p
+        # the drop-in binding linked into the same library (product code under test)
+        L.hf_attach.argtypes = [C.c_void_p, C.POINTER(hp.HFOptions)]
+        L.hf_step.argtypes = [C.c_void_p]
+        L.hf_sync_to_host.argtypes = [C.c_void_p]
+        L.hf_detach.argtypes = [C.c_void_p]
+        L.hf_detach.restype = None
+        L.hf_last_error.restype = C.c_char_p
         _libs[dim] = L
     return _libs[dim]
 
@@ -176,6 +185,11 @@ class RefCase:
     @property
     def t(self) -> float:
         return self.L.hfref_time(self.h)
+
+    @property
+    def ns(self) -> int:
+        """The case's higflow_solver pointer (for the drop-in binding)."""
+        return self.L.hfref_ns(self.h)
 
     def fields(self, names: Optional[Sequence[str]] = None) -> Dict[str, np.ndarray]:
         out = {}
