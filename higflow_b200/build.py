@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "lib", "libhigflow_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("hf_engine.cu",)]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("hf_engine.cu", "hf_server.cpp")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("hf_device.cuh", "hf_amg.cuh", "hf_pcg.cuh")] + \
     [os.path.join(REPO, "include", "higflow_b200.h")]
 

@@ -188,3 +188,106 @@ def device_bytes(prog: hp.Program, opts: Optional[hp.HFOptions] = None) -> int:
     o = opts or options()
     _check(lib().hf_case_device_bytes(C.byref(cp), C.byref(o), C.byref(b)))
     return b.value
+
+
+# ---------------------------------------------------------------------------
+# serving (include/higflow_b200.h, hf_server_*)
+class HFServerOptions(C.Structure):
+    _fields_ = [("hbm_budget_gb", C.c_double), ("max_active", C.c_int32), ("chunk_steps", C.c_int32),
+                ("setup_threads", C.c_int32), ("device", C.c_int32)]
+
+
+class HFFieldData(C.Structure):
+    _fields_ = [("field", C.c_int32), ("comp", C.c_int32), ("data", C.POINTER(C.c_double)), ("n", C.c_int64)]
+
+
+class HFServerCounts(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64),
+                ("active", C.c_int64), ("reserved_bytes", C.c_int64), ("cell_steps", C.c_int64),
+                ("seconds", C.c_double)]
+
+
+def _server_lib() -> C.CDLL:
+    L = lib()
+    if not hasattr(L, "_server_ready"):
+        P, V = C.POINTER, C.c_void_p
+        L.hf_server_create.argtypes = [P(HFServerOptions), P(V)]
+        L.hf_server_submit.argtypes = [V, P(hp.HFProgram), P(hp.HFOptions), C.c_int32, P(HFFieldData), C.c_int32,
+                                       P(C.c_int64)]
+        L.hf_server_wait.argtypes = [V, C.c_int64, C.c_int32, P(C.c_int32), P(C.c_double), P(C.c_double)]
+        L.hf_server_get_field.argtypes = [V, C.c_int64, C.c_int32, C.c_int32, P(C.c_double), C.c_int64]
+        L.hf_server_release.argtypes = [V, C.c_int64]
+        L.hf_server_stats.argtypes = [V, P(HFServerCounts)]
+        L.hf_server_destroy.argtypes = [V]
+        L.hf_server_destroy.restype = None
+        L.hf_server_last_error.restype = C.c_char_p
+        L._server_ready = True
+    return L
+
+
+def _scheck(rc: int) -> None:
+    if rc != 0:
+        raise EngineError(rc, _server_lib().hf_server_last_error().decode(errors="replace"))
+
+
+class Server:
+    """Continuous batching of independent cases on one GPU (hf_server_*)."""
+
+    def __init__(self, budget_gb: float = 150.0, max_active: int = 64, chunk_steps: int = 16,
+                 setup_threads: int = 8, device: int = 0):
+        o = HFServerOptions(budget_gb, max_active, chunk_steps, setup_threads, device)
+        self.h = C.c_void_p()
+        _scheck(_server_lib().hf_server_create(C.byref(o), C.byref(self.h)))
+        self._sizes = {}
+
+    def submit(self, prog: hp.Program, opts: Optional[hp.HFOptions] = None, steps: int = 1,
+               fields: Optional[dict] = None) -> int:
+        """Queue a case; fields: {(field, comp): values}.  Returns its id."""
+        cp = prog.to_c()
+        fl = list((fields or {}).items())
+        arr = (HFFieldData * max(len(fl), 1))()
+        keep = []
+        for k, ((fid, comp), v) in enumerate(fl):
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            keep.append(v)
+            arr[k] = HFFieldData(fid, comp, v.ctypes.data_as(C.POINTER(C.c_double)), v.size)
+        rid = C.c_int64()
+        o = opts or options()
+        _scheck(_server_lib().hf_server_submit(self.h, C.byref(cp), C.byref(o), steps, arr, len(fl), C.byref(rid)))
+        self._sizes[rid.value] = prog
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """(status, queue seconds, submit-to-done seconds); None while still running."""
+        st, q, t = C.c_int32(), C.c_double(), C.c_double()
+        rc = _server_lib().hf_server_wait(self.h, rid, timeout_ms, C.byref(st), C.byref(q), C.byref(t))
+        if rc == -8:
+            return None
+        _scheck(rc)
+        return st.value, q.value, t.value
+
+    def get(self, rid: int, fid: int, comp: int = 0) -> np.ndarray:
+        out = np.empty(self._sizes[rid].field_size(fid, comp), dtype=np.float64)
+        _scheck(_server_lib().hf_server_get_field(self.h, rid, fid, comp,
+                                                  out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
+    def release(self, rid: int) -> None:
+        _scheck(_server_lib().hf_server_release(self.h, rid))
+        self._sizes.pop(rid, None)
+
+    def stats(self) -> HFServerCounts:
+        s = HFServerCounts()
+        _scheck(_server_lib().hf_server_stats(self.h, C.byref(s)))
+        return s
+
+    def close(self) -> None:
+        if self.h:
+            _server_lib().hf_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

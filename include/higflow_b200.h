@@ -337,6 +337,54 @@ int  hf_case_device_bytes(const hf_program *prog, const hf_options *opt, int64_t
 const char *hf_last_error(void);
 
 /* ------------------------------------------------------------------ */
+/* serving: continuous batching of independent cases on one device    */
+/* (no counterpart in the reference, which runs one case per job)      */
+/* ------------------------------------------------------------------ */
+typedef struct hf_server hf_server;
+
+typedef struct hf_server_options {
+    double  hbm_budget_gb;    /* device memory the admitted cases may hold; 0 = 150 */
+    int32_t max_active;       /* cases being created or stepped at once; 0 = 64     */
+    int32_t chunk_steps;      /* steps queued per case per dispatch; 0 = 16         */
+    int32_t setup_threads;    /* host threads creating admitted cases; 0 = 8        */
+    int32_t device;           /* CUDA device ordinal                               */
+} hf_server_options;
+
+typedef struct hf_field_data {
+    int32_t field, comp;      /* HF_FIELD_*, component                           */
+    const double *data;       /* host values, copied at submit                   */
+    int64_t n;
+} hf_field_data;
+
+typedef struct hf_server_counts {
+    int64_t submitted, completed, failed, queued, active;
+    int64_t reserved_bytes;   /* device memory held or reserved by admitted cases */
+    int64_t cell_steps;       /* cells x steps of the completed requests          */
+    double  seconds;          /* since hf_server_create                           */
+} hf_server_counts;
+
+/* Requests are admitted in arrival order while their device memory fits the
+ * budget, created on host threads, then stepped on their own CUDA streams
+ * (chunk_steps graph launches at a time) until done; fields stay on the device
+ * until hf_server_release.  Each request is an engine case of its own, so its
+ * result is the same alone and in any mix. */
+int  hf_server_create(const hf_server_options *opt, hf_server **out);
+/* Queue a case (program, options, initial fields, steps); copies everything. */
+int  hf_server_submit(hf_server *s, const hf_program *prog, const hf_options *opt, int32_t nsteps,
+                      const hf_field_data *fields, int32_t nfields, int64_t *id);
+/* Wait for a request (timeout_ms < 0: until done); HF_ERR_TIMEOUT if still
+ * running.  status: the request's own result; queue_s: submit to admission;
+ * total_s: submit to completion (time to solution). */
+int  hf_server_wait(hf_server *s, int64_t id, int32_t timeout_ms, int32_t *status, double *queue_s,
+                    double *total_s);
+int  hf_server_get_field(hf_server *s, int64_t id, int32_t field, int32_t comp, double *host, int64_t n);
+int  hf_server_release(hf_server *s, int64_t id);
+int  hf_server_stats(hf_server *s, hf_server_counts *out);
+/* Drops requests not yet admitted, waits for the admitted ones, frees all. */
+void hf_server_destroy(hf_server *s);
+const char *hf_server_last_error(void);
+
+/* ------------------------------------------------------------------ */
 /* linear-solver engine: one entry point per _solver_vtable slot       */
 /* (higtree/src/solver.h:42-87).  Row/column indices are global ids in */
 /* [first_gid, first_gid + size).                                      */
