@@ -342,6 +342,8 @@ def run_b200(args, rank, world, device):
     ninst = case.instances()
     e2e = None if args.no_extras else end_to_end(case, prog, args, world, device)
     case.close()
+    if wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras and not args.no_serve:
+        extra["served"] = served(args, device)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -372,6 +374,55 @@ def run_b200(args, rank, world, device):
     }
     line.update(extra)
     return line
+
+
+def served(args, device):
+    """The served stream on one device: the first 64 requests of the seeded
+    stream (Poisson arrivals at 50/s, 2D cavities N in logU[64, 512]; 40 %
+    Newtonian, 40 % Oldroyd-B, 20 % Giesekus), step counts scaled by 1/50,
+    submitted at their arrival times to an hf_server (150 GB budget).  Programs
+    are built before the clock starts (a request carries its program).
+    Time to solution = submission to completion, queueing included."""
+    from higflow_b200 import engine
+    from higflow_b200 import program as hp
+    from higflow_b200 import workloads
+    reqs = workloads.served_requests()
+    progs = [(workloads.program(c), c) for _, c in reqs]
+    srv = engine.Server(budget_gb=150.0, max_active=64, chunk_steps=16, setup_threads=8, device=device)
+    opts = engine.options(rtol=1e-10, atol=1e-300, device=device, precision=hp.PREC_MIXED)
+    ids = []
+    t0 = time.perf_counter()
+    for (t_arr, _), (prog, c) in zip(reqs, progs):
+        lag = t_arr - (time.perf_counter() - t0)
+        if lag > 0:
+            time.sleep(lag)
+        ids.append(srv.submit(prog, opts, c.steps))
+    tts, queue = [], []
+    failed, failures = 0, {}
+    for rid in ids:
+        status, q, t = srv.wait(rid)
+        if status != 0:
+            failed += 1
+            msg = engine._server_lib().hf_server_last_error().decode(errors="replace")
+            failures.setdefault(str(status), msg)
+        tts.append(t)
+        queue.append(q)
+        srv.release(rid)
+    makespan = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    cells = sum(p.ncell * c.steps for p, c in progs)
+    return {
+        "requests": len(ids), "failed": int(failed), "failures": failures, "solves_per_s": len(ids) / makespan,
+        "p50_s": float(np.percentile(tts, 50)), "p99_s": float(np.percentile(tts, 99)),
+        "queue_p50_s": float(np.percentile(queue, 50)), "queue_p99_s": float(np.percentile(queue, 99)),
+        "cell_steps_per_s": cells / makespan, "makespan_s": makespan, "arrival_window_s": reqs[-1][0],
+        "cell_steps": int(st.cell_steps),
+        "workload": "first 64 requests of the served stream (seed 0): Poisson arrivals 50/s, 2D lid-driven "
+                    "cavities N log-uniform [64,512], 40% Newtonian Re 100, 40% Oldroyd-B Wi U[0.1,1.5], 20% "
+                    "Giesekus (cavity geometry), steps U{500..5000} scaled by 1/50; mixed precision; HBM budget "
+                    "150 GB; up to 64 cases stepping at once, 16 steps per dispatch",
+    }
 
 
 def end_to_end(case, prog, args, world, device):
@@ -492,6 +543,7 @@ def main():
     ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU reference sample")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream run")
     ap.add_argument("--eager", action="store_true",
                     help="launch kernels one by one instead of one CUDA graph per step (kernel profilers)")
     ap.add_argument("--no-extras", action="store_true",

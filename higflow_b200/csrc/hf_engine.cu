@@ -856,16 +856,42 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
 int blocks(long n) { return (int)((n + kBlock - 1) / kBlock); }
 
 template <typename T>
-int upload(std::vector<void *> &owned, T **dst, const T *src, size_t n, double &bytes)
+int upload(std::vector<void *> &owned, T **dst, const T *src, size_t n, double &bytes, cudaStream_t st = nullptr)
 {
     *dst = nullptr;
     size_t nb = sizeof(T) * (n ? n : 1);
+    if (st) {
+        // stream-ordered: no device-wide synchronisation, so cases can be
+        // created and freed while others are stepping (or being captured)
+        HF_CK(cudaMallocAsync((void **)dst, nb, st));
+        owned.push_back(*dst);
+        bytes += (double)nb;
+        if (n && src) HF_CK(cudaMemcpyAsync(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+        else HF_CK(cudaMemsetAsync(*dst, 0, nb, st));
+        return HF_OK;
+    }
     HF_CK(cudaMalloc((void **)dst, nb));
     owned.push_back(*dst);
     bytes += (double)nb;
     if (n && src) HF_CK(cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice));
     else HF_CK(cudaMemset(*dst, 0, nb));
     return HF_OK;
+}
+
+// Freed stream-ordered memory stays in the device's default pool for the next
+// case instead of going back to the driver at every synchronisation.
+void keep_pool_memory(int dev)
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.push_back(dev);
 }
 
 }  // namespace
@@ -1462,10 +1488,11 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     C->ntemplates = (int64_t)tp.size() - 1;
 
     char *base = nullptr;
-    HF_CK(cudaMalloc((void **)&base, ar.host.size()));
+    HF_CK(cudaMallocAsync((void **)&base, ar.host.size(), C->stream));
     C->owned.push_back(base);
     C->bytes += (double)ar.host.size();
-    HF_CK(cudaMemcpy(base, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice));
+    HF_CK(cudaMemcpyAsync(base, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice, C->stream));
+    HF_CK(cudaStreamSynchronize(C->stream));   // the host arena goes away with this function
 
     PcgFine &G = C->G;
     G.n = n;
@@ -1528,17 +1555,17 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         double bytes = 0;
         int rc;
         if (mixed) {
-            if ((rc = upload(C->owned, &C->t32, t32.data(), t32.size(), bytes)) ||
-                (rc = upload(C->owned, &C->h32, C->L32, (size_t)nlev, bytes)))
+            if ((rc = upload(C->owned, &C->t32, t32.data(), t32.size(), bytes, C->stream)) ||
+                (rc = upload(C->owned, &C->h32, C->L32, (size_t)nlev, bytes, C->stream)))
                 return rc;
-        } else if ((rc = upload(C->owned, &C->t64, t64.data(), t64.size(), bytes)) ||
-                   (rc = upload(C->owned, &C->h64, C->L64, (size_t)nlev, bytes))) {
+        } else if ((rc = upload(C->owned, &C->t64, t64.data(), t64.size(), bytes, C->stream)) ||
+                   (rc = upload(C->owned, &C->h64, C->L64, (size_t)nlev, bytes, C->stream))) {
             return rc;
         }
         C->bytes += bytes;
     }
-    HF_CK(cudaMallocHost((void **)&C->h_S, sizeof(IScal) * ni));
-    HF_CK(cudaMallocHost((void **)&C->h_ctl, sizeof(Ctl)));
+    C->h_S = new IScal[ni]();
+    C->h_ctl = new Ctl();
     return HF_OK;
 }
 
@@ -1976,7 +2003,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&C->body_stream, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(HF_ERR_CUDA, "stream"));
-    if (cudaMallocHost((void **)&C->h_scal, sizeof(Scal)) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "pinned scalars"));
+    C->h_scal = new Scal();
+    keep_pool_memory(opt.device);
 
     DevProg &P = C->P;
     memset(&P, 0, sizeof P);
@@ -1993,7 +2021,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     P.cns = pg->cell_nslot;
     double &B = C->bytes;
     auto &own = C->owned;
-#define UP(dst, src, n) do { if ((rc = upload(own, dst, src, (size_t)(n), B))) return cleanup(rc); } while (0)
+#define UP(dst, src, n) do { if ((rc = upload(own, dst, src, (size_t)(n), B, C->stream))) return cleanup(rc); } while (0)
     // instances: a plain program is a batch of one
     std::vector<hf_params> ipar;
     std::vector<int> pins;
@@ -2102,8 +2130,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 for (int64_t f = 0; f < nf; f++)
                     if (row[f] < 0) row[f] = -pair_index(-(int64_t)row[f] - 1, tag) - 1;
                 if (overflow) return cleanup(fail(HF_ERR_UNSUPPORTED, "too many velocity-stage rows"));
-                if (cudaMemcpy((int32_t *)P.vslots[d] + (size_t)s * nf, row.data(), sizeof(int32_t) * nf,
-                               cudaMemcpyHostToDevice) != cudaSuccess)
+                if (cudaMemcpyAsync((int32_t *)P.vslots[d] + (size_t)s * nf, row.data(), sizeof(int32_t) * nf,
+                                    cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
                     return cleanup(fail(HF_ERR_CUDA, "velocity slots"));
             }
             UP((uint32_t **)&P.vflags[d], pg->vel_flags[d], pg->nfacet[d]);
@@ -2172,7 +2200,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     {
         Scal h{};
         h.maxit = opt.poisson_maxit;
-        if (cudaMemcpy(sc, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "scalars"));
+        if (cudaMemcpyAsync(sc, &h, sizeof h, cudaMemcpyHostToDevice, C->stream) != cudaSuccess)
+            return cleanup(fail(HF_ERR_CUDA, "scalars"));
     }
     double *partials = nullptr;
     UP(&partials, (const double *)nullptr, (size_t)nb * 4);
@@ -2195,7 +2224,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         V.sc = sc;
     }
 #undef UP
-    if (cudaDeviceSynchronize() != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "create sync"));
+    if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "create sync"));
     C->stats.device_bytes = C->bytes;
     *out = C;
     return HF_OK;
@@ -2411,10 +2440,10 @@ extern "C" void hf_case_destroy(hf_case *C)
     destroy_graphs(C);
     for (int k = 0; k < 2 * HF_NPHASE; k++)
         if (C->ev[k]) cudaEventDestroy(C->ev[k]);
-    for (void *p : C->owned) cudaFree(p);
-    if (C->h_scal) cudaFreeHost(C->h_scal);
-    if (C->h_S) cudaFreeHost(C->h_S);
-    if (C->h_ctl) cudaFreeHost(C->h_ctl);
+    for (void *p : C->owned) cudaFreeAsync(p, C->stream);
+    delete C->h_scal;
+    delete[] C->h_S;
+    delete C->h_ctl;
     if (C->body_stream) cudaStreamDestroy(C->body_stream);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;

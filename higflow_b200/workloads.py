@@ -83,6 +83,19 @@ def served_stream(seed: int = 0, rate: float = 50.0, window_s: float = 60.0):
     return times, cases
 
 
+def served_requests(count: int = 64, step_scale: float = 1.0 / 50.0, seed: int = 0):
+    """The first ``count`` requests of the served stream, step counts scaled by
+    ``step_scale`` (at least 1): [(arrival s, CaseDraw)].  The stream's offered
+    load (about 8.5e9 cell-steps/s) is far above one device; the bounded sample
+    keeps arrivals, sizes and the mix of the stream and makes the run finish."""
+    times, cases = served_stream(seed=seed)
+    out = []
+    for t, c in list(zip(times, cases))[:count]:
+        c = CaseDraw(**{**c.__dict__, "steps": max(1, int(round(c.steps * step_scale)))})
+        out.append((t, c))
+    return out
+
+
 _cache: Dict[tuple, hp.Program] = {}
 
 
