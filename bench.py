@@ -7,8 +7,9 @@ workload.  The default workload is the batched configuration: 256 independent
 2D Giesekus lid-driven cavities (side N log-uniform in [32, 256], seed 0) in one
 batch program, mixed precision; the same batch is also timed in plain FP64 and
 the mixed-vs-plain field error is reported.  With N GPUs every rank runs its own
-replica (the cases are independent; no collective on the data path) and
-``value`` is the cell-steps of all ranks over the slowest rank's device time.
+batch of the same population drawn with seed = rank (independent instances; no
+collective on the data path) and ``value`` is the cell-steps of all ranks over
+the slowest rank's device time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c1|cav2d_1024]
   python bench.py --impl reference ...   # the reference's own CPU step
@@ -61,11 +62,17 @@ WORKLOADS = {
 }
 
 
-def load_program(wl):
+def rank_seed(rank):
+    """Seed of rank r's batch: every GPU draws its own population (shards of
+    independent instances, the per-GPU work fixed as the GPU count grows)."""
+    return rank
+
+
+def load_program(wl, rank=0):
     from higflow_b200 import program as hp
     from higflow_b200 import tiling, workloads
     if wl.get("batch") == "c4":
-        return workloads.batch(workloads.batched_giesekus()[:wl.get("count", 256)])
+        return workloads.batch(workloads.batched_giesekus(seed=rank_seed(rank))[:wl.get("count", 256)])
     if wl.get("tiled"):
         prog = tiling.cavity(wl["dim"], wl["n"])
     else:
@@ -154,10 +161,13 @@ def _row_bytes(prog, codes_list):
 
 
 def cg_iter_bytes(sinfo, mixed):
-    """Compulsory bytes of one preconditioned CG iteration over every instance of
-    the batch (each array a kernel reads or writes counted once per kernel):
-    direction + spmv and update on the FP64 finest operator, then the V-cycle
-    (hf_pcg.cuh) in FP32 (mixed) or FP64, or the Jacobi z."""
+    """Algorithmic bytes of one preconditioned CG iteration over every instance
+    of the batch, each array a pass reads or writes counted once per pass, with
+    the finest operator counted in the reference's CSR layout (4 B per row, 4 + w
+    per non-zero) as the algorithmic-bytes convention does; the engine's row
+    templates read 4 B per row instead, so its DRAM traffic is lower.  Passes:
+    direction + q = A p and update on the FP64 finest operator, then the
+    V-cycle (hf_pcg.cuh) in FP32 (mixed) or FP64, or the Jacobi z."""
     lv = sinfo["levels"]
     n0, nnz0 = lv[0][0], lv[0][1]
     b = n0 * (4 + 8 * 4) + nnz0 * 12          # dir: ptr, col+val, z, p_old -> p, q
@@ -208,11 +218,13 @@ def _barrier(world):
 
 
 def _max_over_ranks(x, world, device):
+    """max of x over the ranks (one scalar all-reduce; the only collective)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], device=f"cuda:{device}", dtype=torch.float64)
+    on_gpu = dist.get_backend() == "nccl"
+    t = torch.tensor([x], device=f"cuda:{device}" if on_gpu else "cpu", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -259,7 +271,7 @@ def run_b200(args, rank, world, device):
 
     wl = WORKLOADS[args.workload]
     t0 = time.perf_counter()
-    prog = load_program(wl)
+    prog = load_program(wl, rank)
     t_program = time.perf_counter() - t0
     mixed = wl["precision"] == "mixed"
     prec = hp.PREC_MIXED if mixed else hp.PREC_FP64
