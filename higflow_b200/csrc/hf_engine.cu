@@ -643,7 +643,27 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
     for (int i = 0; i < D; i++)
 #pragma unroll
         for (int j = 0; j < D; j++) F.Knew[i * D + j][cc] = Knew[i][j];
-    // polymeric tensor from the new kernel (hig-flow-step-viscoelastic.c:244-318)
+}
+
+// Polymeric tensor from the new kernel (hig-flow-step-viscoelastic.c:244-318),
+// one thread per cell, after k_ve_cell (F as k_ve_cell saw it: K_new holds
+// the new kernel).  Kept apart from k_ve_cell so that neither kernel carries
+// both eigensolves: fewer registers per thread and less code per launch.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_ve_stress(DevProg P, DevFields F)
+{
+    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cc >= P.ncell) return;
+    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    const double Re = pr.Re, De = pr.De;
+    double Knew[D][D], Du[D][D];
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            Knew[i][j] = F.Knew[i * D + j][cc];
+            Du[i][j] = F.Du[i * D + j][cc];
+        }
     double lam2[D], R2[D][D], Bk[D][D], A[D][D];
     hf::jacobi<D>(Knew, lam2, R2);
 #pragma unroll
@@ -1645,9 +1665,10 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     if (ve) {
         record(C, HF_PHASE_VE_CELL, 0);
         k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
+        k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
-        fixed++;
+        fixed += 2;
     }
     record(C, HF_PHASE_VELOCITY, 0);
     if (C->P.nvrows) {
@@ -1817,7 +1838,7 @@ int collect_phases(hf_case *C)
         HF_CK(cudaEventElapsedTime(&ms, C->ev[2 * p], C->ev[2 * p + 1]));
         C->phase_ms[p] += ms;
     }
-    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 1;
+    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2;
     C->phase_launches[HF_PHASE_VELOCITY] += 1;
     C->phase_launches[HF_PHASE_POISSON_INIT] += 1;
     C->phase_launches[HF_PHASE_POISSON_ITER] += (C->h_ctl->total_bodies - C->bodies0) * C->body_kernels;
@@ -1868,7 +1889,8 @@ int bicg_step(hf_case *C)
     if (ve) {
         PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
         k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
-        launches++;
+        k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
+        launches += 2;
         for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
         t.stop(launches);
     }
