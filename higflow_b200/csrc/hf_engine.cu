@@ -499,8 +499,8 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
 #pragma unroll
     for (int dim = 0; dim < D; dim++) {
         const int B = HF_C_BLK0 + HF_C_NB * dim;
-        vl[dim] = hf::query(R, CS(B + HF_C_UVL), F.u[dim]);
-        vr[dim] = hf::query(R, CS(B + HF_C_UVR), F.u[dim]);
+        vl[dim] = hf::query_cold(R, CS(B + HF_C_UVL), F.u[dim]);
+        vr[dim] = hf::query_cold(R, CS(B + HF_C_UVR), F.u[dim]);
     }
     // Du (hig-flow-step-generalized-newtonian.c:30-64)
     double Du[D][D];
@@ -517,11 +517,11 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
                 } else {
                     const int Q = HF_C_BLK0 + HF_C_NB * D + HF_C_NQ * pair;
                     pair++;
-                    double vrr = hf::query(R, CS(Q + 0), F.u[dim]);
-                    double vll = hf::query(R, CS(Q + 1), F.u[dim]);
+                    double vrr = hf::query_cold(R, CS(Q + 0), F.u[dim]);
+                    double vll = hf::query_cold(R, CS(Q + 1), F.u[dim]);
                     ul = 0.25 * (vll + vl[dim] + vr[dim] + vrr);
-                    vrr = hf::query(R, CS(Q + 2), F.u[dim]);
-                    vll = hf::query(R, CS(Q + 3), F.u[dim]);
+                    vrr = hf::query_cold(R, CS(Q + 2), F.u[dim]);
+                    vll = hf::query_cold(R, CS(Q + 3), F.u[dim]);
                     ur = 0.25 * (vll + vl[dim] + vr[dim] + vrr);
                 }
                 Du[dim][dim2] = (ur - ul) / (2.0 * 0.5 * cd[dim2]);
@@ -617,11 +617,11 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
                 const int B = HF_C_BLK0 + HF_C_NB * dim;
                 const int il = (fl >> (4 * dim + 0)) & 1, ir = (fl >> (4 * dim + 1)) & 1;
                 const int ill = (fl >> (4 * dim + 2)) & 1, irr = (fl >> (4 * dim + 3)) & 1;
-                const double kl = hf::query(R, CS(B + HF_C_KL), Kf);
-                const double kr = hf::query(R, CS(B + HF_C_KR), Kf);
+                const double kl = hf::query_cold(R, CS(B + HF_C_KL), Kf);
+                const double kr = hf::query_cold(R, CS(B + HF_C_KR), Kf);
                 if (pr.ve_convecdiscrtype == HF_CELL_CUBISTA) {
-                    const double kll = hf::query(R, CS(B + HF_C_KLL), Kf);
-                    const double krr = hf::query(R, CS(B + HF_C_KRR), Kf);
+                    const double kll = hf::query_cold(R, CS(B + HF_C_KLL), Kf);
+                    const double krr = hf::query_cold(R, CS(B + HF_C_KRR), Kf);
                     rhs -= hf::cubista_cell(kl, kr, kll, krr, il, ir, ill, irr, vl[dim], vr[dim], K[i][j], cd[dim]);
                 } else {
                     double dk;
