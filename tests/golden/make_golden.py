@@ -47,6 +47,15 @@ CASES = {
                                                   ve_convecdiscrtype=hp.CELL_CENTRAL), 4, (0.3, 0.1, 0.2)),
     "ve3d_oldroyd_log": (lambda: refpy.cavity(3, 5, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC,
                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG), 2, (0.3, 0.1, 0.2)),
+    # two-level quadtrees: a refined patch in the middle of the cavity (level-1
+    # cells of half the size), so stencils cross coarse/fine interfaces and the
+    # Poisson rows are not symmetric there
+    "amr2d_cubista": (lambda: refpy.cavity(2, 16, Re=100.0, dt=1e-3,
+                                           refine=[([0.5 / 16, 0.5 / 16], [((8, 8), (16, 16))])]), 4, (0.3, 0.1, 0.0)),
+    "amr2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC,
+                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                               refine=[([0.5 / 12, 0.5 / 12], [((6, 6), (12, 12))])]),
+                          3, (0.3, 0.1, 0.2)),
 }
 
 
