@@ -1454,7 +1454,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
             inv_off[i] = mixed ? ar.vec(cast_vec<float>(IH[i].inv)) : ar.vec(IH[i].inv);
     const int n = C->P.ncell;
     const size_t o_r = ar.zeros<double>(n), o_z = ar.zeros<double>(n), o_q = ar.zeros<double>(n);
-    const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n);
+    const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n), o_xprev = ar.zeros<double>(n);
     const size_t o_part = ar.zeros<double>((size_t)LH[0].ablk.size() * 2);
     std::vector<IScal> S(ni);
     for (int i = 0; i < ni; i++) {
@@ -1526,6 +1526,8 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     G.ipar = C->P.ipar;
     G.p = C->F.p;
     G.dp = C->F.dp;
+    G.xprev = (double *)(base + o_xprev);
+    G.cinst = C->P.cinst;
     G.r = (double *)(base + o_r);
     G.z = (double *)(base + o_z);
     G.q = (double *)(base + o_q);
@@ -1679,10 +1681,11 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
     record(C, HF_PHASE_VELOCITY, 1);
     record(C, HF_PHASE_POISSON_INIT, 0);
+    k_pcg_extrapolate<<<blocks(C->P.ncell), kBlock, 0, st>>>(C->G);
     k_pcg_init<D><<<C->G.nblk, kBlock, 0, st>>>(C->P, F, C->G);
     record(C, HF_PHASE_POISSON_INIT, 1);
     record(C, HF_PHASE_POISSON_ITER, 0);
-    fixed += 2;
+    fixed += 3;
 }
 
 // ... and after them: per-instance totals, final velocity and pressure
@@ -1840,7 +1843,7 @@ int collect_phases(hf_case *C)
     }
     if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2;
     C->phase_launches[HF_PHASE_VELOCITY] += 1;
-    C->phase_launches[HF_PHASE_POISSON_INIT] += 1;
+    C->phase_launches[HF_PHASE_POISSON_INIT] += 2;
     C->phase_launches[HF_PHASE_POISSON_ITER] += (C->h_ctl->total_bodies - C->bodies0) * C->body_kernels;
     C->phase_launches[HF_PHASE_FINAL] += 2;
     return HF_OK;
@@ -2288,6 +2291,12 @@ extern "C" int hf_case_set_field(hf_case *C, int32_t field, int32_t comp, const 
     double *p = field_ptr(C, field, comp, &m);
     if (!p || m != n) return fail(HF_ERR_INVALID, "field/component/size mismatch");
     HF_CK(cudaMemcpyAsync(p, host, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, C->stream));
+    // a new value of the solve's unknown restarts its time history (the next
+    // initial guess is the value itself, not an extrapolation)
+    if (C->G.xprev && (field == HF_FIELD_DP || field == HF_FIELD_P)) {
+        k_pcg_restart<<<blocks(C->P.ncell), kBlock, 0, C->stream>>>(C->G);
+        HF_CK(cudaGetLastError());
+    }
     HF_CK(cudaStreamSynchronize(C->stream));
     return HF_OK;
 }

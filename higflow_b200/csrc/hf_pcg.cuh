@@ -130,6 +130,8 @@ struct PcgFine {
     const int32_t *ipin;      // per instance: pinned global row or -1
     const hf_params *ipar;
     double *p, *dp;           // unknown: dp (incremental projection) or p
+    double *xprev;            // the unknown of the step before (initial-guess extrapolation)
+    const int32_t *cinst;     // cell -> instance
     double *r, *z, *q;
     double *partials;
     IScal *S;
@@ -588,6 +590,33 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *
             if (set_cond == 1) cudaGraphSetConditional(cond, (active > 0 && c.bodies < c.maxbodies) ? 1u : 0u);
         }
     }
+}
+
+// Initial guess of the step's solve: linear extrapolation in time of the
+// unknown, x0 = 2 x_n - x_{n-1} (x_n is the previous step's solution, the
+// reference's own initial guess, solver-petsc.c:386-399).  The solution is the
+// same to the solve's tolerance; the extrapolated start is closer to it, so
+// fewer iterations are needed.  The first step of a case keeps x_n.
+__global__ void __launch_bounds__(kBlock) k_pcg_extrapolate(PcgFine G)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G.n) return;
+    const bool incr = G.ipar[__ldg(G.cinst + i)].projtype == HF_INCREMENTAL;
+    double *x = incr ? G.dp : G.p;
+    const double xn = x[i];
+    const double xp = ((volatile const Ctl *)G.ctl)->step == 0 ? xn : G.xprev[i];
+    G.xprev[i] = xn;
+    x[i] = 2.0 * xn - xp;
+}
+
+// restart the time history: the next extrapolation starts from the unknown's
+// current value (after the host has written the pressure or its increment)
+__global__ void __launch_bounds__(kBlock) k_pcg_restart(PcgFine G)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G.n) return;
+    const bool incr = G.ipar[__ldg(G.cinst + i)].projtype == HF_INCREMENTAL;
+    G.xprev[i] = (incr ? G.dp : G.p)[i];
 }
 
 // end of a step: per-instance totals, the first failure, loop counters reset
