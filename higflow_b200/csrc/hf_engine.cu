@@ -1190,17 +1190,90 @@ std::vector<T> cast_vec(const std::vector<double> &v)
     return std::vector<T>(v.begin(), v.end());
 }
 
+// A CSR matrix as row templates: rows whose entries have the same column
+// offsets from the row's anchor and the same values, in entry order, share one
+// template.  The anchor is the row index (square operators, rd only) or the
+// row's first column (transfer operators, kept in base).
+struct TemplateForm {
+    std::vector<uint32_t> rd;    // per row: (first entry << kTLenBits) | entry count
+    std::vector<int32_t> base;   // per row: anchor column (first-column anchors)
+    std::vector<int32_t> toff;
+    std::vector<double> tval;
+    bool ok = false;             // false: a row too long or too many entries
+};
+
+TemplateForm make_templates(const std::vector<int32_t> &ptr, const std::vector<int32_t> &col,
+                            const std::vector<double> &val, bool anchor_is_row)
+{
+    TemplateForm t;
+    const int n = (int)ptr.size() - 1;
+    t.rd.resize(n);
+    if (!anchor_is_row) t.base.resize(n);
+    // 64-bit content hash -> descriptor; a hash shared by different contents
+    // moves to the next hash value (open addressing over the key space)
+    std::unordered_map<uint64_t, uint32_t> seen;
+    seen.reserve(1024);
+    for (int i = 0; i < n; i++) {
+        const int a = ptr[i], len = ptr[i + 1] - a;
+        if (len >= (1 << kTLenBits)) return t;
+        const int32_t anchor = anchor_is_row ? i : (len ? col[a] : 0);
+        if (!anchor_is_row) t.base[i] = anchor;
+        uint64_t h = 0x9e3779b97f4a7c15ull ^ (uint64_t)len;
+        for (int k = a; k < a + len; k++) {
+            uint64_t v;
+            memcpy(&v, &val[k], sizeof v);
+            h = (h ^ (uint64_t)(uint32_t)(col[k] - anchor)) * 0x100000001b3ull;
+            h = (h ^ v) * 0x100000001b3ull;
+            h ^= h >> 29;
+        }
+        for (;; h++) {
+            auto it = seen.find(h);
+            if (it == seen.end()) {
+                if (t.toff.size() + len >= ((size_t)1 << (32 - kTLenBits))) return t;
+                const uint32_t d = ((uint32_t)t.toff.size() << kTLenBits) | (uint32_t)len;
+                for (int k = a; k < a + len; k++) {
+                    t.toff.push_back(col[k] - anchor);
+                    t.tval.push_back(val[k]);
+                }
+                seen.emplace(h, d);
+                t.rd[i] = d;
+                break;
+            }
+            const uint32_t d = it->second;
+            const int k0 = (int)(d >> kTLenBits);
+            bool same = (int)(d & ((1u << kTLenBits) - 1)) == len;
+            for (int k = 0; same && k < len; k++)
+                same = t.toff[k0 + k] == col[a + k] - anchor && memcmp(&t.tval[k0 + k], &val[a + k], sizeof(double)) == 0;
+            if (same) {
+                t.rd[i] = d;
+                break;
+            }
+        }
+    }
+    t.ok = true;
+    return t;
+}
+
 // Host copy of one concatenated level of the batched hierarchy.
 struct LevelHost {
     int n = 0;
     std::vector<int32_t> Ap, Ac, Pp, Pc, Rp, Rc;
     std::vector<double> Av, dinv, Pv, Rv;
     std::vector<Blk> sblk, ablk;
+    TemplateForm At, Pt, Rt;   // the same operators as templates (coarse A; P, R)
 };
 
 struct LevelOff {
     size_t Ap, Ac, Av, dinv, Pp, Pc, Pv, Rp, Rc, Rv, b, x, r, out, sblk, ablk;
+    size_t Ard, Atoff, Atval, Prb, Ptoff, Ptval, Rrb, Rtoff, Rtval;
 };
+
+std::vector<uint2> pack_rb(const TemplateForm &t)
+{
+    std::vector<uint2> rb(t.rd.size());
+    for (size_t i = 0; i < rb.size(); i++) rb[i] = make_uint2(t.rd[i], (uint32_t)t.base[i]);
+    return rb;
+}
 
 // Blocks of kBlock rows over the instances a level-synchronous kernel of level
 // l covers: smooth_only, the instances smoothed there by those kernels (l below
@@ -1240,6 +1313,15 @@ LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
         o.Pp = ar.vec(h.Pp); o.Pc = ar.vec(h.Pc); o.Pv = ar.vec(cast_vec<T>(h.Pv));
         o.Rp = ar.vec(h.Rp); o.Rc = ar.vec(h.Rc); o.Rv = ar.vec(cast_vec<T>(h.Rv));
     }
+    if (h.At.ok) {
+        o.Ard = ar.vec(h.At.rd); o.Atoff = ar.vec(h.At.toff); o.Atval = ar.vec(cast_vec<T>(h.At.tval));
+    }
+    if (h.Pt.ok) {
+        o.Prb = ar.vec(pack_rb(h.Pt)); o.Ptoff = ar.vec(h.Pt.toff); o.Ptval = ar.vec(cast_vec<T>(h.Pt.tval));
+    }
+    if (h.Rt.ok) {
+        o.Rrb = ar.vec(pack_rb(h.Rt)); o.Rtoff = ar.vec(h.Rt.toff); o.Rtval = ar.vec(cast_vec<T>(h.Rt.tval));
+    }
     o.x = ar.zeros<T>(h.n);
     o.r = ar.zeros<T>(h.n);
     o.out = ar.zeros<T>(h.n);
@@ -1267,6 +1349,9 @@ VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const DevM
         v.Pp = (const int32_t *)(base + o.Pp); v.Pc = (const int32_t *)(base + o.Pc); v.Pv = (const T *)(base + o.Pv);
         v.Rp = (const int32_t *)(base + o.Rp); v.Rc = (const int32_t *)(base + o.Rc); v.Rv = (const T *)(base + o.Rv);
     }
+    if (o.Ard) v.At = TRows<T>{(const uint32_t *)(base + o.Ard), (const int32_t *)(base + o.Atoff), (const T *)(base + o.Atval)};
+    if (o.Prb) v.Pt = BRows<T>{(const uint2 *)(base + o.Prb), (const int32_t *)(base + o.Ptoff), (const T *)(base + o.Ptval)};
+    if (o.Rrb) v.Rt = BRows<T>{(const uint2 *)(base + o.Rrb), (const int32_t *)(base + o.Rtoff), (const T *)(base + o.Rtval)};
     v.x = (T *)(base + o.x);
     v.r = (T *)(base + o.r);
     v.out = (T *)(base + o.out);
@@ -1438,6 +1523,19 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         if (off[clev[i]][i + 1] > LH[clev[i]].n || off[clev[i]][i + 1] - off[clev[i]][i] > kCoarseCap)
             return fail(HF_ERR_INVALID, "inconsistent coarsest level");
         if (tail[i] > clev[i] || clev[i] >= kMaxLevels) return fail(HF_ERR_INVALID, "inconsistent tail level");
+    }
+
+    // template forms of the operators and transfers the level-synchronous
+    // kernels read (levels above the last tail start); the tails keep CSR
+    if (amg) {
+        std::vector<std::thread> th;
+        for (int l = 0; l < C->nreg && l + 1 < nlev; l++) {
+            LevelHost &h = LH[l];
+            if (l > 0) th.emplace_back([&h]() { h.At = make_templates(h.Ap, h.Ac, h.Av, true); });
+            th.emplace_back([&h]() { h.Pt = make_templates(h.Pp, h.Pc, h.Pv, false); });
+            th.emplace_back([&h]() { h.Rt = make_templates(h.Rp, h.Rc, h.Rv, false); });
+        }
+        for (auto &t : th) t.join();
     }
 
     // device arena: hierarchy (in the V-cycle's precision), dense inverses,

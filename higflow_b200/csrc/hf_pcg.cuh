@@ -95,16 +95,44 @@ __device__ __forceinline__ T trow(const TRows<T> &A, int i, Fn f)
     return s;
 }
 
+// Rows of a transfer operator (prolongation or restriction) as templates
+// anchored at a per-row column: rb[i] = (descriptor as in TRows, anchor), the
+// entries' columns are anchor + toff[k].  Smoothed aggregation on a uniform
+// grid repeats a few tens of row patterns per level, so a row costs 8 bytes
+// instead of 8 per entry.
+template <typename T>
+struct BRows {
+    const uint2 *rb;
+    const int32_t *toff;
+    const T *tval;
+};
+
+template <typename T, typename Fn>
+__device__ __forceinline__ T brow(const BRows<T> &A, int i, Fn f)
+{
+    const uint2 d = __ldg(A.rb + i);
+    const int k0 = (int)(d.x >> kTLenBits), e = k0 + (int)(d.x & ((1u << kTLenBits) - 1));
+    const int a = (int)d.y;
+    T s = T(0);
+    for (int k = k0; k < e; k++) s += __ldg(A.tval + k) * f(a + __ldg(A.toff + k));
+    return s;
+}
+
+// The level-synchronous kernels read the operator and the transfers of a
+// level as templates (At, Pt, Rt) when the level has them; the per-instance
+// tails read the CSR form (the same entries in the same order, so both give
+// the same sums).
 template <typename T>
 struct VLev {
     int n;
-    const int32_t *Ap, *Ac;   // CSR on the coarse levels; the finest level uses At
+    const int32_t *Ap, *Ac;   // CSR on the coarse levels (the finest level has At only)
     const T *Av, *dinv;
     TRows<T> At;
     const int32_t *Pp, *Pc;   // rows: this level, columns: next level
     const T *Pv;
     const int32_t *Rp, *Rc;   // rows: next level, columns: this level
     const T *Rv;
+    BRows<T> Pt, Rt;
     T *b, *x, *r, *out;       // b unused on the finest level (the CG residual is)
     const Blk *sblk, *ablk;   // smoothed instances' rows / all rows of the level
     int nsblk, nablk;
@@ -302,6 +330,8 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
         T s = T(0);
         if (FINE) {
             s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+        } else if (L.At.rd) {
+            s = trow(L.At, i, [&](int j) { return w * L.dinv[j] * L.b[j]; });
         } else {
             for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
                 const int j = L.Ac[k];
@@ -325,7 +355,9 @@ __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, c
         if (t >= B.cnt) break;
         const int i = B.row0 + t;
         T s = T(0);
-        for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
+        if (L.Rt.rb) s = brow(L.Rt, i, [&](int j) { return L.r[j]; });
+        else
+            for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
         Ln.b[i] = s;
     }
 }
@@ -445,7 +477,9 @@ __global__ void __launch_bounds__(kBlock) k_vc_prolong(VLev<T> L, const T *__res
         if (t >= B.cnt) break;
         const int i = B.row0 + t;
         T s = T(0);
-        for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * e[L.Pc[k]];
+        if (L.Pt.rb) s = brow(L.Pt, i, [&](int j) { return e[j]; });
+        else
+            for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * e[L.Pc[k]];
         L.x[i] += s;
     }
 }
@@ -462,7 +496,9 @@ __global__ void __launch_bounds__(kBlock) k_vc_post(VLev<T> L, const IScal *S)
         if (t >= B.cnt) break;
         const int i = B.row0 + t;
         T s = T(0);
-        for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
+        if (L.At.rd) s = trow(L.At, i, [&](int j) { return L.x[j]; });
+        else
+            for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
         L.out[i] = L.x[i] + T(kSmoothW) * L.dinv[i] * (L.b[i] - s);
     }
 }
