@@ -92,6 +92,8 @@ struct DevProg {
     const uint32_t *cflags;
     int cns;
     int pin;               // single-instance path: instance 0's pin and parameters (par)
+    int projtype_all;      // the projection type of every instance, or -1 when they differ
+                           // (saves the per-element instance lookup before the field loads)
     double pin_value;
     // per-instance parameters and element -> instance maps (batches)
     int ninst;
@@ -483,8 +485,13 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 // ---------------------------------------------------------------------------
 // viscoelastic cell stage (Du, constitutive update, polymeric tensor)
 // ---------------------------------------------------------------------------
+// 128-thread blocks capped at 96 registers (2D): with the prefetched slot
+// values five such blocks (20 warps) fit an SM, where 256-thread blocks at the
+// uncapped ~100 registers would give 16 warps
+constexpr int kVeBlock = 128;
+
 template <int D>
-__global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
+__global__ void __launch_bounds__(kVeBlock, D == 2 ? 5 : 4) k_ve_cell(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     if (cc >= P.ncell) return;
@@ -494,13 +501,29 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
     const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
     const uint32_t fl = __ldg(P.cflags + cc);
     const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    // The velocity values this cell reads: its face velocities (u[dim] at
+    // -/+ half a cell, UVL/UVR) and the Du corner queries (HF_C_NQ per ordered
+    // pair dim != dim2, on u[dim]).  All slot codes, then all values as
+    // independent loads; general rows (cells at boundaries) are fixed up
+    // afterwards, out of line.
+    constexpr int NU = 2 * D, NQ = HF_C_NQ * D * (D - 1);
+    int32_t cu[NU + NQ];
+    double vu[NU + NQ];
+    auto uslot = [](int k) { return k < NU ? HF_C_BLK0 + HF_C_NB * (k >> 1) + (k & 1) : HF_C_BLK0 + HF_C_NB * D + (k - NU); };
+    auto ufield = [&](int k) { return F.u[k < NU ? (k >> 1) : (k - NU) / (HF_C_NQ * (D - 1))]; };
+#pragma unroll
+    for (int k = 0; k < NU + NQ; k++) cu[k] = CS(uslot(k));
+#pragma unroll
+    for (int k = 0; k < NU + NQ; k++) vu[k] = cu[k] >= 0 ? __ldg(ufield(k) + cu[k]) : 0.0;
+#pragma unroll
+    for (int k = 0; k < NU + NQ; k++)
+        if (cu[k] < 0) vu[k] = hf::query_row(R, cu[k], ufield(k));
     // velocity at the faces of this cell, shared by Du, u_c and the CUBISTA flux
     double vl[D], vr[D];
 #pragma unroll
     for (int dim = 0; dim < D; dim++) {
-        const int B = HF_C_BLK0 + HF_C_NB * dim;
-        vl[dim] = hf::query_cold(R, CS(B + HF_C_UVL), F.u[dim]);
-        vr[dim] = hf::query_cold(R, CS(B + HF_C_UVR), F.u[dim]);
+        vl[dim] = vu[2 * dim + 0];
+        vr[dim] = vu[2 * dim + 1];
     }
     // Du (hig-flow-step-generalized-newtonian.c:30-64)
     double Du[D][D];
@@ -515,13 +538,13 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
                     ul = vl[dim];
                     ur = vr[dim];
                 } else {
-                    const int Q = HF_C_BLK0 + HF_C_NB * D + HF_C_NQ * pair;
+                    const int Q = NU + HF_C_NQ * pair;
                     pair++;
-                    double vrr = hf::query_cold(R, CS(Q + 0), F.u[dim]);
-                    double vll = hf::query_cold(R, CS(Q + 1), F.u[dim]);
+                    double vrr = vu[Q + 0];
+                    double vll = vu[Q + 1];
                     ul = 0.25 * (vll + vl[dim] + vr[dim] + vrr);
-                    vrr = hf::query_cold(R, CS(Q + 2), F.u[dim]);
-                    vll = hf::query_cold(R, CS(Q + 3), F.u[dim]);
+                    vrr = vu[Q + 2];
+                    vll = vu[Q + 3];
                     ur = 0.25 * (vll + vl[dim] + vr[dim] + vrr);
                 }
                 Du[dim][dim2] = (ur - ul) / (2.0 * 0.5 * cd[dim2]);
@@ -605,23 +628,37 @@ __global__ void __launch_bounds__(kBlock) k_ve_cell(DevProg P, DevFields F)
             }
             RHS[i][j] = ok - ko + 2.0 * BB[i][j] + MM[i][j] / De;
         }
+    // the kernel's neighbour values: per direction KL, KR, KLL, KRR (the same
+    // codes for every component), loaded component by component, all
+    // directions at once
+    // (KLL/KRR are loaded for every cell, so that no load waits for the
+    // instance's parameters; without CUBISTA their values go unused)
+    const bool cub = pr.ve_convecdiscrtype == HF_CELL_CUBISTA;
+    int32_t ck[4 * D];
+#pragma unroll
+    for (int k = 0; k < 4 * D; k++) ck[k] = CS(HF_C_BLK0 + HF_C_NB * (k >> 2) + HF_C_KL + (k & 3));
     double Knew[D][D];
 #pragma unroll
     for (int i = 0; i < D; i++) {
 #pragma unroll
         for (int j = i; j < D; j++) {
             const double *Kf = F.K[i * D + j];
+            double kv[4 * D];
+#pragma unroll
+            for (int k = 0; k < 4 * D; k++) kv[k] = ck[k] >= 0 ? __ldg(Kf + ck[k]) : 0.0;
+#pragma unroll
+            for (int k = 0; k < 4 * D; k++)
+                if (ck[k] < 0 && ((k & 3) < 2 || cub)) kv[k] = hf::query_row(R, ck[k], Kf);
             double rhs = 0.0;
 #pragma unroll
             for (int dim = 0; dim < D; dim++) {
-                const int B = HF_C_BLK0 + HF_C_NB * dim;
                 const int il = (fl >> (4 * dim + 0)) & 1, ir = (fl >> (4 * dim + 1)) & 1;
                 const int ill = (fl >> (4 * dim + 2)) & 1, irr = (fl >> (4 * dim + 3)) & 1;
-                const double kl = hf::query_cold(R, CS(B + HF_C_KL), Kf);
-                const double kr = hf::query_cold(R, CS(B + HF_C_KR), Kf);
-                if (pr.ve_convecdiscrtype == HF_CELL_CUBISTA) {
-                    const double kll = hf::query_cold(R, CS(B + HF_C_KLL), Kf);
-                    const double krr = hf::query_cold(R, CS(B + HF_C_KRR), Kf);
+                const double kl = kv[4 * dim + 0];
+                const double kr = kv[4 * dim + 1];
+                if (cub) {
+                    const double kll = kv[4 * dim + 2];
+                    const double krr = kv[4 * dim + 3];
                     rhs -= hf::cubista_cell(kl, kr, kll, krr, il, ir, ill, irr, vl[dim], vr[dim], K[i][j], cd[dim]);
                 } else {
                     double dk;
@@ -855,7 +892,8 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
         const int f = e - pick<4>(P.off, d);
         const int nf = pick<3>(P.nf, d);
         const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
-        const double *pp = par.projtype == HF_INCREMENTAL ? F.dp : F.p;
+        const int pt = P.projtype_all >= 0 ? P.projtype_all : par.projtype;
+        const double *pp = pt == HF_INCREMENTAL ? F.dp : F.p;
         const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
         const int32_t *sl = pick<3>(P.vslots, d);
         const int32_t cl = __ldg(sl + (size_t)HF_V_PL * nf + f), cr = __ldg(sl + (size_t)HF_V_PR * nf + f);
@@ -865,7 +903,9 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
         pick<3>(F.u, d)[f] = __ldg(pick<3>(F.us, d) + f) - par.dt * dpdx;
     } else {
         const int c = e - P.off[D];
-        if (c < P.ncell && P.ipar[__ldg(P.cinst + c)].projtype == HF_INCREMENTAL) F.p[c] = F.p[c] + F.dp[c];
+        if (c < P.ncell &&
+            (P.projtype_all >= 0 ? P.projtype_all : P.ipar[__ldg(P.cinst + c)].projtype) == HF_INCREMENTAL)
+            F.p[c] = F.p[c] + F.dp[c];
     }
 }
 
@@ -1635,6 +1675,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     G.blk = (const Blk *)(base + o_fblk);
     G.nblk = (int)LH[0].ablk.size();
     G.ninst = ni;
+    G.projtype_all = C->P.projtype_all;
     G.rtol = C->opt.poisson_rtol;
     G.atol = C->opt.poisson_atol;
     G.maxit = C->opt.poisson_maxit;
@@ -1764,7 +1805,7 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     if (ve) {
         record(C, HF_PHASE_VE_CELL, 0);
-        k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
+        k_ve_cell<D><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
@@ -1989,7 +2030,7 @@ int bicg_step(hf_case *C)
     int64_t launches = 0;
     if (ve) {
         PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
-        k_ve_cell<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
+        k_ve_cell<D><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
         launches += 2;
         for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
@@ -2181,6 +2222,9 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     P.pin = pins[0];
     P.pin_value = pinv[0];
     P.ninst = ni;
+    P.projtype_all = ipar[0].projtype;
+    for (int i = 1; i < ni; i++)
+        if (ipar[i].projtype != P.projtype_all) P.projtype_all = -1;
     {
         std::vector<int32_t> cinst(pg->ncell);
         for (int i = 0; i < ni; i++)

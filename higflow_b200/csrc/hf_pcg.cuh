@@ -166,6 +166,7 @@ struct PcgFine {
     Ctl *ctl;
     const Blk *blk;
     int nblk, ninst;
+    int projtype_all;         // the projection type of every instance, or -1
     double rtol, atol;
     int maxit;
 };
@@ -637,10 +638,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg_extrapolate(PcgFine G)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= G.n) return;
-    const bool incr = G.ipar[__ldg(G.cinst + i)].projtype == HF_INCREMENTAL;
-    double *x = incr ? G.dp : G.p;
-    const double xn = x[i];
-    const double xp = ((volatile const Ctl *)G.ctl)->step == 0 ? xn : G.xprev[i];
+    // (the instance lookup only when the instances differ in projection
+    // type: it would delay every load behind two dependent ones)
+    const int pt = G.projtype_all >= 0 ? G.projtype_all : __ldg(&G.ipar[__ldg(G.cinst + i)].projtype);
+    double *x = pt == HF_INCREMENTAL ? G.dp : G.p;
+    const double xn = x[i], xpv = G.xprev[i];
+    // (a plain load: the step count was written by an earlier kernel)
+    const double xp = __ldg(&G.ctl->step) == 0 ? xn : xpv;
     G.xprev[i] = xn;
     x[i] = 2.0 * xn - xp;
 }
@@ -651,8 +655,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_restart(PcgFine G)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= G.n) return;
-    const bool incr = G.ipar[__ldg(G.cinst + i)].projtype == HF_INCREMENTAL;
-    G.xprev[i] = (incr ? G.dp : G.p)[i];
+    const int pt = G.projtype_all >= 0 ? G.projtype_all : __ldg(&G.ipar[__ldg(G.cinst + i)].projtype);
+    G.xprev[i] = (pt == HF_INCREMENTAL ? G.dp : G.p)[i];
 }
 
 // end of a step: per-instance totals, the first failure, loop counters reset
