@@ -141,7 +141,9 @@ struct VLev {
 // The small levels of one instance, from the first level with at most
 // kTailRows rows (s) down to its coarsest (clev, dense inverse), run by one
 // CTA: phases separated by __syncthreads instead of kernel launches.
-constexpr int kTailRows = 1024;
+// 256 rows: a tail phase is then at most one row per thread, so the tail's
+// dependent load chains stay short; larger levels run level-synchronously
+constexpr int kTailRows = 256;
 constexpr int kTailThreads = 512;
 
 template <typename T>
@@ -255,6 +257,84 @@ __device__ __forceinline__ void finish_instance(IScal &s, Ctl *ctl)
 {
     s.done = 1;
     atomicSub(&ctl->active, 1);
+}
+
+// The rows of one thread in a level-synchronous kernel: row q is
+// row0 + threadIdx.x + q * kBlock, present for q < nrow.
+struct RowSet {
+    int row[kRPT];
+    int nrow;
+};
+
+__device__ __forceinline__ RowSet rowset(const Blk &B)
+{
+    RowSet R;
+    const int left = B.cnt - (int)threadIdx.x;
+    R.nrow = left <= 0 ? 0 : min(kRPT, (left + kBlock - 1) / kBlock);
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) R.row[q] = B.row0 + (int)threadIdx.x + q * kBlock;
+    return R;
+}
+
+// Row sums of a thread's rows, entry k of every row before entry k + 1: the
+// rows' gathers are independent loads in flight together, and each row still
+// adds its entries in its own order (the sums equal trow's / brow's).  Faster
+// than one row after the other on the prolongation and the finest
+// post-smoothing; slower on the long restriction rows and on the kernels with
+// two gathers per entry, which keep the per-row loop.
+template <typename T, typename Fn>
+__device__ __forceinline__ void rows_lockstep(const T *__restrict__ tval, const int32_t *__restrict__ toff,
+                                              const uint32_t (&d)[kRPT], const int (&a)[kRPT], T (&s)[kRPT], Fn f)
+{
+    int k0[kRPT], len[kRPT], maxlen = 0;
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        k0[q] = (int)(d[q] >> kTLenBits);
+        len[q] = (int)(d[q] & ((1u << kTLenBits) - 1));
+        maxlen = max(maxlen, len[q]);
+        s[q] = T(0);
+    }
+    for (int k = 0; k < maxlen; k++) {
+#pragma unroll
+        for (int q = 0; q < kRPT; q++)
+            if (k < len[q]) s[q] += __ldg(tval + k0[q] + k) * f(a[q] + __ldg(toff + k0[q] + k));
+    }
+}
+
+template <typename T, typename Fn>
+__device__ __forceinline__ void trows(const TRows<T> &A, const RowSet &R, T (&s)[kRPT], Fn f)
+{
+    uint32_t d[kRPT];
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) d[q] = q < R.nrow ? __ldg(A.rd + R.row[q]) : 0u;
+    rows_lockstep(A.tval, A.toff, d, R.row, s, f);
+}
+
+template <typename T, typename Fn>
+__device__ __forceinline__ void brows(const BRows<T> &A, const RowSet &R, T (&s)[kRPT], Fn f)
+{
+    uint32_t d[kRPT];
+    int a[kRPT];
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const uint2 v = q < R.nrow ? __ldg(A.rb + R.row[q]) : make_uint2(0u, 0u);
+        d[q] = v.x;
+        a[q] = (int)v.y;
+    }
+    rows_lockstep(A.tval, A.toff, d, a, s, f);
+}
+
+// CSR row sums (the per-instance tails' levels, and levels without templates)
+template <typename T, typename Fn>
+__device__ __forceinline__ void csr_rows(const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                                         const T *__restrict__ val, const RowSet &R, T (&s)[kRPT], Fn f)
+{
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        s[q] = T(0);
+        if (q < R.nrow)
+            for (int k = ptr[R.row[q]]; k < ptr[R.row[q] + 1]; k++) s[q] += val[k] * f(col[k]);
+    }
 }
 
 }  // namespace pcg
@@ -472,17 +552,13 @@ __global__ void __launch_bounds__(kBlock) k_vc_prolong(VLev<T> L, const T *__res
 {
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
+    const pcg::RowSet R = pcg::rowset(B);
+    T s[kRPT];
+    if (L.Pt.rb) pcg::brows(L.Pt, R, s, [&](int j) { return e[j]; });
+    else pcg::csr_rows(L.Pp, L.Pc, L.Pv, R, s, [&](int j) { return e[j]; });
 #pragma unroll
-    for (int q = 0; q < kRPT; q++) {
-        const int t = threadIdx.x + q * kBlock;
-        if (t >= B.cnt) break;
-        const int i = B.row0 + t;
-        T s = T(0);
-        if (L.Pt.rb) s = brow(L.Pt, i, [&](int j) { return e[j]; });
-        else
-            for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * e[L.Pc[k]];
-        L.x[i] += s;
-    }
+    for (int q = 0; q < kRPT; q++)
+        if (q < R.nrow) L.x[R.row[q]] += s[q];
 }
 
 // out = x + w D^-1 (b - A x) on the smoothed rows of a coarse level
@@ -512,12 +588,14 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
     const bool tail0 = G.S[B.inst].tail0;
+    const pcg::RowSet R = pcg::rowset(B);
+    T s[kRPT];
+    if (!JACOBI && !tail0) pcg::trows(L0.At, R, s, [&](int j) { return L0.x[j]; });
     double part[1] = {0.0};
 #pragma unroll
     for (int q = 0; q < kRPT; q++) {
-        const int t = threadIdx.x + q * kBlock;
-        if (t >= B.cnt) break;
-        const int i = B.row0 + t;
+        if (q >= R.nrow) break;
+        const int i = R.row[q];
         const double ri = G.r[i];
         double z;
         if (JACOBI) {
@@ -525,8 +603,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
         } else if (tail0) {
             z = double(L0.out[i]);
         } else {
-            const T s = trow(L0.At, i, [&](int j) { return L0.x[j]; });
-            z = double(L0.x[i] + T(kSmoothW) * L0.dinv[i] * (T(ri) - s));
+            z = double(L0.x[i] + T(kSmoothW) * L0.dinv[i] * (T(ri) - s[q]));
         }
         G.z[i] = z;
         part[0] += ri * z;
@@ -590,17 +667,28 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *
     Blk B;
     const bool skip = pcg::load_blk(G.blk, G.S, B);
     if (!skip) {
-        const bool incr = G.ipar[B.inst].projtype == HF_INCREMENTAL;
-        double *x = incr ? G.dp : G.p;
+        const int pt = G.projtype_all >= 0 ? G.projtype_all : G.ipar[B.inst].projtype;
+        double *x = pt == HF_INCREMENTAL ? G.dp : G.p;
         const double alpha = G.S[B.inst].alpha;
+        const pcg::RowSet R = pcg::rowset(B);
+        double xv[kRPT], pv[kRPT], rv[kRPT], qv[kRPT];
+#pragma unroll
+        for (int q = 0; q < kRPT; q++) {
+            if (q < R.nrow) {
+                const int i = R.row[q];
+                xv[q] = x[i];
+                pv[q] = pn[i];
+                rv[q] = G.r[i];
+                qv[q] = G.q[i];
+            }
+        }
         double part[1] = {0.0};
 #pragma unroll
         for (int q = 0; q < kRPT; q++) {
-            const int t = threadIdx.x + q * kBlock;
-            if (t >= B.cnt) break;
-            const int i = B.row0 + t;
-            x[i] += alpha * pn[i];
-            const double r = G.r[i] - alpha * G.q[i];
+            if (q >= R.nrow) break;
+            const int i = R.row[q];
+            x[i] = xv[q] + alpha * pv[q];
+            const double r = rv[q] - alpha * qv[q];
             G.r[i] = r;
             part[0] += r * r;
         }
