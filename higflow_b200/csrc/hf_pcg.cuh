@@ -107,6 +107,17 @@ struct BRows {
     const T *tval;
 };
 
+// trow with the row's descriptor already loaded (kernels load the descriptors
+// of all their rows up front, as independent loads)
+template <typename T, typename Fn>
+__device__ __forceinline__ T trow_d(const TRows<T> &A, uint32_t d, int i, Fn f)
+{
+    const int k0 = (int)(d >> kTLenBits), e = k0 + (int)(d & ((1u << kTLenBits) - 1));
+    T s = T(0);
+    for (int k = k0; k < e; k++) s += __ldg(A.tval + k) * f(i + __ldg(A.toff + k));
+    return s;
+}
+
 template <typename T, typename Fn>
 __device__ __forceinline__ T brow(const BRows<T> &A, int i, Fn f)
 {
@@ -117,6 +128,7 @@ __device__ __forceinline__ T brow(const BRows<T> &A, int i, Fn f)
     for (int k = k0; k < e; k++) s += __ldg(A.tval + k) * f(a + __ldg(A.toff + k));
     return s;
 }
+
 
 // The level-synchronous kernels read the operator and the transfers of a
 // level as templates (At, Pt, Rt) when the level has them; the per-instance
@@ -276,6 +288,18 @@ __device__ __forceinline__ RowSet rowset(const Blk &B)
     return R;
 }
 
+// The row descriptors of a thread's rows (row0 + threadIdx.x + q * kBlock),
+// loaded together before any row is evaluated; absent rows (or no table) get 0
+template <typename D>
+__device__ __forceinline__ void row_descs(const D *tab, const Blk &B, D (&d)[kRPT])
+{
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = (int)threadIdx.x + q * kBlock;
+        d[q] = tab && t < B.cnt ? __ldg(tab + B.row0 + t) : D{};
+    }
+}
+
 // Row sums of a thread's rows, entry k of every row before entry k + 1: the
 // rows' gathers are independent loads in flight together, and each row still
 // adds its entries in its own order (the sums equal trow's / brow's).  Faster
@@ -402,6 +426,10 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
     const T w = T(kSmoothW);
+    // (the finest level's descriptors up front: faster there, slower on the
+    // coarse levels)
+    uint32_t d[kRPT];
+    if (FINE) pcg::row_descs(L.At.rd, B, d);
 #pragma unroll
     for (int q = 0; q < kRPT; q++) {
         const int t = threadIdx.x + q * kBlock;
@@ -410,7 +438,7 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
         const T bi = FINE ? T(r0[i]) : L.b[i];
         T s = T(0);
         if (FINE) {
-            s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+            s = trow_d(L.At, d[q], i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
         } else if (L.At.rd) {
             s = trow(L.At, i, [&](int j) { return w * L.dinv[j] * L.b[j]; });
         } else {
@@ -625,6 +653,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
     const IScal &sc = G.S[B.inst];
     const bool first = sc.iters == 0;
     const double beta = sc.beta;
+    uint32_t d[kRPT];
+    pcg::row_descs(G.A.rd, B, d);
     double part[1] = {0.0};
 #pragma unroll
     for (int q = 0; q < kRPT; q++) {
@@ -633,10 +663,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
         const int i = B.row0 + t;
         double qi, p;
         if (first) {
-            qi = trow(G.A, i, [&](int j) { return G.z[j]; });
+            qi = trow_d(G.A, d[q], i, [&](int j) { return G.z[j]; });
             p = G.z[i];
         } else {
-            qi = trow(G.A, i, [&](int j) { return G.z[j] + beta * po[j]; });
+            qi = trow_d(G.A, d[q], i, [&](int j) { return G.z[j] + beta * po[j]; });
             p = G.z[i] + beta * po[i];
         }
         pn[i] = p;
