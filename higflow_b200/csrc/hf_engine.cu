@@ -1348,7 +1348,7 @@ LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
         o.b = ar.zeros<T>(h.n);
     }
     if (!fine) o.Av = ar.vec(cast_vec<T>(h.Av));   // the finest level's operator is the row templates
-    if (!fine || !std::is_same<T, double>::value) o.dinv = ar.vec(cast_vec<T>(h.dinv));
+    o.dinv = ar.vec(cast_vec<T>(h.dinv));   // omega D^-1 (the finest level's too)
     if (!h.Pp.empty()) {
         o.Pp = ar.vec(h.Pp); o.Pc = ar.vec(h.Pc); o.Pv = ar.vec(cast_vec<T>(h.Pv));
         o.Rp = ar.vec(h.Rp); o.Rc = ar.vec(h.Rc); o.Rv = ar.vec(cast_vec<T>(h.Rv));
@@ -1371,13 +1371,12 @@ LevelOff place_level(Arena &ar, const LevelHost &h, bool fine)
 }
 
 template <typename T>
-VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const DevMat &M, const TRows<T> &At, bool fine)
+VLev<T> make_level(char *base, const LevelOff &o, const LevelHost &h, const TRows<T> &At, bool fine)
 {
     VLev<T> v{};
     v.n = h.n;
     if (fine) {
         v.At = At;
-        if (std::is_same<T, double>::value) v.dinv = (const T *)M.dinv;
     } else {
         v.Ap = (const int32_t *)(base + o.Ap);
         v.Ac = (const int32_t *)(base + o.Ac);
@@ -1488,9 +1487,12 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         if (l == 0) {
             C->lnnz_a[0] = (int64_t)mcol.size();
             if (amg) {
+                // the smoothing sweeps' omega D^-1, with each instance's own weight
                 h.dinv.resize(h.n);
-                for (int i = 0; i < ni; i++)
-                    std::copy(IH[i].H[0].dinv.begin(), IH[i].H[0].dinv.end(), h.dinv.begin() + off[0][i]);
+                for (int i = 0; i < ni; i++) {
+                    const hf::HostLevel &hl = IH[i].H[0];
+                    for (size_t r = 0; r < hl.dinv.size(); r++) h.dinv[off[0][i] + r] = hl.omega * hl.dinv[r];
+                }
             }
         } else {
             h.Ap.assign(1, 0);
@@ -1504,7 +1506,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
                     }
                     h.Ap.push_back((int32_t)h.Ac.size());
                 }
-                h.dinv.insert(h.dinv.end(), hl.dinv.begin(), hl.dinv.end());
+                for (double d : hl.dinv) h.dinv.push_back(hl.omega * d);
             }
             C->lnnz_a[l] = (int64_t)h.Ac.size();
         }
@@ -1685,9 +1687,9 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         for (int l = 0; l < nlev; l++) {
             if (mixed) {
                 const TRows<float> At32{G.A.rd, G.A.toff, (const float *)(base + o_tval32)};
-                C->L32[l] = make_level<float>(base, LO[l], LH[l], C->M, At32, l == 0);
+                C->L32[l] = make_level<float>(base, LO[l], LH[l], At32, l == 0);
             } else {
-                C->L64[l] = make_level<double>(base, LO[l], LH[l], C->M, G.A, l == 0);
+                C->L64[l] = make_level<double>(base, LO[l], LH[l], G.A, l == 0);
             }
         }
         // the per-instance tails: level table and row ranges

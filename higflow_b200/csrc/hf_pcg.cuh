@@ -185,7 +185,8 @@ struct PcgFine {
     int maxit;
 };
 
-constexpr double kSmoothW = 2.0 / 3.0;
+// The smoothing sweeps use each level's dinv array already scaled by the
+// level's damped-Jacobi weight (omega_l D^-1, per instance; hf_amg.cuh).
 
 namespace pcg {
 
@@ -425,7 +426,6 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
 {
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
-    const T w = T(kSmoothW);
     // (the finest level's descriptors up front: faster there, slower on the
     // coarse levels)
     uint32_t d[kRPT];
@@ -438,16 +438,16 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__r
         const T bi = FINE ? T(r0[i]) : L.b[i];
         T s = T(0);
         if (FINE) {
-            s = trow_d(L.At, d[q], i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+            s = trow_d(L.At, d[q], i, [&](int j) { return __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
         } else if (L.At.rd) {
-            s = trow(L.At, i, [&](int j) { return w * L.dinv[j] * L.b[j]; });
+            s = trow(L.At, i, [&](int j) { return L.dinv[j] * L.b[j]; });
         } else {
             for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
                 const int j = L.Ac[k];
-                s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+                s += L.Av[k] * (L.dinv[j] * L.b[j]);
             }
         }
-        L.x[i] = w * L.dinv[i] * bi;
+        L.x[i] = L.dinv[i] * bi;
         L.r[i] = bi - s;
     }
 }
@@ -492,7 +492,6 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
     }
     __syncthreads();
     if (done) return;
-    const T w = T(kSmoothW);
     const int tid = threadIdx.x;
     // down: x = w D^-1 b, r = b - A x, b_next = R r
     for (int l = ti.s; l < ti.clev; l++) {
@@ -506,15 +505,15 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
             T bi, s = T(0);
             if (l == 0) {
                 bi = T(r0[i]);
-                s = trow(L.At, i, [&](int j) { return w * __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
+                s = trow(L.At, i, [&](int j) { return __ldg(L.dinv + j) * T(__ldg(r0 + j)); });
             } else {
                 bi = L.b[i];
                 for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) {
                     const int j = L.Ac[k];
-                    s += L.Av[k] * (w * L.dinv[j] * L.b[j]);
+                    s += L.Av[k] * (L.dinv[j] * L.b[j]);
                 }
             }
-            L.x[i] = w * L.dinv[i] * bi;
+            L.x[i] = L.dinv[i] * bi;
             L.r[i] = bi - s;
         }
         __syncthreads();
@@ -568,7 +567,7 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
                 s = T(0);
                 for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
             }
-            L.out[i] = L.x[i] + w * L.dinv[i] * (bi - s);
+            L.out[i] = L.x[i] + L.dinv[i] * (bi - s);
         }
         __syncthreads();
     }
@@ -604,7 +603,7 @@ __global__ void __launch_bounds__(kBlock) k_vc_post(VLev<T> L, const IScal *S)
         if (L.At.rd) s = trow(L.At, i, [&](int j) { return L.x[j]; });
         else
             for (int k = L.Ap[i]; k < L.Ap[i + 1]; k++) s += L.Av[k] * L.x[L.Ac[k]];
-        L.out[i] = L.x[i] + T(kSmoothW) * L.dinv[i] * (L.b[i] - s);
+        L.out[i] = L.x[i] + L.dinv[i] * (L.b[i] - s);
     }
 }
 
@@ -631,7 +630,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
         } else if (tail0) {
             z = double(L0.out[i]);
         } else {
-            z = double(L0.x[i] + T(kSmoothW) * L0.dinv[i] * (T(ri) - s[q]));
+            z = double(L0.x[i] + L0.dinv[i] * (T(ri) - s[q]));
         }
         G.z[i] = z;
         part[0] += ri * z;
