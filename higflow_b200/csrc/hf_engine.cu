@@ -86,6 +86,12 @@ struct DevProg {
     const uint8_t *vtag;
     int nvrows;
     double *rowval;
+    // the same pairs for k_vrows: per pair ((first entry << vlenbits) | count,
+    // base), and the template entries packed as (weight, column) in 16 bytes;
+    // vdesc is null when a program's templates do not fit the packing
+    const uint2 *vdesc;
+    const int4 *vent;
+    int vlenbits;
     const int32_t *dslots;
     const uint16_t *cdelta;
     const int32_t *cslots;
@@ -253,11 +259,27 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 // The general rows the velocity stage reads, one thread per row: the long
 // interpolation stencils (tens of entries) run here, coalesced and without
 // divergence, instead of inside the per-facet kernel.
+// Each entry is one 16-byte load of (weight, column) and one gather; the sum
+// is hf::query's: -rhs, then the entries in template order.
 __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= P.nvrows) return;
-    P.rowval[u] = hf::query(P.vrow, -u - 1, vtag_field(F, __ldg(P.vtag + u)));
+    if (!P.vdesc) {
+        P.rowval[u] = hf::query(P.vrow, -u - 1, vtag_field(F, __ldg(P.vtag + u)));
+        return;
+    }
+    const uint2 d = __ldg(P.vdesc + u);
+    const double *__restrict__ fb = vtag_field(F, __ldg(P.vtag + u)) + d.y;
+    double res = 0.0;
+    res += -__ldg(P.vrow.rhs + u);
+    const int k0 = (int)(d.x >> P.vlenbits), e = k0 + (int)(d.x & ((1u << P.vlenbits) - 1));
+#pragma unroll 4
+    for (int k = k0; k < e; k++) {
+        const int4 t = __ldg(P.vent + k);
+        res += __ldg(fb + t.z) * __hiloint2double(t.y, t.x);
+    }
+    P.rowval[u] = res;
 }
 
 // 128-thread blocks: the prefetched slots take ~170 registers per thread, and
@@ -2307,6 +2329,29 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             UP((uint16_t **)&P.vdelta[d], pg->vel_delta[d], pg->nfacet[d]);
         }
         P.nvrows = (int)ptmpl.size();
+        // the packed form: the count field is as wide as the longest template
+        // needs, the rest of the word holds the first entry
+        int64_t maxlen = 0;
+        for (int64_t t = 0; t < pg->ntmpl; t++) maxlen = std::max(maxlen, pg->tmpl_ptr[t + 1] - pg->tmpl_ptr[t]);
+        int lb = 1;
+        while (((int64_t)1 << lb) <= maxlen) lb++;
+        P.vlenbits = lb;
+        if (!ptmpl.empty() && lb < 32 && pg->nnz < ((int64_t)1 << (32 - lb))) {
+            std::vector<uint2> vdesc(ptmpl.size());
+            for (size_t u = 0; u < ptmpl.size(); u++) {
+                const int64_t a = pg->tmpl_ptr[ptmpl[u]], len = pg->tmpl_ptr[ptmpl[u] + 1] - a;
+                vdesc[u] = make_uint2(((uint32_t)a << lb) | (uint32_t)len, (uint32_t)pbase[u]);
+            }
+            UP((uint2 **)&P.vdesc, vdesc.data(), vdesc.size());
+            std::vector<int4> vent((size_t)pg->nnz);
+            for (int64_t k = 0; k < pg->nnz; k++) {
+                const double w = pg->tmpl_w[k];
+                int64_t bits;
+                memcpy(&bits, &w, sizeof bits);
+                vent[k] = make_int4((int)(uint32_t)(bits & 0xffffffff), (int)(uint32_t)((uint64_t)bits >> 32), pg->tmpl_col[k], 0);
+            }
+            UP((int4 **)&P.vent, vent.data(), vent.size());
+        }
         P.vrow.tptr = P.rows.tptr;
         P.vrow.col = P.rows.col;
         P.vrow.w = P.rows.w;
