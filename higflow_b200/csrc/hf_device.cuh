@@ -193,8 +193,11 @@ __device__ __forceinline__ double kernel_jacobian(int kind, double l, double tol
     return 1.0;
 }
 
-// hig_flow_convective_cell_term_cubista (hig-flow-step.c:1185-1358)
-__device__ inline double cubista_cell(double kl, double kr, double kll, double krr, int il, int ir,
+// hig_flow_convective_cell_term_cubista (hig-flow-step.c:1185-1358).  Out of
+// line: the VE cell stage calls it D(D+1)/2 x D times, and six inlined copies
+// of its branches made that kernel instruction-fetch bound (1.74 -> 1.38 ms on
+// 4.29 M cells with one shared copy).
+__device__ __noinline__ double cubista_cell(double kl, double kr, double kll, double krr, int il, int ir,
                                       int ill, int irr, double vl, double vr, double kc, double cdelta)
 {
     const double a = 1.7500, b = 0.3750, c = 0.7500, d = 0.1250, e = 0.2500;
