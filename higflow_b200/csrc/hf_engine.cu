@@ -282,6 +282,73 @@ __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
     P.rowval[u] = res;
 }
 
+// CUBISTA convective flux of the facet velocity along one direction
+// (higflow_computational_cell, hig-flow-discret.c:157-260), out of line: k_velocity
+// would otherwise carry one inlined copy of these branches per direction.
+// conv1 / conv2 come in with the previous direction's values, as in the
+// reference, where a NaN ratio leaves them unassigned.
+__device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double ur, double ull, double urr,
+                                              int infll, int infrr, double vcr, double vcl, double conv1,
+                                              double conv2)
+{
+    const double a = 1.7500, b = 0.3750, c = 0.7500, dd = 0.1250, ee = 0.2500;
+    if (vcr > 0.0) {
+        if (HF_FLT_EQ(ur, ul)) {
+            conv1 = vcr * ufacet;
+        } else {
+            const double fi = (ufacet - ul) / (ur - ul);
+            if ((fi <= 0.0) || (fi >= 1.0)) {
+                conv1 = vcr * ufacet;
+            } else {
+                if (fi < b) conv1 = vcr * (a * ufacet - c * ul);
+                if ((fi >= b) && (fi <= c)) conv1 = vcr * (c * ufacet + b * ur - dd * ul);
+                if (fi > c) conv1 = vcr * (ee * ufacet + c * ur);
+            }
+        }
+    } else {
+        if (HF_FLT_EQ(ufacet, urr)) {
+            conv1 = vcr * ur;
+        } else {
+            const double fi = (ur - urr) / (ufacet - urr);
+            if ((fi <= 0.0) || (fi >= 1.0)) {
+                conv1 = vcr * ur;
+            } else {
+                if (fi < b) conv1 = infrr == 1 ? vcr * (a * ur - c * urr) : vcr * ur;
+                if ((fi >= b) && (fi <= c)) conv1 = infrr == 1 ? vcr * (c * ur + b * ufacet - dd * urr) : vcr * ur;
+                if (fi > c) conv1 = vcr * (c * ufacet + ee * ur);
+            }
+        }
+    }
+    if (vcl > 0.0) {
+        if (HF_FLT_EQ(ufacet, ull)) {
+            conv2 = vcl * ul;
+        } else {
+            const double fi = (ul - ull) / (ufacet - ull);
+            if ((fi <= 0.0) || (fi >= 1.0)) {
+                conv2 = vcl * ul;
+            } else {
+                if (fi < b) conv2 = infll == 1 ? vcl * (a * ul - c * ull) : vcl * ul;
+                if ((fi >= b) && (fi <= c)) conv2 = infll == 1 ? vcl * (b * ufacet + c * ul - dd * ull) : vcl * ul;
+                if (fi > c) conv2 = vcl * (c * ufacet + ee * ul);
+            }
+        }
+    } else {
+        if (HF_FLT_EQ(ul, ur)) {
+            conv2 = vcl * ufacet;
+        } else {
+            const double fi = (ufacet - ur) / (ul - ur);
+            if ((fi <= 0.0) || (fi >= 1.0)) {
+                conv2 = vcl * ufacet;
+            } else {
+                if (fi < b) conv2 = vcl * (a * ufacet - c * ur);
+                if ((fi >= b) && (fi <= c)) conv2 = vcl * (b * ul + c * ufacet - dd * ur);
+                if (fi > c) conv2 = vcl * (c * ul + ee * ufacet);
+            }
+        }
+    }
+    return make_double2(conv1, conv2);
+}
+
 // 128-thread blocks: the prefetched slots take ~170 registers per thread, and
 // three such blocks fit an SM where one 256-thread block would
 constexpr int kVelBlock = 128;
@@ -363,61 +430,10 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
                 dudxll[d2] = (ul - ull) / (1.0 * fd[d2]);
             } else if (second == HF_CUBISTA) {
                 const double vcr = SLQ(B + HF_V_VCR, F.u[d2]);
-                if (vcr > 0.0) {
-                    if (HF_FLT_EQ(ur, ul)) {
-                        conv1 = vcr * ufacet;
-                    } else {
-                        const double fi = (ufacet - ul) / (ur - ul);
-                        if ((fi <= 0.0) || (fi >= 1.0)) {
-                            conv1 = vcr * ufacet;
-                        } else {
-                            if (fi < b) conv1 = vcr * (a * ufacet - c * ul);
-                            if ((fi >= b) && (fi <= c)) conv1 = vcr * (c * ufacet + b * ur - dd * ul);
-                            if (fi > c) conv1 = vcr * (ee * ufacet + c * ur);
-                        }
-                    }
-                } else {
-                    if (HF_FLT_EQ(ufacet, urr)) {
-                        conv1 = vcr * ur;
-                    } else {
-                        const double fi = (ur - urr) / (ufacet - urr);
-                        if ((fi <= 0.0) || (fi >= 1.0)) {
-                            conv1 = vcr * ur;
-                        } else {
-                            if (fi < b) conv1 = infrr == 1 ? vcr * (a * ur - c * urr) : vcr * ur;
-                            if ((fi >= b) && (fi <= c)) conv1 = infrr == 1 ? vcr * (c * ur + b * ufacet - dd * urr) : vcr * ur;
-                            if (fi > c) conv1 = vcr * (c * ufacet + ee * ur);
-                        }
-                    }
-                }
                 const double vcl = SLQ(B + HF_V_VCL, F.u[d2]);
-                if (vcl > 0.0) {
-                    if (HF_FLT_EQ(ufacet, ull)) {
-                        conv2 = vcl * ul;
-                    } else {
-                        const double fi = (ul - ull) / (ufacet - ull);
-                        if ((fi <= 0.0) || (fi >= 1.0)) {
-                            conv2 = vcl * ul;
-                        } else {
-                            if (fi < b) conv2 = infll == 1 ? vcl * (a * ul - c * ull) : vcl * ul;
-                            if ((fi >= b) && (fi <= c)) conv2 = infll == 1 ? vcl * (b * ufacet + c * ul - dd * ull) : vcl * ul;
-                            if (fi > c) conv2 = vcl * (c * ufacet + ee * ul);
-                        }
-                    }
-                } else {
-                    if (HF_FLT_EQ(ul, ur)) {
-                        conv2 = vcl * ufacet;
-                    } else {
-                        const double fi = (ufacet - ur) / (ul - ur);
-                        if ((fi <= 0.0) || (fi >= 1.0)) {
-                            conv2 = vcl * ufacet;
-                        } else {
-                            if (fi < b) conv2 = vcl * (a * ufacet - c * ur);
-                            if ((fi >= b) && (fi <= c)) conv2 = vcl * (b * ul + c * ufacet - dd * ur);
-                            if (fi > c) conv2 = vcl * (c * ul + ee * ufacet);
-                        }
-                    }
-                }
+                const double2 cv = cubista_facet(ufacet, ul, ur, ull, urr, infll, infrr, vcr, vcl, conv1, conv2);
+                conv1 = cv.x;
+                conv2 = cv.y;
                 vc[d2] = ((conv1 - conv2) / fd[d]);
             }
         }
