@@ -523,13 +523,14 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 // ---------------------------------------------------------------------------
 // viscoelastic cell stage (Du, constitutive update, polymeric tensor)
 // ---------------------------------------------------------------------------
-// 128-thread blocks capped at 96 registers (2D): with the prefetched slot
-// values five such blocks (20 warps) fit an SM, where 256-thread blocks at the
-// uncapped ~100 registers would give 16 warps
+// 128-thread blocks capped at 64 registers in 2D (8 blocks, 32 warps per SM):
+// the kernel is latency bound, and occupancy beats the spills it costs
+// (measured on 4.29 M cells: 4 blocks 1.60 ms, 5: 1.38, 6: 1.31, 7: 1.24,
+// 8: 1.22, 16 at 32 registers: 1.19 with far more spill traffic)
 constexpr int kVeBlock = 128;
 
 template <int D>
-__global__ void __launch_bounds__(kVeBlock, D == 2 ? 5 : 4) k_ve_cell(DevProg P, DevFields F)
+__global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     if (cc >= P.ncell) return;
