@@ -1582,6 +1582,31 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         h.sblk = block_table(off, tail, l, true);
         h.ablk = block_table(off, tail, l, false);
     }
+    // the finest level's blocks carry their halo, for the kernels that stage a
+    // vector over the block's rows and halo in shared memory: every column the
+    // block's rows reach lies in [row0 + pad0, row0 + cnt + pad1), pad0 <= 0 <=
+    // pad1, and that range lies inside the level (columns are valid indices)
+    {
+        const int n0 = LH[0].n;
+        std::vector<int32_t> cmin(n0), cmax(n0);
+        for (int i = 0; i < n0; i++) {
+            cmin[i] = cmax[i] = i;
+            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
+                cmin[i] = std::min(cmin[i], mcol[k]);
+                cmax[i] = std::max(cmax[i], mcol[k]);
+            }
+        }
+        for (std::vector<Blk> *t : {&LH[0].sblk, &LH[0].ablk})
+            for (Blk &b : *t) {
+                int lo = b.row0, hi = b.row0 + b.cnt - 1;
+                for (int i = b.row0; i < b.row0 + b.cnt; i++) {
+                    lo = std::min(lo, cmin[i]);
+                    hi = std::max(hi, cmax[i]);
+                }
+                b.pad0 = lo - b.row0;
+                b.pad1 = hi - (b.row0 + b.cnt - 1);
+            }
+    }
 
     // every index the kernels follow must stay inside its array
     for (int l = 0; l < nlev; l++) {
@@ -1596,8 +1621,10 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         bool ok = l == 0 || cols_ok(h.Ap, h.Ac, h.n, h.n);
         if (ok && l + 1 < nlev) ok = cols_ok(h.Pp, h.Pc, h.n, nn) && cols_ok(h.Rp, h.Rc, nn, h.n);
         for (const std::vector<Blk> *t : {&h.sblk, &h.ablk})
-            for (const Blk &b : *t)
+            for (const Blk &b : *t) {
                 if (b.row0 < 0 || b.cnt <= 0 || b.cnt > kBlockRows || b.row0 + b.cnt > h.n) ok = false;
+                if (l == 0 && (b.pad0 > 0 || b.pad1 < 0 || b.row0 + b.pad0 < 0 || b.row0 + b.cnt + b.pad1 > h.n)) ok = false;
+            }
         if (!ok) return fail(HF_ERR_INVALID, "inconsistent multigrid level " + std::to_string(l));
     }
     for (int i = 0; i < ni && amg; i++) {
@@ -1606,6 +1633,41 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         if (tail[i] > clev[i] || clev[i] >= kMaxLevels) return fail(HF_ERR_INVALID, "inconsistent tail level");
     }
 
+    // the finest operator as row templates: rows with the same column offsets
+    // and values (in entry order) share one template
+    const int nf = C->P.ncell;
+    std::vector<uint32_t> rd(nf);
+    std::vector<int32_t> tp(1, 0), toff;
+    std::vector<double> tval;
+    {
+        std::unordered_map<std::string, uint32_t> seen;
+        std::string key;
+        for (int i = 0; i < nf; i++) {
+            key.clear();
+            const int len = mptr[i + 1] - mptr[i];
+            if (len >= (1 << kTLenBits)) return fail(HF_ERR_UNSUPPORTED, "Poisson row with more than 63 entries");
+            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
+                const int32_t o = mcol[k] - i;
+                key.append((const char *)&o, sizeof o);
+                key.append((const char *)&mval[k], sizeof(double));
+            }
+            auto it = seen.find(key);
+            if (it != seen.end()) {
+                rd[i] = it->second;
+                continue;
+            }
+            if (toff.size() + len >= ((size_t)1 << (32 - kTLenBits)))
+                return fail(HF_ERR_UNSUPPORTED, "too many distinct Poisson rows for the template table");
+            const uint32_t d = ((uint32_t)toff.size() << kTLenBits) | (uint32_t)len;
+            seen.emplace(key, d);
+            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
+                toff.push_back(mcol[k] - i);
+                tval.push_back(mval[k]);
+            }
+            tp.push_back((int32_t)toff.size());
+            rd[i] = d;
+        }
+    }
     // template forms of the operators and transfers the level-synchronous
     // kernels read (levels above the last tail start); the tails keep CSR
     if (amg) {
@@ -1648,40 +1710,6 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     std::vector<int32_t> ipin(pins.begin(), pins.end());
     const size_t o_pin = ar.vec(ipin);
     const size_t o_fblk = ar.vec(LH[0].ablk);
-    // the finest operator as row templates: rows with the same column offsets
-    // and values (in entry order) share one template
-    std::vector<uint32_t> rd(n);
-    std::vector<int32_t> tp(1, 0), toff;
-    std::vector<double> tval;
-    {
-        std::unordered_map<std::string, uint32_t> seen;
-        std::string key;
-        for (int i = 0; i < n; i++) {
-            key.clear();
-            const int len = mptr[i + 1] - mptr[i];
-            if (len >= (1 << kTLenBits)) return fail(HF_ERR_UNSUPPORTED, "Poisson row with more than 63 entries");
-            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
-                const int32_t o = mcol[k] - i;
-                key.append((const char *)&o, sizeof o);
-                key.append((const char *)&mval[k], sizeof(double));
-            }
-            auto it = seen.find(key);
-            if (it != seen.end()) {
-                rd[i] = it->second;
-                continue;
-            }
-            if (toff.size() + len >= ((size_t)1 << (32 - kTLenBits)))
-                return fail(HF_ERR_UNSUPPORTED, "too many distinct Poisson rows for the template table");
-            const uint32_t d = ((uint32_t)toff.size() << kTLenBits) | (uint32_t)len;
-            seen.emplace(key, d);
-            for (int k = mptr[i]; k < mptr[i + 1]; k++) {
-                toff.push_back(mcol[k] - i);
-                tval.push_back(mval[k]);
-            }
-            tp.push_back((int32_t)toff.size());
-            rd[i] = d;
-        }
-    }
     const size_t o_rd = ar.vec(rd), o_toff = ar.vec(toff), o_tval = ar.vec(tval);
     const size_t o_tval32 = mixed ? ar.vec(cast_vec<float>(tval)) : 0;
     C->ntemplates = (int64_t)tp.size() - 1;

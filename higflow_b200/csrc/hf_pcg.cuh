@@ -44,10 +44,18 @@ constexpr int kRPT = 4;
 constexpr int kBlockRows = kBlock * kRPT;
 
 // rows [row0, row0 + cnt) of instance inst at one level (cnt <= kBlockRows);
-// first/nblk: the instance's block range in the same table (for reductions)
+// first/nblk: the instance's block range in the same table (for reductions).
+// On the finest level pad0 <= 0 <= pad1 are the lowest and highest column
+// offsets the block's rows reach (its halo).
 struct Blk {
     int32_t row0, cnt, inst, first, nblk, pad0, pad1, pad2;
 };
+
+// A finest-level kernel that applies the operator to a vector it derives per
+// row (p = z + beta p_old) stages that vector over the block's rows and halo in
+// shared memory when the span fits: each value is then loaded and formed once
+// per block instead of once per referencing row.
+constexpr int kStageRows = kBlockRows + 1024;
 
 // Krylov state of one instance
 struct IScal {
@@ -654,6 +662,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
     const double beta = sc.beta;
     uint32_t d[kRPT];
     pcg::row_descs(G.A.rd, B, d);
+    __shared__ double sp[kStageRows];
+    const int s0 = B.row0 + B.pad0, ns = B.cnt + B.pad1 - B.pad0;
+    const bool staged = ns <= kStageRows;
+    if (staged) {
+        for (int j = threadIdx.x; j < ns; j += kBlock) sp[j] = first ? G.z[s0 + j] : G.z[s0 + j] + beta * po[s0 + j];
+        __syncthreads();
+    }
     double part[1] = {0.0};
 #pragma unroll
     for (int q = 0; q < kRPT; q++) {
@@ -661,7 +676,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
         if (t >= B.cnt) break;
         const int i = B.row0 + t;
         double qi, p;
-        if (first) {
+        if (staged) {
+            qi = trow_d(G.A, d[q], i, [&](int j) { return sp[j - s0]; });
+            p = sp[i - s0];
+        } else if (first) {
             qi = trow_d(G.A, d[q], i, [&](int j) { return G.z[j]; });
             p = G.z[i];
         } else {
