@@ -11,7 +11,7 @@ batch of the same population drawn with seed = rank (independent instances; no
 collective on the data path) and ``value`` is the cell-steps of all ranks over
 the slowest rank's device time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c1|cav2d_1024]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c4|c4_64|c1|cav2d_1024|cav3d_128]
   python bench.py --impl reference ...   # the reference's own CPU step
 """
 from __future__ import annotations
@@ -52,6 +52,12 @@ WORKLOADS = {
              "explicit Euler dt=1e-4, CUBISTA, incremental projection, Poisson CG to 1e-10 relative residual, "
              "zero initial fields",
         program="c1_cavity2d_64.prog.npz", dim=2, n=64, Re=100.0, dt=1e-4, precision="fp64",
+    ),
+    "cav3d_128": dict(
+        name="3D Newtonian lid-driven cavity 128^3 (uniform octree, unit cube), Re=400, lid u=1, explicit "
+             "Euler dt=1e-4, CUBISTA, incremental projection, AMG-CG Poisson to 1e-10 relative residual with "
+             "the V-cycle in FP32 (FP64 CG), zero initial fields; program tiled from the recorded 16^3 seed",
+        tiled=True, dim=3, n=128, Re=400.0, dt=1e-4, precision="mixed",
     ),
     "cav2d_1024": dict(
         name="2D Newtonian lid-driven cavity 1024x1024 (uniform quadtree, unit square), Re=100, lid u=1, "

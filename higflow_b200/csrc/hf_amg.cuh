@@ -3,7 +3,8 @@
 //
 // Host: the hierarchy is built once per program from the reduced Poisson
 // operator itself (no mesh geometry is needed, so AMR programs work too):
-// greedy aggregation on strong connections (|a_ij| >= theta sqrt(a_ii a_jj)),
+// greedy aggregation on strong connections (|a_ij| >= theta sqrt(a_ii a_jj),
+// theta = 0.08 halved per level),
 // a tentative piecewise-constant prolongator smoothed by one damped-Jacobi
 // step (P = (I - w D^-1 A) T, w = 4/3 over the Gershgorin bound of D^-1 A),
 // Galerkin coarse operators A_c = P^T A P, and a dense inverse of the coarsest
@@ -199,7 +200,12 @@ inline std::vector<HostLevel> build_hierarchy(HostCSR A, int max_coarse = 256, i
             break;
         }
         std::vector<int> agg;
-        const int na = aggregate(A, agg);
+        // strength threshold halved per level (0.08, 0.04, ...): the smoothed
+        // prolongator makes the Galerkin operators' off-diagonals small against
+        // their diagonals, and at a fixed 0.08 most level-1 rows of a 3D
+        // 7-point operator had no strong connection and stayed singletons
+        // (coarsening stalled, operator complexity 7.4 instead of 1.6)
+        const int na = aggregate(A, agg, 0.08 * std::pow(0.5, lev));
         if (na >= A.n * 0.95) {  // coarsening stalled: stop here
             h.A = std::move(A);
             L.push_back(std::move(h));
