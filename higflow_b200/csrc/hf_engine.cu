@@ -92,6 +92,12 @@ struct DevProg {
     const uint2 *vdesc;
     const int4 *vent;
     int vlenbits;
+    // semi-implicit Euler: the velocity kernel writes each direction's
+    // right-hand side, u + dt (sources - grad p [+ div S] - conv) plus the
+    // system's boundary part sie_bc, into sie_b instead of u*
+    int sie;
+    double *sie_b[3];
+    const double *sie_bc[3];
     const int32_t *dslots;
     const uint16_t *cdelta;
     const int32_t *cslots;
@@ -504,6 +510,20 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 #pragma unroll
     for (int d2 = 0; d2 < D; d2++) diff += du2dx2[d2];
     diff /= par.Re;
+    if (P.sie) {
+        // semi-implicit Euler (hig-flow-step.c:812-829; viscoelastic
+        // hig-flow-step-viscoelastic.c:1136-1147): diffusion moves to the
+        // system matrix; its boundary part is added to the right-hand side
+        double rhs = 0.0;
+        rhs += Fs;
+        rhs -= pterm;
+        if (VE) rhs += tens;
+        rhs -= conv;
+        rhs *= par.dt;
+        rhs += ufacet;
+        pick<3>(P.sie_b, d)[f] = rhs + __ldg(pick<3>(P.sie_bc, d) + f);
+        return;
+    }
     double rhs = 0.0;
     if (!VE) {
         rhs -= pterm;
@@ -917,6 +937,44 @@ __global__ void __launch_bounds__(kBlock) k_bi_update(DevMat M, BiVec V)
     }
 }
 
+// BiCGStab start on a given system: r = b - A x, scalars reset; first: the
+// tolerance from ||b|| (hf_slv_solve, the semi-implicit velocity systems)
+__global__ void __launch_bounds__(kBlock) k_slv_init(DevMat M, BiVec V, double rtol, double atol, int first)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double part[3] = {0.0, 0.0, 0.0};
+    if (i < M.n) {
+        double ax = 0.0;
+        for (int k = M.ptr[i]; k < M.ptr[i + 1]; k++) ax += M.val[k] * V.x[M.col[k]];
+        const double r = V.b[i] - ax;
+        V.r[i] = r;
+        V.rh[i] = r;
+        V.p[i] = 0.0;
+        V.v[i] = 0.0;
+        part[0] = r * r;
+        part[1] = V.b[i] * V.b[i];
+    }
+    double tot[3];
+    if (grid_sum<3>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
+        Scal &s = *V.sc;
+        s.rr = tot[0];
+        if (first) {
+            s.bb = tot[1];
+            const double t = fmax(rtol * sqrt(tot[1]), atol);
+            s.tol2 = t * t;
+            s.iters = 0;
+        }
+        s.rho = 1.0;
+        s.alpha = 1.0;
+        s.omega = 1.0;
+        s.rho1 = tot[0];
+        s.beta = 0.0;
+        s.status = 0;
+        s.done = !(tot[0] > s.tol2);
+        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // final velocity and pressure
 // ---------------------------------------------------------------------------
@@ -1004,6 +1062,14 @@ struct hf_case {
     DevMat M;
     BiVec bi;
     bool use_cg;
+    // semi-implicit Euler: per direction (I - dt/Re Lap_h) as CSR, solved by
+    // BiCGStab into u* (scratch Vu shared by the directions)
+    bool sie = false;
+    DevMat Mu[3] = {};
+    BiVec Vu{};
+    int64_t vel_iters = 0;          // their BiCGStab iterations, all steps
+    int64_t sie_launches = 0;       // their kernels, all steps
+    int sie_rc = 0;                 // status of the last step's solves
     // instances
     int ninst = 1;
     std::vector<int> coff;          // ninst + 1
@@ -1856,6 +1922,59 @@ void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, 
     }
 }
 
+// The semi-implicit velocity systems of one step (after the velocity kernel
+// wrote their right-hand sides): per direction BiCGStab with Jacobi scaling,
+// from u as the initial guess, into u*, to the Poisson solve's tolerances (the
+// reference hands both systems to the same solver engine).  Host-driven: the
+// host reads the scalars between chunks of iterations.
+int sie_solves(hf_case *C, int64_t &launches)
+{
+    cudaStream_t st = C->stream;
+    const double rtol = C->opt.poisson_rtol, atol = C->opt.poisson_atol;
+    for (int d = 0; d < C->D; d++) {
+        const DevMat &Mu = C->Mu[d];
+        const int n = Mu.n;
+        BiVec V = C->Vu;
+        V.x = C->F.us[d];
+        V.b = C->P.sie_b[d];
+        HF_CK(cudaMemcpyAsync(V.x, C->F.u[d], sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        Scal h{};
+        h.maxit = C->opt.poisson_maxit;
+        *C->h_scal = h;
+        HF_CK(cudaMemcpyAsync(V.sc, C->h_scal, sizeof(Scal), cudaMemcpyHostToDevice, st));
+        int restarts = 0, first = 1;
+        for (;;) {
+            k_slv_init<<<blocks(n), kBlock, 0, st>>>(Mu, V, rtol, atol, first);
+            launches++;
+            first = 0;
+            int chunk = 4;
+            for (;;) {
+                for (int k = 0; k < chunk; k++) {
+                    k_bi_p<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.ph, V.v, 0);
+                    k_bi_s<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.sh, V.t, 1);
+                    k_bi_update<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                    launches += 5;
+                }
+                HF_CK(cudaMemcpyAsync(C->h_scal, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+                HF_CK(cudaStreamSynchronize(st));
+                if (C->h_scal->done) break;
+                chunk = std::min(chunk * 2, 32);
+            }
+            if (C->h_scal->status == 1 && restarts++ < 50) continue;   // breakdown: restart from x
+            break;
+        }
+        HF_CK(cudaGetLastError());
+        const int status = C->h_scal->status;
+        if (status)
+            return fail(status == 1 ? HF_ERR_NOT_CONVERGED : status,
+                        "semi-implicit velocity BiCGStab failed in direction " + std::to_string(d));
+        C->vel_iters += C->h_scal->iters;
+    }
+    return HF_OK;
+}
+
 // a phase timing event; while a step graph is captured it becomes an
 // event-record node of the graph
 void record(hf_case *C, int phase, int end)
@@ -1887,6 +2006,7 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     }
     if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
     else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    if (C->sie) C->sie_rc = sie_solves(C, C->sie_launches);   // eager steps only (no graph for this form)
     record(C, HF_PHASE_VELOCITY, 1);
     record(C, HF_PHASE_POISSON_INIT, 0);
     k_pcg_extrapolate<<<blocks(C->P.ncell), kBlock, 0, st>>>(C->G);
@@ -1916,6 +2036,7 @@ int eager_step(hf_case *C)
     DevFields F = C->F;
     int fixed = 0, body = 0;
     enqueue_pre<D>(C, F, fixed);
+    if (C->sie_rc) return C->sie_rc;
     for (;;) {
         body = 0;
         enqueue_body(C, C->stream, 0, body);
@@ -2060,7 +2181,9 @@ int collect_phases(hf_case *C)
 template <int D>
 int graph_steps(hf_case *C, int nsteps, bool sync)
 {
-    const bool eager = C->opt.eager != 0;
+    // the semi-implicit form solves its velocity systems with a host-driven
+    // loop, so its steps run eagerly
+    const bool eager = C->opt.eager != 0 || C->sie;
     int rc = eager ? HF_OK : ensure_graphs<D>(C);
     if (rc) return rc;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
@@ -2114,6 +2237,10 @@ int bicg_step(hf_case *C)
         if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
         else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
         launches++;
+        if (C->sie) {
+            int rc = sie_solves(C, launches);
+            if (rc) return rc;
+        }
         t.stop(launches);
     }
     HF_CK(cudaGetLastError());
@@ -2431,6 +2558,89 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             UP(&F.Du[k], (const double *)nullptr, pg->ncell);
         }
     }
+    // semi-implicit Euler (higflow_semi_implicit_euler_intermediate_velocity,
+    // hig-flow-step.c:788-883): the row of facet f of direction d is
+    //   alpha u_f + sum_d2 w_d2 (S(f + delta_d2) + S(f - delta_d2)),
+    //   w_d2 = -dt / (Re delta_d2^2),  alpha = 1 - 2 sum_d2 w_d2,
+    // where S(point) is the point's interpolation stencil: the recorded UR / UL
+    // slots of block d2 (the same sfd_get_stencil queries, made there with
+    // weight 1); entries on one facet are added in stencil order, and each
+    // stencil's boundary term (w times the row's rhs) goes to the right-hand
+    // side, as sfd_get_stencil does with stn_add_to_rhs.
+    if (pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER) {
+        if (ni > 1) return cleanup(fail(HF_ERR_UNSUPPORTED, "semi-implicit Euler in a batch"));
+        C->sie = true;
+        P.sie = 1;
+        const double dt = pg->par.dt, Re = pg->par.Re;
+        int maxnf = 0;
+        for (int d = 0; d < D; d++) {
+            const int nf = pg->nfacet[d];
+            maxnf = std::max(maxnf, nf);
+            std::vector<int32_t> ptr(1, 0), col;
+            std::vector<double> val, dg(nf, 0.0), bc(nf, 0.0);
+            std::vector<std::pair<int32_t, double>> row;
+            auto add = [&](int32_t c, double v) {
+                for (auto &e : row)
+                    if (e.first == c) { e.second += v; return; }
+                row.emplace_back(c, v);
+            };
+            for (int f = 0; f < nf; f++) {
+                row.clear();
+                const double *fd = pg->delta + (size_t)pg->vel_delta[d][f] * D;
+                double alpha = 0.0, b = 0.0;
+                for (int d2 = 0; d2 < D; d2++) {
+                    const double w = -dt / (Re * fd[d2] * fd[d2]);
+                    alpha -= 2.0 * w;
+                    for (int side : {HF_V_UR, HF_V_UL}) {
+                        const int32_t code = pg->vel_slots[d][(size_t)(HF_V_BLK0 + HF_V_NB * d2 + side) * nf + f];
+                        if (code >= 0) {
+                            if (code >= nf) return cleanup(fail(HF_ERR_INVALID, "velocity slot outside its field"));
+                            add(code, w);
+                            continue;
+                        }
+                        const int64_t r = -(int64_t)code - 1;
+                        if (r >= pg->nrows) return cleanup(fail(HF_ERR_INVALID, "velocity slot outside the rows"));
+                        const int64_t t = pg->row_tmpl[r];
+                        for (int64_t k = pg->tmpl_ptr[t]; k < pg->tmpl_ptr[t + 1]; k++) {
+                            const int64_t c = (int64_t)pg->row_base[r] + pg->tmpl_col[k];
+                            if (c < 0 || c >= nf) return cleanup(fail(HF_ERR_INVALID, "stencil column outside its field"));
+                            add((int32_t)c, w * pg->tmpl_w[k]);
+                        }
+                        b += w * pg->row_rhs[r];
+                    }
+                }
+                alpha = 1.0 + alpha;
+                add(f, alpha);
+                for (auto &e : row) {
+                    col.push_back(e.first);
+                    val.push_back(e.second);
+                    if (e.first == f) dg[f] = e.second;
+                }
+                ptr.push_back((int32_t)col.size());
+                bc[f] = b;
+            }
+            for (int f = 0; f < nf; f++) dg[f] = dg[f] != 0.0 ? 1.0 / dg[f] : 1.0;
+            DevMat &Mu = C->Mu[d];
+            Mu.n = nf;
+            UP((int32_t **)&Mu.ptr, ptr.data(), ptr.size());
+            UP((int32_t **)&Mu.col, col.data(), col.size());
+            UP((double **)&Mu.val, val.data(), val.size());
+            UP((double **)&Mu.dinv, dg.data(), dg.size());
+            UP((double **)&P.sie_bc[d], bc.data(), bc.size());
+            UP(&P.sie_b[d], (const double *)nullptr, nf);
+        }
+        BiVec &V = C->Vu;
+        UP(&V.r, (const double *)nullptr, maxnf);
+        UP(&V.rh, (const double *)nullptr, maxnf);
+        UP(&V.p, (const double *)nullptr, maxnf);
+        UP(&V.v, (const double *)nullptr, maxnf);
+        UP(&V.s, (const double *)nullptr, maxnf);
+        UP(&V.t, (const double *)nullptr, maxnf);
+        UP(&V.ph, (const double *)nullptr, maxnf);
+        UP(&V.sh, (const double *)nullptr, maxnf);
+        UP(&V.partials, (const double *)nullptr, (size_t)blocks(maxnf) * 4);
+        UP(&V.sc, (const Scal *)nullptr, 1);
+    }
     // Poisson operator
     std::vector<int32_t> mptr, mcol;
     std::vector<double> mval, dinv, apin;
@@ -2584,7 +2794,7 @@ extern "C" int hf_case_stats(hf_case *C, hf_stats *out)
             s.last_residual = std::max(s.last_residual, q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr));
             s.total_iters += q.total_iters;
         }
-        s.kernel_launches = s.steps * C->fixed_kernels + C->h_ctl->total_bodies * C->body_kernels;
+        s.kernel_launches = s.steps * C->fixed_kernels + C->h_ctl->total_bodies * C->body_kernels + C->sie_launches;
     }
     *out = C->stats;
     out->last_outer = 1;
@@ -2724,41 +2934,6 @@ extern "C" void hf_case_destroy(hf_case *C)
 // ---------------------------------------------------------------------------
 namespace {
 
-__global__ void __launch_bounds__(kBlock) k_slv_init(DevMat M, BiVec V, double rtol, double atol, int first)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double part[3] = {0.0, 0.0, 0.0};
-    if (i < M.n) {
-        double ax = 0.0;
-        for (int k = M.ptr[i]; k < M.ptr[i + 1]; k++) ax += M.val[k] * V.x[M.col[k]];
-        const double r = V.b[i] - ax;
-        V.r[i] = r;
-        V.rh[i] = r;
-        V.p[i] = 0.0;
-        V.v[i] = 0.0;
-        part[0] = r * r;
-        part[1] = V.b[i] * V.b[i];
-    }
-    double tot[3];
-    if (grid_sum<3>(part, V.partials, &V.sc->counter, tot) && threadIdx.x == 0) {
-        Scal &s = *V.sc;
-        s.rr = tot[0];
-        if (first) {
-            s.bb = tot[1];
-            const double t = fmax(rtol * sqrt(tot[1]), atol);
-            s.tol2 = t * t;
-            s.iters = 0;
-        }
-        s.rho = 1.0;
-        s.alpha = 1.0;
-        s.omega = 1.0;
-        s.rho1 = tot[0];
-        s.beta = 0.0;
-        s.status = 0;
-        s.done = !(tot[0] > s.tol2);
-        if (!finite(tot[0])) { s.status = HF_ERR_NAN; s.done = 1; }
-    }
-}
 
 }  // namespace
 

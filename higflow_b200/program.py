@@ -19,6 +19,7 @@ import numpy as np
 
 # enumerations (include/higflow_b200.h)
 NEWTONIAN, VISCOELASTIC = 0, 3
+EXPLICIT_EULER, SEMI_IMPLICIT_EULER = 0, 3
 NON_INCREMENTAL, INCREMENTAL = 0, 1
 CENTRAL, FIRST_ORDER, SECOND_ORDER = 0, 1, 2
 MCU, CUBISTA, QUICK = 0, 1, 2
@@ -80,6 +81,7 @@ class HFParams(C.Structure):
         ("Re", C.c_double), ("dt", C.c_double),
         ("De", C.c_double), ("beta", C.c_double), ("kernel_tol", C.c_double),
         ("alpha", C.c_double), ("epsilon", C.c_double), ("xi", C.c_double),
+        ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
@@ -137,6 +139,10 @@ class HFStats(C.Structure):
 
 
 _PARAM_NAMES = [n for n, _ in HFParams._fields_]
+# parameters that programs written before they existed do not carry
+_PARAM_DEFAULTS = {"tempdiscrtype": 0, "pad_": 0}
+_INT_PARAMS = ("dim", "flowtype", "projtype", "convecdiscrtype", "secondconvecdiscrtype", "ve_model",
+               "ve_convecdiscrtype", "kernel", "tempdiscrtype", "pad_")
 
 
 def _np_from(ptr, n, dtype):
@@ -246,7 +252,7 @@ class Program:
 
         p = HFProgram()
         for n in _PARAM_NAMES:
-            setattr(p.par, n, self.par[n])
+            setattr(p.par, n, self.par.get(n, _PARAM_DEFAULTS.get(n, 0)))
         p.ncell = self.ncell
         for d in range(3):
             p.nfacet[d] = self.nfacet[d] if d < self.dim else 0
@@ -286,7 +292,7 @@ class Program:
             pars = (HFParams * n)()
             for i, ip in enumerate(self.inst_par):
                 for nm in _PARAM_NAMES:
-                    setattr(pars[i], nm, ip[nm])
+                    setattr(pars[i], nm, ip.get(nm, _PARAM_DEFAULTS.get(nm, 0)))
             keep.append(pars)
             p.ninst = n
             p.inst_par = C.cast(pars, C.POINTER(HFParams))
@@ -445,7 +451,8 @@ class Program:
     # ------------------------------------------------------------------
     def save(self, path: str) -> None:
         arrs = dict(
-            par_keys=np.array(_PARAM_NAMES), par_vals=np.array([float(self.par[n]) for n in _PARAM_NAMES]),
+            par_keys=np.array(_PARAM_NAMES),
+            par_vals=np.array([float(self.par.get(n, _PARAM_DEFAULTS.get(n, 0))) for n in _PARAM_NAMES]),
             ncell=np.int64(self.ncell), nfacet=np.array(self.nfacet, dtype=np.int64),
             delta=self.delta, row_tmpl=self.row_tmpl, row_base=self.row_base, row_rhs=self.row_rhs,
             tmpl_ptr=self.tmpl_ptr, tmpl_col=self.tmpl_col, tmpl_w=self.tmpl_w, div_slots=self.div_slots, cell_delta=self.cell_delta,
@@ -467,9 +474,9 @@ class Program:
         par = {}
         for k, v in zip(z["par_keys"], z["par_vals"]):
             k = str(k)
-            par[k] = int(v) if k in ("dim", "flowtype", "projtype", "convecdiscrtype",
-                                     "secondconvecdiscrtype", "ve_model",
-                                     "ve_convecdiscrtype", "kernel") else float(v)
+            par[k] = int(v) if k in _INT_PARAMS else float(v)
+        for k, v in _PARAM_DEFAULTS.items():
+            par.setdefault(k, v)
         dim = par["dim"]
         return cls(
             par=par, ncell=int(z["ncell"]), nfacet=[int(x) for x in z["nfacet"]],

@@ -57,6 +57,10 @@ enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order 
 enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2 };        /* VE model       */
 enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
 enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
+/* intermediate velocity (hig-flow-kernel.h:169-176); the semi-implicit form
+ * solves (I - dt/Re Lap_h) u* = u + dt (sources - grad p - conv [+ div S]) per
+ * direction (hig-flow-step.c:788-883, hig-flow-step-viscoelastic.c:1108-1210) */
+enum { HF_EXPLICIT_EULER = 0, HF_SEMI_IMPLICIT_EULER = 3 };
 
 /* precision forms */
 enum {
@@ -183,6 +187,8 @@ typedef struct hf_params {
     int32_t kernel;               /* HF_KERNEL_*                             */
     double Re, dt;
     double De, beta, kernel_tol, alpha, epsilon, xi;
+    int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER (contr.tempdiscrtype) */
+    int32_t pad_;
 } hf_params;
 
 /* A flattened step program (host memory, read-only for the engine). */

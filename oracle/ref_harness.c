@@ -45,6 +45,8 @@ typedef struct hfref_params {
     double bc_c[HFREF_MAXBC], bc_h[HFREF_MAXBC];
     double bc_p[HFREF_MAXBC];
     double k_init[3][3];        /* initial kernel tensor (get_tensor) */
+    int32_t tempdiscrtype;      /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER */
+    int32_t pad_;
 } hfref_params;
 
 typedef struct hfref_case {
@@ -182,7 +184,7 @@ int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
     ns->contr.projtype = p->projtype;
     ns->contr.flowtype = p->flowtype;
     ns->contr.eoflow = false;
-    ns->contr.tempdiscrtype = EXPLICIT_EULER;
+    ns->contr.tempdiscrtype = p->tempdiscrtype == HF_SEMI_IMPLICIT_EULER ? SEMI_IMPLICIT_EULER : EXPLICIT_EULER;
     ns->contr.spatialdiscrtype = ORDER2;
     ns->contr.convecdiscrtype = p->convecdiscrtype;
     ns->contr.secondconvecdiscrtype = p->secondconvecdiscrtype;

@@ -37,6 +37,7 @@ class RefParams(C.Structure):
         ("bc_tdim", C.c_int32 * MAXBC), ("bc_c", C.c_double * MAXBC), ("bc_h", C.c_double * MAXBC),
         ("bc_p", C.c_double * MAXBC),
         ("k_init", (C.c_double * 3) * 3),
+        ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
     ]
 
 
@@ -291,6 +292,7 @@ class CaseSpec:
         p.alpha = g("alpha", 0.2)
         p.epsilon = g("epsilon", 0.25)
         p.xi = g("xi", 0.0)
+        p.tempdiscrtype = g("tempdiscrtype", hp.EXPLICIT_EULER)
         for b, face in enumerate(self.faces):
             for d, v in enumerate(face.get("uval", [0.0] * self.dim)):
                 p.bc_u[b][d] = v

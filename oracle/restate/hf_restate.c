@@ -1,6 +1,6 @@
 /*
- * CPU restatement of HigFlow's explicit time step over a flattened step
- * program (test infrastructure: the oracle the GPU engine is checked against;
+ * CPU restatement of HigFlow's time step (explicit or semi-implicit Euler
+ * velocity) over a flattened step program (test infrastructure: the oracle the GPU engine is checked against;
  * never linked into the product).
  *
  * Each function follows the reference routine cited beside it, statement by
@@ -238,8 +238,174 @@ static void velocity_stage(const hf_program *P, hfr_fields *F, int d)
             rhs -= conv;
             rhs += diff;
         }
+        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER) {
+            /* higflow_semi_implicit_euler_intermediate_velocity
+             * (hig-flow-step.c:812-829; viscoelastic
+             * hig-flow-step-viscoelastic.c:1136-1147): the right-hand side
+             * without diffusion; the system is solved by sie_solve */
+            double r = 0.0;
+            r += Fs;
+            r -= pterm;
+            if (ve) {
+                double tens = 0.0;
+                for (int d2 = 0; d2 < D; d2++) tens += dSdx[d2];
+                r += tens;
+            }
+            r -= conv;
+            r *= P->par.dt;
+            r += ufacet;
+            F->us[d][f] = r;
+            continue;
+        }
         F->us[d][f] = ufacet + P->par.dt * rhs;
     }
+}
+
+/* ------------------------------------------------------------------ */
+/* semi-implicit Euler: the velocity system of direction d              */
+/* (hig-flow-step.c:830-883): row f = alpha u_f + sum_d2 w_d2 (S(f +    */
+/* delta_d2) + S(f - delta_d2)), w_d2 = -dt/(Re delta_d2^2), alpha = 1 - */
+/* 2 sum w_d2; S(point) = the recorded UR/UL stencils (sfd_get_stencil  */
+/* at fcenter +/- fdelta[d2], here scaled by w_d2); their boundary terms */
+/* (w times the row's rhs) join the right-hand side held in us[d].      */
+/* Solved by BiCGStab with Jacobi scaling from u.                       */
+/* ------------------------------------------------------------------ */
+typedef struct csr { int n; int64_t *ptr; int32_t *col; double *val; } csr;
+
+static double dot(int n, const double *a, const double *b);
+
+static void csr_spmv(const csr *A, const double *x, double *y)
+{
+    for (int i = 0; i < A->n; i++) {
+        double s = 0.0;
+        for (int64_t k = A->ptr[i]; k < A->ptr[i + 1]; k++) s += A->val[k] * x[A->col[k]];
+        y[i] = s;
+    }
+}
+
+static int csr_bicgstab(const csr *A, const double *bvec, double *x, double rtol)
+{
+    const int n = A->n;
+    double *mem = malloc(sizeof(double) * (size_t)n * 9);
+    double *r = mem, *rh = r + n, *p = rh + n, *v = p + n, *s = v + n, *t = s + n, *ph = t + n,
+           *sh = ph + n, *dinv = sh + n;
+    for (int i = 0; i < n; i++) {
+        double dg = 0.0;
+        for (int64_t k = A->ptr[i]; k < A->ptr[i + 1]; k++)
+            if (A->col[k] == i) dg += A->val[k];
+        dinv[i] = dg != 0.0 ? 1.0 / dg : 1.0;
+    }
+    csr_spmv(A, x, r);
+    for (int i = 0; i < n; i++) r[i] = bvec[i] - r[i];
+    const double bn = sqrt(dot(n, bvec, bvec));
+    const double tol = rtol * (bn > 0 ? bn : 1.0);
+    double rn = sqrt(dot(n, r, r));
+    memcpy(rh, r, sizeof(double) * (size_t)n);
+    memset(p, 0, sizeof(double) * (size_t)n);
+    memset(v, 0, sizeof(double) * (size_t)n);
+    double rho = 1.0, alpha = 1.0, omega = 1.0;
+    int it = 0, restarts = 0;
+    while (rn > tol && it < 200000) {
+        const double rho1 = dot(n, rh, r);
+        if (rho1 == 0.0 || omega == 0.0) {
+            if (++restarts > 100) break;
+            csr_spmv(A, x, r);
+            for (int i = 0; i < n; i++) r[i] = bvec[i] - r[i];
+            memcpy(rh, r, sizeof(double) * (size_t)n);
+            memset(p, 0, sizeof(double) * (size_t)n);
+            memset(v, 0, sizeof(double) * (size_t)n);
+            rho = alpha = omega = 1.0;
+            continue;
+        }
+        const double beta = (rho1 / rho) * (alpha / omega);
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        for (int i = 0; i < n; i++) ph[i] = dinv[i] * p[i];
+        csr_spmv(A, ph, v);
+        alpha = rho1 / dot(n, rh, v);
+        for (int i = 0; i < n; i++) s[i] = r[i] - alpha * v[i];
+        for (int i = 0; i < n; i++) sh[i] = dinv[i] * s[i];
+        csr_spmv(A, sh, t);
+        const double tt = dot(n, t, t);
+        omega = tt > 0.0 ? dot(n, t, s) / tt : 0.0;
+        for (int i = 0; i < n; i++) {
+            x[i] += alpha * ph[i] + omega * sh[i];
+            r[i] = s[i] - omega * t[i];
+        }
+        rho = rho1;
+        rn = sqrt(dot(n, r, r));
+        it++;
+        if (it % 50 == 0) {
+            csr_spmv(A, x, r);
+            for (int i = 0; i < n; i++) r[i] = bvec[i] - r[i];
+            rn = sqrt(dot(n, r, r));
+        }
+    }
+    free(mem);
+    return rn <= tol ? 0 : HF_ERR_NOT_CONVERGED;
+}
+
+static void row_add(int32_t *cols, double *vals, int *len, int32_t c, double v)
+{
+    for (int k = 0; k < *len; k++)
+        if (cols[k] == c) { vals[k] += v; return; }
+    cols[*len] = c;
+    vals[*len] = v;
+    (*len)++;
+}
+
+static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
+{
+    const int D = P->par.dim, nf = P->nfacet[d];
+    const double dt = P->par.dt, Re = P->par.Re;
+    /* entries per row: the centre plus 2D stencils of at most maxlen entries */
+    int64_t maxlen = 1;
+    for (int64_t t = 0; t < P->ntmpl; t++) {
+        const int64_t l = P->tmpl_ptr[t + 1] - P->tmpl_ptr[t];
+        if (l > maxlen) maxlen = l;
+    }
+    const int cap = (int)(1 + 2 * D * maxlen);
+    csr A;
+    A.n = nf;
+    A.ptr = malloc(sizeof(int64_t) * (size_t)(nf + 1));
+    A.col = malloc(sizeof(int32_t) * (size_t)nf * cap);
+    A.val = malloc(sizeof(double) * (size_t)nf * cap);
+    double *bvec = malloc(sizeof(double) * (size_t)nf);
+    double *x = F->us[d];
+    int32_t *rc = malloc(sizeof(int32_t) * cap);
+    double *rv = malloc(sizeof(double) * cap);
+    int64_t nz = 0;
+    A.ptr[0] = 0;
+    for (int f = 0; f < nf; f++) {
+        const double *fd = P->delta + (size_t)P->vel_delta[d][f] * D;
+        double alpha = 0.0, b = F->us[d][f];
+        int len = 0;
+        for (int d2 = 0; d2 < D; d2++) {
+            const double w = -dt / (Re * fd[d2] * fd[d2]);
+            alpha -= 2.0 * w;
+            const int sides[2] = {HF_V_UR, HF_V_UL};
+            for (int k = 0; k < 2; k++) {
+                const int32_t code = P->vel_slots[d][(size_t)(HF_V_BLK0 + HF_V_NB * d2 + sides[k]) * nf + f];
+                if (code >= 0) { row_add(rc, rv, &len, code, w); continue; }
+                const int64_t r = -(int64_t)code - 1;
+                const int64_t t = P->row_tmpl[r];
+                for (int64_t e = P->tmpl_ptr[t]; e < P->tmpl_ptr[t + 1]; e++)
+                    row_add(rc, rv, &len, (int32_t)(P->row_base[r] + P->tmpl_col[e]), w * P->tmpl_w[e]);
+                b += w * P->row_rhs[r];
+            }
+        }
+        alpha = 1.0 + alpha;
+        row_add(rc, rv, &len, f, alpha);
+        memcpy(A.col + nz, rc, sizeof(int32_t) * len);
+        memcpy(A.val + nz, rv, sizeof(double) * len);
+        nz += len;
+        A.ptr[f + 1] = nz;
+        bvec[f] = b;
+    }
+    /* initial guess u */
+    memcpy(x, F->u[d], sizeof(double) * (size_t)nf);
+    const int status = csr_bicgstab(&A, bvec, x, rtol);
+    free(A.ptr); free(A.col); free(A.val); free(bvec); free(rc); free(rv);
+    return status;
 }
 
 /* ------------------------------------------------------------------ */
@@ -801,6 +967,9 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
             polymeric_stage(P, F);
         }
         for (int d = 0; d < D; d++) velocity_stage(P, F, d);
+        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER)
+            for (int d = 0; d < D && rc == 0; d++) rc = sie_solve(P, F, d, rtol);
+        if (rc) break;
         rc = pressure_stage(P, F, rtol, iters);
         final_stage(P, F);
     }
@@ -813,6 +982,8 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
 void hfr_velocity(const hf_program *P, hfr_fields *F)
 {
     for (int d = 0; d < P->par.dim; d++) velocity_stage(P, F, d);
+    if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER)
+        for (int d = 0; d < P->par.dim; d++) sie_solve(P, F, d, 1e-14);
 }
 
 int hfr_pressure(const hf_program *P, hfr_fields *F, double rtol, int *iters)

@@ -56,6 +56,20 @@ CASES = {
                                                ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                                refine=[([0.5 / 12, 0.5 / 12], [((6, 6), (12, 12))])]),
                           3, (0.3, 0.1, 0.2)),
+    # semi-implicit Euler velocity (higflow_semi_implicit_euler_intermediate_velocity):
+    # a low-Re Newtonian cavity, an Oldroyd-B log cavity and a two-level
+    # Oldroyd-B case (the contraction configuration's form: non-symmetric
+    # Poisson rows at the level interface)
+    "sie2d_cubista": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
+                      4, (0.3, 0.1, 0.0)),
+    "sie2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                               tempdiscrtype=hp.SEMI_IMPLICIT_EULER), 3, (0.3, 0.1, 0.2)),
+    "amr2d_sie_oldroyd": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                               tempdiscrtype=hp.SEMI_IMPLICIT_EULER,
+                                               refine=[([0.5 / 12, 0.5 / 12], [((6, 6), (12, 12))])]),
+                          3, (0.3, 0.1, 0.2)),
 }
 
 

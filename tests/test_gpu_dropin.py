@@ -31,6 +31,10 @@ CASES = {
     "newtonian": lambda: refpy.cavity(2, 16, Re=100.0, dt=1e-3),
     "giesekus_log": lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GIESEKUS,
                                          kernel=hp.KERNEL_LOG, alpha=0.3, beta=0.1, De=0.5),
+    # semi-implicit Euler velocity (the reference's own slvu solvers on its side)
+    "oldroyd_sie": lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC, ve_model=hp.OLDROYD_B,
+                                        kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                        tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
 }
 
 

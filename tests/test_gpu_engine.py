@@ -176,3 +176,25 @@ def test_solver_engine_known_answer():
     assert L.hf_slv_get_x(s, x) == 0
     assert abs(x[0] - 1.0) < 1e-12 and abs(x[1] - 4.0) < 1e-12 and abs(x[2] + 2.0) < 1e-12
     L.hf_slv_destroy(s)
+
+
+def test_semi_implicit_velocity_refused_in_a_batch():
+    """The semi-implicit form solves each direction's velocity system on one
+    instance; a batch of such programs is refused at create."""
+    prog, _ = load_golden("sie2d_cubista")
+    batch = hp.Program.concatenate([prog, prog])
+    with pytest.raises(engine.EngineError) as e:
+        engine.Case(batch, _opts())
+    assert e.value.code == -2 and "semi-implicit" in str(e.value)   # HF_ERR_UNSUPPORTED
+
+
+def test_semi_implicit_velocity_iterates_and_counts_launches():
+    """A semi-implicit step runs eagerly and its velocity solves' kernels are
+    counted in the step statistics."""
+    prog, data = load_golden("sie2d_cubista")
+    case = engine.Case(prog, _opts())
+    load_init(case, prog, data)
+    case.step(2)
+    st = case.stats()
+    assert st.steps == 2 and st.kernel_launches > 2 * 10
+    case.close()
