@@ -163,6 +163,18 @@ int hf_sync_to_host(higflow_solver *ns)
     return copy_fields(b, k_out, (int)(sizeof k_out / sizeof k_out[0]), 0);
 }
 
+/* the other direction, for a case that changed its fields on the host: after
+ * higflow_load_properties (a restart from the reference's own checkpoint
+ * files, pdomain.c:1358-1385) or any edit of ns->dp*->values between steps.
+ * The source fields are copied as they are (the GPU path keeps them fixed);
+ * a new pressure also restarts the engine's initial-guess history. */
+int hf_sync_to_device(higflow_solver *ns)
+{
+    hf_binding *b = find(ns);
+    if (!b) return HF_ERR_INVALID;
+    return copy_fields(b, k_in, (int)(sizeof k_in / sizeof k_in[0]), 1);
+}
+
 void hf_detach(higflow_solver *ns)
 {
     hf_binding *b = find(ns);

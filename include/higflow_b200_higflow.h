@@ -15,6 +15,9 @@
  *                    (hig-flow-step-viscoelastic.c:2091)
  *   hf_sync_to_host  copies the device fields back into ns->dp*->values so
  *                    HigFlow's printers and savers see them
+ *   hf_sync_to_device copies ns->dp*->values (state and sources) to the
+ *                    device, after higflow_load_properties
+ *                    (higflow/src/hig-flow-io.c:5716) or a host-side edit
  *   hf_detach        syncs and frees the GPU state
  *   hf_solver_step   void wrapper with the reference's calling convention;
  *                    aborts with a message on a non-zero status, as the
@@ -39,6 +42,7 @@ const char *hf_flatten_error(void);
 int  hf_attach(struct higflow_solver *ns, const hf_options *opt);
 int  hf_step(struct higflow_solver *ns);
 int  hf_sync_to_host(struct higflow_solver *ns);
+int  hf_sync_to_device(struct higflow_solver *ns);
 void hf_detach(struct higflow_solver *ns);
 void hf_solver_step(struct higflow_solver *ns);
 

@@ -75,6 +75,7 @@ def lib(dim: int) -> C.CDLL:
         L.hf_attach.argtypes = [C.c_void_p, C.POINTER(hp.HFOptions)]
         L.hf_step.argtypes = [C.c_void_p]
         L.hf_sync_to_host.argtypes = [C.c_void_p]
+        L.hf_sync_to_device.argtypes = [C.c_void_p]
         L.hf_detach.argtypes = [C.c_void_p]
         L.hf_detach.restype = None
         L.hf_last_error.restype = C.c_char_p

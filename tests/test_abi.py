@@ -38,7 +38,8 @@ def test_binding_exports_the_higflow_facing_header():
     if not os.path.exists(BINDING):
         pytest.skip("binding build (oracle/_ref) not present")
     names = _declared("higflow_b200_higflow.h")
-    assert set(names) >= {"hf_flatten", "hf_attach", "hf_step", "hf_sync_to_host", "hf_detach", "hf_solver_step"}
+    assert set(names) >= {"hf_flatten", "hf_attach", "hf_step", "hf_sync_to_host", "hf_sync_to_device", "hf_detach",
+                          "hf_solver_step"}
     missing = sorted(set(names) - _exported(BINDING))
     assert not missing, missing
     # the link-time interposition targets for the case main loop

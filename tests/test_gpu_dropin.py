@@ -104,3 +104,40 @@ def test_detach_leaves_the_gpu_fields_on_the_host():
     u = gpu.get(hp.FIELD_U, 0)
     assert np.abs(u).max() > 0.0  # the lid has started to drive the flow
     gpu.close()
+
+
+def test_sync_to_device_after_a_host_side_restart():
+    """A case that replaces its fields on the host between steps (as after
+    higflow_load_properties) pushes them to the GPU with hf_sync_to_device;
+    the GPU then steps from the new state exactly as the reference does."""
+    if not refpy.available(2):
+        pytest.skip("oracle build of the reference not present")
+    ref = refpy.RefCase(CASES["giesekus_log"]())
+    gpu = refpy.RefCase(CASES["giesekus_log"]())
+    _perturb(ref, True)
+    _perturb(gpu, True)
+    ref.flatten()
+    ref.step(2)
+    L = gpu.L
+    opts = engine.options(rtol=1e-13, atol=1e-300)
+    assert L.hf_attach(gpu.ns, C.byref(opts)) == 0, L.hf_last_error()
+    for _ in range(2):
+        assert L.hf_step(gpu.ns) == 0, L.hf_last_error()
+    # both copies load the same new u, p and K (a restart; the other fields
+    # stay as the steps left them, so the GPU copy syncs them out first), then
+    # step twice more
+    assert L.hf_sync_to_host(gpu.ns) == 0, L.hf_last_error()
+    _perturb(ref, True, seed=5)
+    _perturb(gpu, True, seed=5)
+    assert L.hf_sync_to_device(gpu.ns) == 0, L.hf_last_error()
+    ref.step(2)
+    for _ in range(2):
+        assert L.hf_step(gpu.ns) == 0, L.hf_last_error()
+    assert L.hf_sync_to_host(gpu.ns) == 0, L.hf_last_error()
+    want, got = _fields(ref, True), _fields(gpu, True)
+    for k in want:
+        err = np.linalg.norm(got[k] - want[k]) / max(np.linalg.norm(want[k]), 1e-300)
+        assert err < TOL, (k, err)
+    L.hf_detach(gpu.ns)
+    ref.close()
+    gpu.close()
