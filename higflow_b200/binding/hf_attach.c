@@ -205,6 +205,35 @@ void hf_solver_step(higflow_solver *ns)
     }
 }
 
+/* higflow_adjust_timestep (hig-flow-timestep.c:115-139) on the GPU state:
+ * the engine computes the CFL number from its velocity and sets the new dt,
+ * which is written back to ns->par.dt as the reference does */
+int hf_adjust_timestep(higflow_solver *ns)
+{
+    hf_binding *b = find(ns);
+    if (!b) return HF_ERR_INVALID;
+    double cfl = 0.0, dt = 0.0;
+    int rc = hf_case_adjust_timestep(b->c, &cfl, &dt, 1);
+    if (rc == HF_OK) ns->par.dt = dt;
+    return rc;
+}
+
 /* targets of -Wl,--wrap=higflow_solver_step[_viscoelastic] */
 void __wrap_higflow_solver_step(higflow_solver *ns) { hf_solver_step(ns); }
 void __wrap_higflow_solver_step_viscoelastic(higflow_solver *ns) { hf_solver_step(ns); }
+/* target of -Wl,--wrap=higflow_adjust_timestep: the GPU state's CFL; an
+ * unattached case keeps the reference's own routine (weak: links that wrap
+ * only the step functions do not define the __real_ alias) */
+extern void __real_higflow_adjust_timestep(higflow_solver *ns) __attribute__((weak));
+void __wrap_higflow_adjust_timestep(higflow_solver *ns)
+{
+    if (!find(ns)) {
+        if (__real_higflow_adjust_timestep) __real_higflow_adjust_timestep(ns);
+        return;
+    }
+    const int rc = hf_adjust_timestep(ns);
+    if (rc) {
+        fprintf(stderr, "higflow_b200: adaptive time step failed (%d): %s\n", rc, hf_last_error());
+        exit(1);
+    }
+}

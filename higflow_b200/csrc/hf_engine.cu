@@ -937,6 +937,34 @@ __global__ void __launch_bounds__(kBlock) k_bi_update(DevMat M, BiVec V)
     }
 }
 
+// CFL number of every instance (higflow_compute_CFL, hig-flow-timestep.c:7-40):
+// per cell, sum over d of |(u_l + u_r) / 2| / (the cell's face area normal to d),
+// u_l and u_r the face velocities (the divergence's own queries, on u); the
+// instance's maximum by an atomic max on the bit patterns (non-negative doubles
+// order as their bits, so the result does not depend on the order).
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_cfl(DevProg P, DevFields F, unsigned long long *imax)
+{
+    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cc >= P.ncell) return;
+    const int n = P.ncell;
+    const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
+    double u_dx_norm = 0.0;
+#pragma unroll
+    for (int dim = 0; dim < D; dim++) {
+        const double ul = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UL(dim) * n + cc), F.u[dim]);
+        const double ur = hf::query(P.rows, __ldg(P.dslots + (size_t)HF_P_UR(dim) * n + cc), F.u[dim]);
+        const double u = (ul + ur) / 2.0;
+        double facet_area = 1.0;
+#pragma unroll
+        for (int dim2 = 0; dim2 < D; dim2++)
+            if (dim2 != dim) facet_area *= cd[dim2];
+        u_dx_norm += fabs(u) / facet_area;
+    }
+    if (u_dx_norm > 0.0)
+        atomicMax(imax + __ldg(P.cinst + cc), (unsigned long long)__double_as_longlong(u_dx_norm));
+}
+
 // BiCGStab start on a given system: r = b - A x, scalars reset; first: the
 // tolerance from ||b|| (hf_slv_solve, the semi-implicit velocity systems)
 __global__ void __launch_bounds__(kBlock) k_slv_init(DevMat M, BiVec V, double rtol, double atol, int first)
@@ -1070,6 +1098,9 @@ struct hf_case {
     int64_t vel_iters = 0;          // their BiCGStab iterations, all steps
     int64_t sie_launches = 0;       // their kernels, all steps
     int sie_rc = 0;                 // status of the last step's solves
+    std::vector<hf_params> h_ipar;  // per-instance parameters as last uploaded
+    std::vector<double> dt0;        // per-instance dt at create (adaptive time step)
+    unsigned long long *cfl_max = nullptr;   // per-instance CFL scratch
     // instances
     int ninst = 1;
     std::vector<int> coff;          // ninst + 1
@@ -2433,6 +2464,10 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             UP((int32_t **)&P.finst[d], finst.data(), finst.size());
         }
         UP((hf_params **)&P.ipar, ipar.data(), ipar.size());
+        C->h_ipar = ipar;
+        C->dt0.resize(ni);
+        for (int i = 0; i < ni; i++) C->dt0[i] = ipar[i].dt;
+        UP(&C->cfl_max, (const unsigned long long *)nullptr, ni);
         UP((double **)&P.ipinv, pinv.data(), pinv.size());
     }
     UP((double **)&P.delta, pg->delta, (size_t)pg->ndelta * D);
@@ -2825,6 +2860,46 @@ extern "C" int hf_case_instance_result(hf_case *C, int32_t inst, int32_t *iters,
     if (iters) *iters = q.iters;
     if (status) *status = q.status;
     if (residual) *residual = q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr);
+    return HF_OK;
+}
+
+// Adaptive time step (higflow_adjust_timestep, hig-flow-timestep.c:115-139),
+// every instance on its own CFL number.  Waits for the case's stream.
+extern "C" int hf_case_adjust_timestep(hf_case *C, double *cfl, double *dt, int32_t n)
+{
+    if (!C) return fail(HF_ERR_INVALID, "null case");
+    if ((cfl || dt) && n != C->ninst) return fail(HF_ERR_INVALID, "array size is not the instance count");
+    if (C->sie) return fail(HF_ERR_UNSUPPORTED, "adaptive time step with the semi-implicit velocity (its matrix holds dt)");
+    const int ni = C->ninst;
+    cudaStream_t st = C->stream;
+    if (C->D == 2 || C->D == 3) {
+        HF_CK(cudaMemsetAsync(C->cfl_max, 0, sizeof(unsigned long long) * ni, st));
+        if (C->D == 2) k_cfl<2><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F, C->cfl_max);
+        else k_cfl<3><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F, C->cfl_max);
+        HF_CK(cudaGetLastError());
+    }
+    std::vector<unsigned long long> bits(ni);
+    HF_CK(cudaMemcpyAsync(bits.data(), C->cfl_max, sizeof(unsigned long long) * ni, cudaMemcpyDeviceToHost, st));
+    HF_CK(cudaStreamSynchronize(st));
+    const double max_cfl = 0.1, max_dt_factor = 1.1;   // MAX_CFL, MAX_DT_FACTOR (hig-flow-timestep.h:13-14)
+    for (int i = 0; i < ni; i++) {
+        double norm;
+        memcpy(&norm, &bits[i], sizeof norm);
+        hf_params &par = C->h_ipar[i];
+        const double c = norm * par.dt;
+        const double dtmax = C->dt0[i] * 32.0;
+        const double dt_factor = std::min(max_cfl / (c + 1.0e-12), max_dt_factor);
+        const double newdt = dt_factor * par.dt;
+        par.dt = std::min(newdt, dtmax);
+        if (cfl) cfl[i] = c;
+        if (dt) dt[i] = par.dt;
+    }
+    // the kernels read dt from the device parameter array (captured step
+    // graphs included), so the next step uses the new values
+    HF_CK(cudaMemcpyAsync((void *)C->P.ipar, C->h_ipar.data(), sizeof(hf_params) * ni, cudaMemcpyHostToDevice, st));
+    HF_CK(cudaStreamSynchronize(st));
+    C->par.dt = C->h_ipar[0].dt;
+    C->P.par.dt = C->h_ipar[0].dt;
     return HF_OK;
 }
 

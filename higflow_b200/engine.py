@@ -43,6 +43,7 @@ def lib() -> C.CDLL:
         L.hf_case_step_async.argtypes = [V, C.c_int32]
         L.hf_case_launch_counts.argtypes = [V, P(C.c_int32), P(C.c_int32)]
         L.hf_case_instance_iters.argtypes = [V, P(C.c_int64), C.c_int32]
+        L.hf_case_adjust_timestep.argtypes = [V, P(C.c_double), P(C.c_double), C.c_int32]
         L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
         L.hf_case_synchronize.argtypes = [V]
         L.hf_case_destroy.argtypes = [V]
@@ -118,6 +119,16 @@ class Case:
         out = np.zeros(n, dtype=np.int64)
         _check(lib().hf_case_instance_iters(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), n))
         return out
+
+    def adjust_timestep(self):
+        """Adaptive time step of every instance (higflow_adjust_timestep):
+        returns (CFL numbers, new time steps), one per instance."""
+        n = self.instances()
+        cfl = np.zeros(n)
+        dt = np.zeros(n)
+        _check(lib().hf_case_adjust_timestep(self.h, cfl.ctypes.data_as(C.POINTER(C.c_double)),
+                                             dt.ctypes.data_as(C.POINTER(C.c_double)), n))
+        return cfl, dt
 
     def launch_counts(self):
         """(kernels per step outside the Poisson loop, kernels per loop body)."""

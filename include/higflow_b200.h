@@ -319,6 +319,15 @@ int  hf_case_instance_result(hf_case *c, int32_t inst, int32_t *iters, int32_t *
 /* Poisson iterations of every instance summed over all steps so far (n = ninst). */
 int  hf_case_instance_iters(hf_case *c, int64_t *total_iters, int32_t n);
 
+/* Adaptive time step (higflow_adjust_timestep, higflow/src/hig-flow-timestep.c:
+ * 115-139), each instance on its own CFL number: CFL = dt * max over cells of
+ * sum_d |(u_l + u_r)/2| / (face area normal to d); dt <- min(min(0.1/(CFL +
+ * 1e-12), 1.1) dt, 32 dt0), dt0 = the instance's dt at create.  Writes each
+ * instance's CFL and new dt (n = ninst; either array may be null); the next
+ * steps use the new dt.  HF_ERR_UNSUPPORTED for the semi-implicit velocity,
+ * whose system matrix holds dt. */
+int  hf_case_adjust_timestep(hf_case *c, double *cfl, double *dt, int32_t n);
+
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);
 

@@ -43,6 +43,9 @@ int  hf_attach(struct higflow_solver *ns, const hf_options *opt);
 int  hf_step(struct higflow_solver *ns);
 int  hf_sync_to_host(struct higflow_solver *ns);
 int  hf_sync_to_device(struct higflow_solver *ns);
+/* higflow_adjust_timestep on the GPU state (hf_case_adjust_timestep); sets
+ * ns->par.dt */
+int  hf_adjust_timestep(struct higflow_solver *ns);
 void hf_detach(struct higflow_solver *ns);
 void hf_solver_step(struct higflow_solver *ns);
 

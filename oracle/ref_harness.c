@@ -22,6 +22,7 @@
 #include "hig-flow-kernel.h"
 #include "hig-flow-ic.h"
 #include "hig-flow-bc.h"
+#include "hig-flow-timestep.h"
 #include "hig-flow-step.h"
 #include "hig-flow-step-viscoelastic.h"
 #include "hig-flow-step-generalized-newtonian.h"
@@ -380,6 +381,23 @@ double hfref_time(hfref_case *C) { return C->ns->par.t; }
 
 /* the case's higflow_solver, for the drop-in binding (hf_attach & co.) */
 void *hfref_ns(hfref_case *C) { return C->ns; }
+
+/* the case's current time step (ns->par.dt), and the reference's own CFL
+ * number and adaptive step on its state (hig-flow-timestep.c:7-40, :115-139;
+ * both print through print0f, silenced here like the rest of the harness) */
+double hfref_dt(hfref_case *C) { return C->ns->par.dt; }
+
+double hfref_cfl(hfref_case *C)
+{
+    g_cur = C;
+    return higflow_compute_CFL(C->ns);
+}
+
+void hfref_adjust_timestep(hfref_case *C)
+{
+    g_cur = C;
+    higflow_adjust_timestep(C->ns);
+}
 
 /* flatten through the binding (hf_flatten) and hand the program to Python */
 int hfref_flatten(hfref_case *C, hf_program **out)

@@ -71,6 +71,13 @@ def lib(dim: int) -> C.CDLL:
                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.hfref_ns.argtypes = [C.c_void_p]
         L.hfref_ns.restype = C.c_void_p
+        L.hfref_dt.argtypes = [C.c_void_p]
+        L.hfref_dt.restype = C.c_double
+        L.hfref_cfl.argtypes = [C.c_void_p]
+        L.hfref_cfl.restype = C.c_double
+        L.hfref_adjust_timestep.argtypes = [C.c_void_p]
+        L.hfref_adjust_timestep.restype = None
+        L.hf_adjust_timestep.argtypes = [C.c_void_p]
         # the drop-in binding linked into the same library (product code under test)
         L.hf_attach.argtypes = [C.c_void_p, C.POINTER(hp.HFOptions)]
         L.hf_step.argtypes = [C.c_void_p]
@@ -187,6 +194,18 @@ class RefCase:
     @property
     def t(self) -> float:
         return self.L.hfref_time(self.h)
+
+    @property
+    def dt(self) -> float:
+        return self.L.hfref_dt(self.h)
+
+    def cfl(self) -> float:
+        """The reference's own CFL number of the current velocity."""
+        return self.L.hfref_cfl(self.h)
+
+    def adjust_timestep(self) -> None:
+        """The reference's own adaptive time step (sets its dt)."""
+        self.L.hfref_adjust_timestep(self.h)
 
     @property
     def ns(self) -> int:

@@ -38,6 +38,8 @@ def lib():
         L.hfr_final.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields)]
         L.hfr_ve_cell.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields)]
         L.hfr_divergence_rhs.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields), _D]
+        L.hfr_cfl.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields)]
+        L.hfr_cfl.restype = C.c_double
         _lib = L
     return _lib
 
@@ -120,3 +122,7 @@ class State:
         b = np.zeros(self.prog.ncell)
         lib().hfr_divergence_rhs(C.byref(self.cprog), C.byref(self.f), b.ctypes.data_as(_D))
         return b
+
+    def cfl(self) -> float:
+        """CFL number of the current velocity (higflow_compute_CFL)."""
+        return lib().hfr_cfl(C.byref(self.cprog), C.byref(self.f))

@@ -1024,3 +1024,27 @@ void hfr_divergence_rhs(const hf_program *P, hfr_fields *F, double *bvec)
     if (P->pin_row >= 0)
         bvec[P->pin_row] = P->par.projtype == HF_INCREMENTAL ? P->pin_value - F->p[P->pin_row] : P->pin_value;
 }
+
+/* CFL number (higflow_compute_CFL, hig-flow-timestep.c:7-40): dt times the
+ * largest over cells of sum_d |(u_l + u_r)/2| / (the face area normal to d),
+ * u_l, u_r the face velocities from the divergence's own queries on u */
+double hfr_cfl(const hf_program *P, hfr_fields *F)
+{
+    const int D = P->par.dim, n = P->ncell;
+    double maxu_dx_norm = 0.0;
+    for (int cc = 0; cc < n; cc++) {
+        const double *cd = P->delta + (size_t)P->cell_delta[cc] * D;
+        double u_dx_norm = 0.0;
+        for (int dim = 0; dim < D; dim++) {
+            const double ul = q(P, P->div_slots[(size_t)HF_P_UL(dim) * n + cc], F->u[dim]);
+            const double ur = q(P, P->div_slots[(size_t)HF_P_UR(dim) * n + cc], F->u[dim]);
+            const double u = (ul + ur) / 2.0;
+            double facet_area = 1.0;
+            for (int dim2 = 0; dim2 < D; dim2++)
+                if (dim2 != dim) facet_area *= cd[dim2];
+            u_dx_norm += fabs(u) / facet_area;
+        }
+        if (u_dx_norm > maxu_dx_norm) maxu_dx_norm = u_dx_norm;
+    }
+    return maxu_dx_norm * P->par.dt;
+}

@@ -141,3 +141,28 @@ def test_sync_to_device_after_a_host_side_restart():
     L.hf_detach(gpu.ns)
     ref.close()
     gpu.close()
+
+
+def test_adjust_timestep_through_the_binding_matches_the_reference():
+    """hf_adjust_timestep (the target of -Wl,--wrap=higflow_adjust_timestep)
+    sets ns->par.dt from the GPU state as the reference's own routine does
+    from its host state."""
+    if not refpy.available(2):
+        pytest.skip("oracle build of the reference not present")
+    ref = refpy.RefCase(CASES["newtonian"]())
+    gpu = refpy.RefCase(CASES["newtonian"]())
+    _perturb(ref, False)
+    _perturb(gpu, False)
+    ref.flatten()
+    L = gpu.L
+    opts = engine.options(rtol=1e-13, atol=1e-300)
+    assert L.hf_attach(gpu.ns, C.byref(opts)) == 0, L.hf_last_error()
+    ref.step(2)
+    for _ in range(2):
+        assert L.hf_step(gpu.ns) == 0, L.hf_last_error()
+    ref.adjust_timestep()
+    assert L.hf_adjust_timestep(gpu.ns) == 0, L.hf_last_error()
+    assert abs(gpu.dt - ref.dt) <= 1e-10 * ref.dt, (gpu.dt, ref.dt)
+    L.hf_detach(gpu.ns)
+    ref.close()
+    gpu.close()

@@ -198,3 +198,75 @@ def test_semi_implicit_velocity_iterates_and_counts_launches():
     st = case.stats()
     assert st.steps == 2 and st.kernel_launches > 2 * 10
     case.close()
+
+
+def _random_velocity(obj, prog, seed, amp=0.7):
+    rng = np.random.default_rng(seed)
+    for d in range(prog.dim):
+        obj.set(hp.FIELD_U, d, amp * rng.standard_normal(prog.nfacet[d]))
+
+
+@pytest.mark.parametrize("name", ["cav2d_cubista", "ve2d_oldroyd_log", "cav3d_cubista"])
+def test_adaptive_timestep_matches_restatement(name):
+    """hf_case_adjust_timestep: the CFL number of the device velocity against the
+    restatement's (higflow_compute_CFL) and the reference's update of dt."""
+    prog, _ = load_golden(name)
+    case = engine.Case(prog, _opts())
+    st = restate.State(prog)
+    _random_velocity(case, prog, 1)
+    _random_velocity(st, prog, 1)
+    dt0 = prog.par["dt"]
+    cfl, dt = case.adjust_timestep()
+    want = st.cfl()
+    assert abs(cfl[0] - want) <= 1e-13 * want, (cfl, want)
+    assert abs(dt[0] - min(min(0.1 / (want + 1e-12), 1.1) * dt0, 32 * dt0)) <= 1e-15 * dt[0]
+    case.close()
+
+
+def test_adaptive_timestep_per_instance_in_a_batch():
+    """Each instance of a batch adapts its own dt from its own CFL number, and
+    the next step uses it: a batch member steps as a case created with the new dt."""
+    names = ["cav2d_cubista", "cav2d_lid"]
+    progs = [load_golden(n)[0] for n in names]
+    batch = hp.Program.concatenate(progs)
+    case = engine.Case(batch, _opts())
+    alone = []
+    for i, p in enumerate(progs):
+        c = engine.Case(p, _opts())
+        _random_velocity(c, p, 10 + i, 0.7 * (1 + 9 * i))   # the second one's CFL limits its step
+        alone.append((c, c.adjust_timestep()))
+    # the same velocity per instance in the batch
+    for i, p in enumerate(progs):
+        rng = np.random.default_rng(10 + i)
+        for d in range(p.dim):
+            u = case.get(hp.FIELD_U, d)
+            off = batch.facet_off[d]
+            u[off[i]:off[i + 1]] = 0.7 * (1 + 9 * i) * rng.standard_normal(p.nfacet[d])
+            case.set(hp.FIELD_U, d, u)
+    cfl, dt = case.adjust_timestep()
+    for i, (c, (ca, dta)) in enumerate(alone):
+        assert abs(cfl[i] - ca[0]) <= 1e-14 * ca[0] and abs(dt[i] - dta[0]) <= 1e-15 * dta[0], (i, cfl, ca)
+    assert dt[0] != dt[1]
+    # one step with the adapted dt, against a fresh case created with that dt
+    p2 = hp.Program.load(__import__("os").path.join(__import__("tests.helpers", fromlist=["GOLDEN"]).GOLDEN,
+                                                      names[0] + ".prog.npz"))
+    p2.par["dt"] = float(dt[0])
+    ref = engine.Case(p2, _opts())
+    _random_velocity(ref, p2, 10)
+    case.step(1)
+    ref.step(1)
+    u = case.get_instance(hp.FIELD_U, 0, 0)
+    ur = ref.get(hp.FIELD_U, 0)
+    assert np.linalg.norm(u - ur) <= TOL * np.linalg.norm(ur)
+    for c, _ in alone:
+        c.close()
+    ref.close()
+    case.close()
+
+
+def test_adaptive_timestep_refused_for_semi_implicit():
+    prog, _ = load_golden("sie2d_cubista")
+    case = engine.Case(prog, _opts())
+    with pytest.raises(engine.EngineError):
+        case.adjust_timestep()
+    case.close()

@@ -151,3 +151,30 @@ def test_program_roundtrip(tmp_path):
     assert np.array_equal(q.cell_slots, prog.cell_slots)
     c = q.to_c()
     assert c.ncell == prog.ncell and c.vel_nslot == prog.vel_slots[0].shape[0]
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not present")
+@pytest.mark.parametrize("dim,ve", [(2, False), (2, True), (3, False)])
+def test_cfl_matches_reference(dim, ve):
+    """The restated CFL number (higflow_compute_CFL, hig-flow-timestep.c:7-40)
+    against the reference's own on the same random velocity, and the adaptive
+    step's formula against the reference's higflow_adjust_timestep."""
+    kw = dict(Re=10.0, dt=1e-3)
+    if ve:
+        kw.update(flowtype=hp.VISCOELASTIC, ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG)
+    c = refpy.RefCase(refpy.cavity(dim, 12 if dim == 2 else 6, **kw))
+    rng = np.random.default_rng(3)
+    for d in range(dim):
+        c.set(hp.FIELD_U, d, 0.7 * rng.standard_normal(c.nfacet[d]))
+    prog = c.flatten()   # also warms HigTree's stencil cache, as every step after the first reads it
+    st = restate.State(prog)
+    for d in range(dim):
+        st.set(hp.FIELD_U, d, c.get(hp.FIELD_U, d))
+    want = c.cfl()
+    got = st.cfl()
+    assert abs(got - want) <= 1e-14 * abs(want), (got, want)
+    dt0 = c.dt
+    c.adjust_timestep()
+    expect = min(min(0.1 / (want + 1e-12), 1.1) * dt0, 32 * dt0)
+    assert abs(c.dt - expect) <= 1e-15 * expect, (c.dt, expect)
+    c.close()
