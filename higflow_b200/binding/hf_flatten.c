@@ -268,8 +268,9 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
     *out = NULL;
     g_err[0] = 0;
     if (ns->contr.spatialdiscrtype != ORDER2) return REASON(HF_ERR_UNSUPPORTED, "spatial discretisation is not second order");
-    if (ns->contr.tempdiscrtype != EXPLICIT_EULER && ns->contr.tempdiscrtype != SEMI_IMPLICIT_EULER)
-        return REASON(HF_ERR_UNSUPPORTED, "time discretisation is neither explicit nor semi-implicit Euler");
+    if (ns->contr.tempdiscrtype != EXPLICIT_EULER && ns->contr.tempdiscrtype != EXPLICIT_RK2 &&
+        ns->contr.tempdiscrtype != EXPLICIT_RK3 && ns->contr.tempdiscrtype != SEMI_IMPLICIT_EULER)
+        return REASON(HF_ERR_UNSUPPORTED, "time discretisation is Crank-Nicolson or BDF2");
     if (ns->contr.flowtype != NEWTONIAN && ns->contr.flowtype != VISCOELASTIC) return REASON(HF_ERR_UNSUPPORTED, "flow type is neither Newtonian nor viscoelastic");
     if (ns->contr.eoflow) return REASON(HF_ERR_UNSUPPORTED, "electro-osmotic flow");
     const int ve = ns->contr.flowtype == VISCOELASTIC;
@@ -318,7 +319,9 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
      * by the engine from the recorded UL/UR stencils of every direction: the
      * same sfd_get_stencil queries at fcenter -/+ fdelta[dim2], here with
      * weight 1 and there with weight -dt/(Re fdelta[dim2]^2) */
-    par->tempdiscrtype = ns->contr.tempdiscrtype == SEMI_IMPLICIT_EULER ? HF_SEMI_IMPLICIT_EULER : HF_EXPLICIT_EULER;
+    par->tempdiscrtype = ns->contr.tempdiscrtype == SEMI_IMPLICIT_EULER ? HF_SEMI_IMPLICIT_EULER
+                         : ns->contr.tempdiscrtype == EXPLICIT_RK2 ? HF_EXPLICIT_RK2
+                         : ns->contr.tempdiscrtype == EXPLICIT_RK3 ? HF_EXPLICIT_RK3 : HF_EXPLICIT_EULER;
     if (ve) {
         par->ve_model = ns->ed.ve.contr.model;
         par->ve_convecdiscrtype = ns->ed.ve.contr.convecdiscrtype;

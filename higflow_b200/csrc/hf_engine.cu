@@ -937,6 +937,22 @@ __global__ void __launch_bounds__(kBlock) k_bi_update(DevMat M, BiVec V)
     }
 }
 
+// Runge-Kutta combinations of the intermediate velocity on every facet
+// (hig-flow-step.c:697, :772): which 0: u* = 0.5 (u + u*); 2: u* = u/3 + 2 u*/3
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_rk_combine(DevProg P, DevFields F, int which)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.off[D]) return;
+    int d = 0;
+#pragma unroll
+    for (int k = 1; k < D; k++) d += (e >= P.off[k]);
+    const int f = e - pick<4>(P.off, d);
+    const double u = pick<3>(F.u, d)[f], ustar = pick<3>(F.us, d)[f];
+    if (which == 0) pick<3>(F.us, d)[f] = 0.5 * (u + ustar);
+    else pick<3>(F.us, d)[f] = u / 3.0 + 2.0 * ustar / 3.0;
+}
+
 // CFL number of every instance (higflow_compute_CFL, hig-flow-timestep.c:7-40):
 // per cell, sum over d of |(u_l + u_r) / 2| / (the cell's face area normal to d),
 // u_l and u_r the face velocities (the divergence's own queries, on u); the
@@ -2015,6 +2031,35 @@ void record(hf_case *C, int phase, int end)
     else cudaEventRecord(C->ev[2 * phase + end], C->stream);
 }
 
+// The velocity stage of one step: explicit Euler (k_vrows + k_velocity), and
+// for the explicit Runge-Kutta forms its combination with u.  The reference's
+// Runge-Kutta stages call higflow_explicit_euler_intermediate_velocity(ns, in,
+// out), whose computational cell reads ns->dpu whatever `in` is
+// (hig-flow-step.c:639; viscoelastic hig-flow-step-viscoelastic.c:957), so
+// every stage evaluates the same E(u) and the schemes reduce to RK2: u* =
+// 0.5 (u + E(u)); RK3: u* = u/3 + 2 E(u)/3 (the auxiliary velocity feeds no
+// later stage).  E(u) is evaluated once here: a repeat would give the same bits.
+// Returns the kernels launched.
+template <int D>
+int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
+{
+    const bool ve = C->par.flowtype == HF_VISCOELASTIC;
+    int n = 0;
+    if (C->P.nvrows) {
+        k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
+        n++;
+    }
+    if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    n++;
+    const int scheme = C->par.tempdiscrtype;
+    if (scheme == HF_EXPLICIT_RK2 || scheme == HF_EXPLICIT_RK3) {
+        k_rk_combine<D><<<blocks(C->nfacet_total), kBlock, 0, st>>>(C->P, F, scheme == HF_EXPLICIT_RK2 ? 0 : 2);
+        n++;
+    }
+    return n;
+}
+
 // The kernels of a step before the Poisson iterations: viscoelastic cell stage
 // (F's K/Knew swap after it), intermediate velocity, Poisson right-hand side.
 template <int D>
@@ -2031,12 +2076,7 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
         fixed += 2;
     }
     record(C, HF_PHASE_VELOCITY, 0);
-    if (C->P.nvrows) {
-        k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
-        fixed++;
-    }
-    if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
-    else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    fixed += enqueue_velocity<D>(C, F, st);
     if (C->sie) C->sie_rc = sie_solves(C, C->sie_launches);   // eager steps only (no graph for this form)
     record(C, HF_PHASE_VELOCITY, 1);
     record(C, HF_PHASE_POISSON_INIT, 0);
@@ -2261,13 +2301,7 @@ int bicg_step(hf_case *C)
     }
     {
         PhaseTimer t(C, HF_PHASE_VELOCITY, launches);
-        if (C->P.nvrows) {
-            k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, C->F);
-            launches++;
-        }
-        if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
-        else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, C->F);
-        launches++;
+        launches += enqueue_velocity<D>(C, C->F, st);
         if (C->sie) {
             int rc = sie_solves(C, launches);
             if (rc) return rc;
@@ -2425,6 +2459,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             pinv.push_back(pg->inst_pin_value[i]);
             if (pg->inst_par[i].dim != D || pg->inst_par[i].flowtype != pg->par.flowtype)
                 return cleanup(fail(HF_ERR_INVALID, "batch members differ in dim or flow type"));
+            if (pg->inst_par[i].tempdiscrtype != pg->par.tempdiscrtype)
+                return cleanup(fail(HF_ERR_UNSUPPORTED, "batch members differ in intermediate-velocity scheme"));
         }
         C->coff.assign(pg->cell_off, pg->cell_off + pg->ninst + 1);
         for (int d = 0; d < D; d++) C->foff[d].assign(pg->facet_off[d], pg->facet_off[d] + pg->ninst + 1);
@@ -2577,6 +2613,9 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     // fields
     DevFields &F = C->F;
     memset(&F, 0, sizeof F);
+    const bool rk = pg->par.tempdiscrtype == HF_EXPLICIT_RK2 || pg->par.tempdiscrtype == HF_EXPLICIT_RK3;
+    if (pg->par.tempdiscrtype != HF_EXPLICIT_EULER && !rk && pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_EULER)
+        return cleanup(fail(HF_ERR_UNSUPPORTED, "unknown intermediate-velocity scheme"));
     for (int d = 0; d < D; d++) {
         UP(&F.u[d], (const double *)nullptr, pg->nfacet[d]);
         UP(&F.us[d], (const double *)nullptr, pg->nfacet[d]);

@@ -19,7 +19,7 @@ import numpy as np
 
 # enumerations (include/higflow_b200.h)
 NEWTONIAN, VISCOELASTIC = 0, 3
-EXPLICIT_EULER, SEMI_IMPLICIT_EULER = 0, 3
+EXPLICIT_EULER, EXPLICIT_RK2, EXPLICIT_RK3, SEMI_IMPLICIT_EULER = 0, 1, 2, 3
 NON_INCREMENTAL, INCREMENTAL = 0, 1
 CENTRAL, FIRST_ORDER, SECOND_ORDER = 0, 1, 2
 MCU, CUBISTA, QUICK = 0, 1, 2

@@ -57,10 +57,13 @@ enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order 
 enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2 };        /* VE model       */
 enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
 enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
-/* intermediate velocity (hig-flow-kernel.h:169-176); the semi-implicit form
- * solves (I - dt/Re Lap_h) u* = u + dt (sources - grad p - conv [+ div S]) per
- * direction (hig-flow-step.c:788-883, hig-flow-step-viscoelastic.c:1108-1210) */
-enum { HF_EXPLICIT_EULER = 0, HF_SEMI_IMPLICIT_EULER = 3 };
+/* intermediate velocity (hig-flow-kernel.h:169-176): explicit Euler; the
+ * explicit Runge-Kutta forms chain Euler stages E (RK2: u* = (u + E(E(u)))/2;
+ * RK3: v = E(u), w = 3u/4 + E(v)/4, u* = u/3 + 2 E(w)/3; hig-flow-step.c:
+ * 666-784); the semi-implicit form solves (I - dt/Re Lap_h) u* = u + dt
+ * (sources - grad p - conv [+ div S]) per direction (hig-flow-step.c:788-883,
+ * hig-flow-step-viscoelastic.c:1108-1210) */
+enum { HF_EXPLICIT_EULER = 0, HF_EXPLICIT_RK2 = 1, HF_EXPLICIT_RK3 = 2, HF_SEMI_IMPLICIT_EULER = 3 };
 
 /* precision forms */
 enum {
@@ -187,7 +190,7 @@ typedef struct hf_params {
     int32_t kernel;               /* HF_KERNEL_*                             */
     double Re, dt;
     double De, beta, kernel_tol, alpha, epsilon, xi;
-    int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER (contr.tempdiscrtype) */
+    int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / _RK2 / _RK3 / HF_SEMI_IMPLICIT_EULER */
     int32_t pad_;
 } hf_params;
 

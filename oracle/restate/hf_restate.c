@@ -950,6 +950,32 @@ static void polymeric_stage(const hf_program *P, hfr_fields *F)
     }
 }
 
+/* explicit Runge-Kutta velocity (higflow_explicit_runge_kutta_{2,3}_
+ * intermediate_velocity, hig-flow-step.c:666-784), stage by stage: each
+ * explicit Euler stage writes its output field, but its computational cell
+ * reads ns->dpu (hig-flow-step.c:639), so every stage's input is u */
+static void rk_stage(const hf_program *P, hfr_fields *F)
+{
+    const int D = P->par.dim;
+    double *ua[3] = {0};
+    for (int d = 0; d < D; d++) ua[d] = malloc(sizeof(double) * (size_t)P->nfacet[d]);
+    hfr_fields F1 = *F;
+    for (int d = 0; d < D; d++) F1.us[d] = ua[d];
+    for (int d = 0; d < D; d++) velocity_stage(P, &F1, d);   /* dpuaux = E(u) */
+    for (int d = 0; d < D; d++) velocity_stage(P, F, d);     /* dpustar = E(u) (input dpuaux unread) */
+    if (P->par.tempdiscrtype == HF_EXPLICIT_RK2) {
+        for (int d = 0; d < D; d++)
+            for (int f = 0; f < P->nfacet[d]; f++) F->us[d][f] = 0.5 * (F->u[d][f] + F->us[d][f]);
+    } else {
+        for (int d = 0; d < D; d++)
+            for (int f = 0; f < P->nfacet[d]; f++) ua[d][f] = 0.75 * F->u[d][f] + 0.25 * F->us[d][f];
+        for (int d = 0; d < D; d++) velocity_stage(P, F, d);     /* dpustar = E(u) */
+        for (int d = 0; d < D; d++)
+            for (int f = 0; f < P->nfacet[d]; f++) F->us[d][f] = F->u[d][f] / 3.0 + 2.0 * F->us[d][f] / 3.0;
+    }
+    for (int d = 0; d < D; d++) free(ua[d]);
+}
+
 /* one or more full time steps; returns 0 or a negative HF_ERR_* code */
 int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *iters)
 {
@@ -966,7 +992,9 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
             for (int k = 0; k < D * D; k++) memcpy(F->K[k], knew[k], sizeof(double) * (size_t)P->ncell);
             polymeric_stage(P, F);
         }
-        for (int d = 0; d < D; d++) velocity_stage(P, F, d);
+        if (P->par.tempdiscrtype == HF_EXPLICIT_RK2 || P->par.tempdiscrtype == HF_EXPLICIT_RK3) rk_stage(P, F);
+        else
+            for (int d = 0; d < D; d++) velocity_stage(P, F, d);
         if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER)
             for (int d = 0; d < D && rc == 0; d++) rc = sie_solve(P, F, d, rtol);
         if (rc) break;

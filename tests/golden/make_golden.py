@@ -60,6 +60,12 @@ CASES = {
     # a low-Re Newtonian cavity, an Oldroyd-B log cavity and a two-level
     # Oldroyd-B case (the contraction configuration's form: non-symmetric
     # Poisson rows at the level interface)
+    # explicit Runge-Kutta velocity (every stage evaluates E(u): the reference's
+    # stages read ns->dpu, hig-flow-step.c:639)
+    "rk2_cav2d": (lambda: refpy.cavity(2, 16, Re=10.0, dt=1e-3, tempdiscrtype=hp.EXPLICIT_RK2), 4, (0.3, 0.1, 0.0)),
+    "rk3_giesekus_log": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC,
+                                              ve_model=hp.GIESEKUS, kernel=hp.KERNEL_LOG, alpha=0.3, beta=0.1,
+                                              De=0.5, tempdiscrtype=hp.EXPLICIT_RK3), 3, (0.3, 0.1, 0.2)),
     "sie2d_cubista": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
                       4, (0.3, 0.1, 0.0)),
     "sie2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
