@@ -277,8 +277,14 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
     int32_t kernel = HF_KERNEL_IDENTITY;
     if (ve) {
         if (ns->ed.ve.contr.discrtype != EXPLICIT) return REASON(HF_ERR_UNSUPPORTED, "implicit constitutive step");
+        /* FENE-P is left out: the reference's polymeric tensor reads xi without
+         * assigning it for this model (hig-flow-step-viscoelastic.c:285-292),
+         * so its stress has no defined value to reproduce */
+        if (ns->ed.ve.contr.model == FENE_P)
+            return REASON(HF_ERR_UNSUPPORTED, "FENE-P (the reference's stress for it reads an unassigned xi)");
         if (ns->ed.ve.contr.model != OLDROYD_B && ns->ed.ve.contr.model != GIESEKUS &&
-            ns->ed.ve.contr.model != LPTT) return REASON(HF_ERR_UNSUPPORTED, "viscoelastic model other than Oldroyd-B, Giesekus, LPTT");
+            ns->ed.ve.contr.model != LPTT && ns->ed.ve.contr.model != E_FENE)
+            return REASON(HF_ERR_UNSUPPORTED, "viscoelastic model other than Oldroyd-B, Giesekus, LPTT, e-FENE");
         if (detect_kernel(ns, &kernel)) return REASON(HF_ERR_UNSUPPORTED, "kernel transform callbacks are not identity, log or sqrt");
     }
 
@@ -332,6 +338,9 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
         par->alpha = ns->ed.ve.par.alpha;
         par->epsilon = ns->ed.ve.par.epsilon;
         par->xi = ns->ed.ve.par.xi;
+        par->L2_fene = ns->ed.ve.par.L2_fene;
+        par->lambda_fene = ns->ed.ve.par.lambda_fene;
+        par->E_fene = ns->ed.ve.par.E_fene;
     }
 
     const int ncell = psd_get_local_domain_size(ns->psdp);

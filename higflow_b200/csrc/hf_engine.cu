@@ -655,6 +655,15 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
     for (int i = 0; i < D; i++) jl[i] = hf::kernel_jacobian(pr.kernel, lam[i], tol);
     double Ba[D][D], BB[D][D], Ma[D][D], MM[D][D];
+    // e-FENE (hig_flow_calculate_m_e_fene, hig-flow-step-viscoelastic.c:1855-1876)
+    double fA = 0.0;
+    if (pr.ve_model == HF_E_FENE) {
+        double trA = 0.0;
+#pragma unroll
+        for (int i = 0; i < D; i++) trA += lam[i];
+        const double b = pr.L2_fene, lf = pr.lambda_fene, E = pr.E_fene;
+        fA = b / (b - trA) - E * sqrt(b) * exp(-sqrt(trA) / lf) * (1.0 / (trA * lf) + 1 / (trA * sqrt(trA)));
+    }
 #pragma unroll
     for (int i = 0; i < D; i++) {
 #pragma unroll
@@ -668,6 +677,8 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
             Ma[i][i] = (aux - pr.alpha * aux * aux) * jl[i];
         } else if (pr.ve_model == HF_LPTT) {
             Ma[i][i] = (1.0 - lam[i]) * (1.0 + (pr.epsilon * Re * De * trS) / (1.0 - pr.beta)) * jl[i];
+        } else if (pr.ve_model == HF_E_FENE) {
+            Ma[i][i] = (1.0 - fA * lam[i]) * jl[i];
         } else {
             Ma[i][i] = (1.0 - lam[i]) * jl[i];
         }
@@ -769,6 +780,9 @@ __global__ void __launch_bounds__(kBlock) k_ve_stress(DevProg P, DevFields F)
         Bk[i][i] = hf::kernel_inverse(pr.kernel, lam2[i]);
     }
     hf::mtprod<D>(Bk, R2, A);
+    // the model switch of hig-flow-step-viscoelastic.c:274-309: LPTT sets xi;
+    // e-FENE computes its fA there but falls through to the default, so its
+    // stress is formed with fA = a = 1, xi = 0 like Oldroyd-B and Giesekus
     const double fA = 1.0, aa = 1.0, beta = pr.beta;
     const double xi = pr.ve_model == HF_LPTT ? pr.xi : 0.0;
 #pragma unroll

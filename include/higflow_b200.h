@@ -54,7 +54,8 @@ enum { HF_NEWTONIAN = 0, HF_VISCOELASTIC = 3 };                 /* flow_type    
 enum { HF_NON_INCREMENTAL = 0, HF_INCREMENTAL = 1 };            /* projection     */
 enum { HF_CENTRAL = 0, HF_FIRST_ORDER = 1, HF_SECOND_ORDER = 2 };/* convecdiscr   */
 enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order   */
-enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2 };        /* VE model       */
+enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2,           /* VE model       */
+       HF_FENE_P = 4, HF_E_FENE = 5 };
 enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
 enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
 /* intermediate velocity (hig-flow-kernel.h:169-176): explicit Euler; the
@@ -192,6 +193,7 @@ typedef struct hf_params {
     double De, beta, kernel_tol, alpha, epsilon, xi;
     int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / _RK2 / _RK3 / HF_SEMI_IMPLICIT_EULER */
     int32_t pad_;
+    double L2_fene, lambda_fene, E_fene;   /* FENE-P / e-FENE (ve_parameters, hig-flow-kernel.h:443-445) */
 } hf_params;
 
 /* A flattened step program (host memory, read-only for the engine). */

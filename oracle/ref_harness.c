@@ -48,6 +48,7 @@ typedef struct hfref_params {
     double k_init[3][3];        /* initial kernel tensor (get_tensor) */
     int32_t tempdiscrtype;      /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER */
     int32_t pad_;
+    double L2_fene, lambda_fene, E_fene;
 } hfref_params;
 
 typedef struct hfref_case {
@@ -201,6 +202,9 @@ int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
         ns->ed.ve.par.alpha = p->alpha;
         ns->ed.ve.par.epsilon = p->epsilon;
         ns->ed.ve.par.xi = p->xi;
+        ns->ed.ve.par.L2_fene = p->L2_fene;
+        ns->ed.ve.par.lambda_fene = p->lambda_fene;
+        ns->ed.ve.par.E_fene = p->E_fene;
     }
 
     higflow_set_external_functions(ns, cb_get_pressure, cb_get_velocity, cb_get_source_term,

@@ -38,6 +38,7 @@ class RefParams(C.Structure):
         ("bc_p", C.c_double * MAXBC),
         ("k_init", (C.c_double * 3) * 3),
         ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
+        ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
     ]
 
 
@@ -313,6 +314,9 @@ class CaseSpec:
         p.epsilon = g("epsilon", 0.25)
         p.xi = g("xi", 0.0)
         p.tempdiscrtype = g("tempdiscrtype", hp.EXPLICIT_EULER)
+        p.L2_fene = g("L2_fene", 100.0)
+        p.lambda_fene = g("lambda_fene", 1.0)
+        p.E_fene = g("E_fene", 0.0)
         for b, face in enumerate(self.faces):
             for d, v in enumerate(face.get("uval", [0.0] * self.dim)):
                 p.bc_u[b][d] = v

@@ -854,6 +854,13 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
         mtprod(D, Ba, R, BB);
         /* model terms (:1710-1770) */
         double Ma[3][3], MM[3][3];
+        /* e-FENE (:1855-1876): trace of the eigenvalues */
+        double trA = 0.0, fA = 0.0;
+        for (int i = 0; i < D; i++) trA += lam[i];
+        if (pr->ve_model == HF_E_FENE) {
+            const double b = pr->L2_fene, lf = pr->lambda_fene, E = pr->E_fene;
+            fA = b / (b - trA) - E * sqrt(b) * exp(-sqrt(trA) / lf) * (1.0 / (trA * lf) + 1 / (trA * sqrt(trA)));
+        }
         for (int i = 0; i < D; i++) {
             for (int j = i + 1; j < D; j++) { Ma[i][j] = 0.0; Ma[j][i] = 0.0; }
             if (pr->ve_model == HF_GIESEKUS) {
@@ -861,6 +868,8 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
                 Ma[i][i] = (aux - pr->alpha * aux * aux) * jl[i];
             } else if (pr->ve_model == HF_LPTT) {
                 Ma[i][i] = (1.0 - lam[i]) * (1.0 + (pr->epsilon * Re * De * trS) / (1.0 - pr->beta)) * jl[i];
+            } else if (pr->ve_model == HF_E_FENE) {
+                Ma[i][i] = (1.0 - fA * lam[i]) * jl[i];
             } else {
                 Ma[i][i] = (1.0 - lam[i]) * jl[i];
             }
@@ -940,6 +949,8 @@ static void polymeric_stage(const hf_program *P, hfr_fields *F)
             B[i][i] = kinv(pr->kernel, lam[i]);
         }
         mtprod(D, B, R, A);
+        /* the model switch of :274-309: LPTT sets xi; e-FENE computes its fA
+         * there but falls through to the default (fA = a = 1, xi = 0) */
         double fA = 1.0, a = 1.0, xi = 0.0;
         if (pr->ve_model == HF_LPTT) xi = pr->xi;
         for (int i = 0; i < D; i++) {

@@ -178,3 +178,15 @@ def test_cfl_matches_reference(dim, ve):
     expect = min(min(0.1 / (want + 1e-12), 1.1) * dt0, 32 * dt0)
     assert abs(c.dt - expect) <= 1e-15 * expect, (c.dt, expect)
     c.close()
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not present")
+def test_fene_p_is_refused_with_its_reason():
+    """FENE-P stays off the GPU path: the reference's polymeric tensor reads xi
+    without assigning it for this model, so there is no defined stress to match."""
+    c = refpy.RefCase(refpy.cavity(2, 8, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.FENE_P,
+                                   kernel=hp.KERNEL_LOG, L2_fene=100.0))
+    with pytest.raises(Exception) as e:
+        c.flatten()
+    assert "FENE-P" in str(e.value)
+    c.close()
