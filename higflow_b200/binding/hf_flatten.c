@@ -276,7 +276,8 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
     const int ve = ns->contr.flowtype == VISCOELASTIC;
     int32_t kernel = HF_KERNEL_IDENTITY;
     if (ve) {
-        if (ns->ed.ve.contr.discrtype != EXPLICIT) return REASON(HF_ERR_UNSUPPORTED, "implicit constitutive step");
+        if (ns->ed.ve.contr.discrtype != EXPLICIT && ns->ed.ve.contr.discrtype != IMPLICIT)
+            return REASON(HF_ERR_UNSUPPORTED, "constitutive step neither explicit nor implicit Euler");
         /* FENE-P is left out: the reference's polymeric tensor reads xi without
          * assigning it for this model (hig-flow-step-viscoelastic.c:285-292),
          * so its stress has no defined value to reproduce */
@@ -341,6 +342,7 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
         par->L2_fene = ns->ed.ve.par.L2_fene;
         par->lambda_fene = ns->ed.ve.par.lambda_fene;
         par->E_fene = ns->ed.ve.par.E_fene;
+        par->ve_discrtype = ns->ed.ve.contr.discrtype == IMPLICIT ? HF_VE_IMPLICIT : HF_VE_EXPLICIT;
     }
 
     const int ncell = psd_get_local_domain_size(ns->psdp);

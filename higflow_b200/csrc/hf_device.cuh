@@ -193,6 +193,58 @@ __device__ __forceinline__ double kernel_jacobian(int kind, double l, double tol
     return 1.0;
 }
 
+// The implicit constitutive step's per-cell system: the matrix of
+// hig_flow_kernel_system_matrix (hig-flow-step-viscoelastic.c:1964-1989) for
+// Omega (row-major D x D) and dt, solved for the right-hand side x (n = D*D,
+// overwritten by the solution) by hig_flow_solve_system_constitutive_equation
+// (:1912-1953): Gauss elimination with partial pivoting, in its order.  Out of
+// line: only cells of instances with the implicit form call it.
+template <int D>
+__device__ __noinline__ void implicit_kernel_solve(const double *Om, double dt, double *x)
+{
+    constexpr int n = D * D;
+    double A[n][n + 1];
+    for (int i = 0; i < D; i++)
+        for (int j = i; j < D; j++)
+            for (int k = 0; k < D; k++)
+                for (int l = 0; l < D; l++) {
+                    const double I = k == l ? 1.0 : 0.0;
+                    if (i == j) {
+                        A[i * D + k][j * D + l] = I - dt * Om[k * D + l] - dt * Om[i * D + i] * I;
+                    } else {
+                        A[i * D + k][j * D + l] = dt * Om[j * D + i] * I;
+                        A[j * D + l][i * D + k] = -dt * Om[j * D + i] * I;
+                    }
+                }
+    for (int j = 0; j < n; j++) A[j][n] = x[j];
+    for (int k = 0; k < n - 1; k++) {
+        double mx = fabs(A[k][k]);
+        int l = k;
+        for (int i = k + 1; i < n; i++)
+            if (fabs(A[i][k]) > mx) {
+                mx = fabs(A[i][k]);
+                l = i;
+            }
+        if (l != k)
+            for (int j = k; j <= n; j++) {
+                const double aux = A[k][j];
+                A[k][j] = A[l][j];
+                A[l][j] = aux;
+            }
+        for (int i = k + 1; i < n; i++) {
+            const double s = A[i][k] / A[k][k];
+            A[i][k] = 0;
+            for (int j = k + 1; j <= n; j++) A[i][j] -= s * A[k][j];
+        }
+    }
+    x[n - 1] = A[n - 1][n] / A[n - 1][n - 1];
+    for (int i = n - 2; i >= 0; i--) {
+        double s = 0;
+        for (int j = i + 1; j < n; j++) s += A[i][j] * x[j];
+        x[i] = (A[i][n] - s) / A[i][i];
+    }
+}
+
 // hig_flow_convective_cell_term_cubista (hig-flow-step.c:1185-1358).  Out of
 // line: the VE cell stage calls it D(D+1)/2 x D times, and six inlined copies
 // of its branches made that kernel instruction-fetch bound (1.74 -> 1.38 ms on

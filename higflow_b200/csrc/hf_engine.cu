@@ -549,7 +549,10 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 // 8: 1.22, 16 at 32 registers: 1.19 with far more spill traffic)
 constexpr int kVeBlock = 128;
 
-template <int D>
+// IMPL: the implicit constitutive step (hf_params.ve_discrtype, the same for
+// every instance of a case), a separate instantiation so that the explicit
+// kernel carries none of its code
+template <int D, bool IMPL>
 __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
@@ -685,11 +688,19 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
     }
     hf::mtprod<D>(Ba, Rm, BB);
     hf::mtprod<D>(Ma, Rm, MM);
+    // explicit: RHS = Omega K - K Omega + 2B + M/De (hig_flow_kernel_rhs);
+    // implicit: RHS = 2B + M/De (hig_flow_implicit_kernel_rhs, :1956-1963), the
+    // Omega terms being in the per-cell system
+    constexpr bool implicit = IMPL;
     double RHS[D][D];
 #pragma unroll
     for (int i = 0; i < D; i++)
 #pragma unroll
         for (int j = 0; j < D; j++) {
+            if (implicit) {
+                RHS[i][j] = 2.0 * BB[i][j] + MM[i][j] / De;
+                continue;
+            }
             double ok = 0.0, ko = 0.0;
 #pragma unroll
             for (int k = 0; k < D; k++) {
@@ -708,6 +719,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
     for (int k = 0; k < 4 * D; k++) ck[k] = CS(HF_C_BLK0 + HF_C_NB * (k >> 2) + HF_C_KL + (k & 3));
     double Knew[D][D];
+    double bsys[D * D];   // implicit form: the per-cell system's right-hand side
 #pragma unroll
     for (int i = 0; i < D; i++) {
 #pragma unroll
@@ -739,11 +751,44 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
                     rhs -= uc * dk;
                 }
             }
+            if (implicit) {
+                // hig-flow-step-viscoelastic.c:861-864 for (i, j) and (j, i);
+                // their convective parts are equal (K is stored symmetric)
+                double r1 = rhs;
+                r1 += RHS[i][j];
+                r1 *= pr.dt;
+                r1 += K[i][j];
+                bsys[i * D + j] = r1;
+                if (j != i) {
+                    double r2 = rhs;
+                    r2 += RHS[j][i];
+                    r2 *= pr.dt;
+                    r2 += K[j][i];
+                    bsys[j * D + i] = r2;
+                }
+                continue;
+            }
             rhs += RHS[i][j];
             const double kernel = K[i][j] + pr.dt * rhs;
             Knew[i][j] = kernel;
             Knew[j][i] = kernel;
         }
+    }
+    if (implicit) {
+        double om[D * D];
+#pragma unroll
+        for (int i = 0; i < D; i++)
+#pragma unroll
+            for (int j = 0; j < D; j++) om[i * D + j] = Om[i][j];
+        hf::implicit_kernel_solve<D>(om, pr.dt, bsys);
+        // the upper triangle of the solution, mirrored (:868-877)
+#pragma unroll
+        for (int i = 0; i < D; i++)
+#pragma unroll
+            for (int j = i; j < D; j++) {
+                Knew[i][j] = bsys[i * D + j];
+                Knew[j][i] = bsys[i * D + j];
+            }
     }
 #undef CS
 #pragma unroll
@@ -2083,7 +2128,10 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     if (ve) {
         record(C, HF_PHASE_VE_CELL, 0);
-        k_ve_cell<D><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
+        if (C->par.ve_discrtype == HF_VE_IMPLICIT)
+            k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
+        else
+            k_ve_cell<D, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
@@ -2307,7 +2355,10 @@ int bicg_step(hf_case *C)
     int64_t launches = 0;
     if (ve) {
         PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
-        k_ve_cell<D><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
+        if (C->par.ve_discrtype == HF_VE_IMPLICIT)
+            k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
+        else
+            k_ve_cell<D, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
         launches += 2;
         for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
@@ -2475,6 +2526,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 return cleanup(fail(HF_ERR_INVALID, "batch members differ in dim or flow type"));
             if (pg->inst_par[i].tempdiscrtype != pg->par.tempdiscrtype)
                 return cleanup(fail(HF_ERR_UNSUPPORTED, "batch members differ in intermediate-velocity scheme"));
+            if (pg->inst_par[i].ve_discrtype != pg->par.ve_discrtype)
+                return cleanup(fail(HF_ERR_UNSUPPORTED, "batch members differ in constitutive scheme"));
         }
         C->coff.assign(pg->cell_off, pg->cell_off + pg->ninst + 1);
         for (int d = 0; d < D; d++) C->foff[d].assign(pg->facet_off[d], pg->facet_off[d] + pg->ninst + 1);

@@ -20,6 +20,7 @@ import numpy as np
 # enumerations (include/higflow_b200.h)
 NEWTONIAN, VISCOELASTIC = 0, 3
 FENE_P, E_FENE = 4, 5
+VE_EXPLICIT, VE_IMPLICIT = 0, 1
 EXPLICIT_EULER, EXPLICIT_RK2, EXPLICIT_RK3, SEMI_IMPLICIT_EULER = 0, 1, 2, 3
 NON_INCREMENTAL, INCREMENTAL = 0, 1
 CENTRAL, FIRST_ORDER, SECOND_ORDER = 0, 1, 2
@@ -84,6 +85,7 @@ class HFParams(C.Structure):
         ("alpha", C.c_double), ("epsilon", C.c_double), ("xi", C.c_double),
         ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
         ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
+        ("ve_discrtype", C.c_int32), ("pad2_", C.c_int32),
     ]
 
 
@@ -142,9 +144,10 @@ class HFStats(C.Structure):
 
 _PARAM_NAMES = [n for n, _ in HFParams._fields_]
 # parameters that programs written before they existed do not carry
-_PARAM_DEFAULTS = {"tempdiscrtype": 0, "pad_": 0, "L2_fene": 0.0, "lambda_fene": 0.0, "E_fene": 0.0}
+_PARAM_DEFAULTS = {"tempdiscrtype": 0, "pad_": 0, "L2_fene": 0.0, "lambda_fene": 0.0, "E_fene": 0.0,
+                   "ve_discrtype": 0, "pad2_": 0}
 _INT_PARAMS = ("dim", "flowtype", "projtype", "convecdiscrtype", "secondconvecdiscrtype", "ve_model",
-               "ve_convecdiscrtype", "kernel", "tempdiscrtype", "pad_")
+               "ve_convecdiscrtype", "kernel", "tempdiscrtype", "pad_", "ve_discrtype", "pad2_")
 
 
 def _np_from(ptr, n, dtype):

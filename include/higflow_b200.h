@@ -57,6 +57,10 @@ enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order 
 enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2,           /* VE model       */
        HF_FENE_P = 4, HF_E_FENE = 5 };
 enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
+/* constitutive step (hig-flow-kernel.h:305-308): explicit Euler, or the
+ * implicit form that solves (I - dt (Omega x I - I x Omega)) K = K + dt (-conv
+ * + 2B + M/De) per cell (hig-flow-step-viscoelastic.c:720-926) */
+enum { HF_VE_EXPLICIT = 0, HF_VE_IMPLICIT = 1 };
 enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
 /* intermediate velocity (hig-flow-kernel.h:169-176): explicit Euler; the
  * explicit Runge-Kutta forms chain Euler stages E (RK2: u* = (u + E(E(u)))/2;
@@ -193,7 +197,9 @@ typedef struct hf_params {
     double De, beta, kernel_tol, alpha, epsilon, xi;
     int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / _RK2 / _RK3 / HF_SEMI_IMPLICIT_EULER */
     int32_t pad_;
-    double L2_fene, lambda_fene, E_fene;   /* FENE-P / e-FENE (ve_parameters, hig-flow-kernel.h:443-445) */
+    double L2_fene, lambda_fene, E_fene;   /* e-FENE (ve_parameters, hig-flow-kernel.h:443-445) */
+    int32_t ve_discrtype;         /* HF_VE_EXPLICIT / HF_VE_IMPLICIT (constitutive step) */
+    int32_t pad2_;
 } hf_params;
 
 /* A flattened step program (host memory, read-only for the engine). */

@@ -49,6 +49,8 @@ typedef struct hfref_params {
     int32_t tempdiscrtype;      /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER */
     int32_t pad_;
     double L2_fene, lambda_fene, E_fene;
+    int32_t ve_discrtype;       /* HF_VE_EXPLICIT / HF_VE_IMPLICIT */
+    int32_t pad2_;
 } hfref_params;
 
 typedef struct hfref_case {
@@ -194,7 +196,7 @@ int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
     ns->contr.secondconvecdiscrtype = p->secondconvecdiscrtype;
     if (p->flowtype == VISCOELASTIC) {
         ns->ed.ve.contr.model = p->ve_model;
-        ns->ed.ve.contr.discrtype = EXPLICIT;
+        ns->ed.ve.contr.discrtype = p->ve_discrtype == HF_VE_IMPLICIT ? IMPLICIT : EXPLICIT;
         ns->ed.ve.contr.convecdiscrtype = p->ve_convecdiscrtype;
         ns->ed.ve.par.De = p->De;
         ns->ed.ve.par.beta = p->beta;

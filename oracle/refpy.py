@@ -39,6 +39,7 @@ class RefParams(C.Structure):
         ("k_init", (C.c_double * 3) * 3),
         ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
         ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
+        ("ve_discrtype", C.c_int32), ("pad2_", C.c_int32),
     ]
 
 
@@ -317,6 +318,7 @@ class CaseSpec:
         p.L2_fene = g("L2_fene", 100.0)
         p.lambda_fene = g("lambda_fene", 1.0)
         p.E_fene = g("E_fene", 0.0)
+        p.ve_discrtype = g("ve_discrtype", hp.VE_EXPLICIT)
         for b, face in enumerate(self.faces):
             for d, v in enumerate(face.get("uval", [0.0] * self.dim)):
                 p.bc_u[b][d] = v

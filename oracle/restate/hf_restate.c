@@ -802,6 +802,86 @@ static void du_stage(const hf_program *P, hfr_fields *F)
 
 /* explicit constitutive step (hig-flow-step-viscoelastic.c:352-544); the new
  * kernel goes to knew[] (the reference stores it in dpS, then copies) */
+/* implicit Euler constitutive step of one cell (higflow_implicit_euler_
+ * constitutive_equation, hig-flow-step-viscoelastic.c:841-877): right-hand
+ * side for every (i, j), the Kronecker system of hig_flow_kernel_system_matrix
+ * (:1964-1989), Gauss elimination with partial pivoting
+ * (hig_flow_solve_system_constitutive_equation, :1912-1953) */
+static void implicit_cell(const hf_program *P, hfr_fields *F, const hf_params *pr, int cc, uint32_t fl,
+                          const double *cd, const double *vl, const double *vr, const double *uc,
+                          double K[3][3], double RHS[3][3], double Om[3][3], double **knew)
+{
+    const int D = P->par.dim, n = D * D, nc = P->ncell;
+    const double dt = pr->dt;
+    double b[9], w[9][10];
+    for (int i = 0; i < D; i++)
+        for (int j = 0; j < D; j++) {
+            const double *Kf = F->K[i * D + j];
+            double rhs = 0.0;
+            for (int dim = 0; dim < D; dim++) {
+                const int B = HF_C_BLK0 + HF_C_NB * dim;
+                int il = (fl >> (4 * dim + 0)) & 1, ir = (fl >> (4 * dim + 1)) & 1;
+                int ill = (fl >> (4 * dim + 2)) & 1, irr = (fl >> (4 * dim + 3)) & 1;
+                double kl = q(P, P->cell_slots[(size_t)(B + HF_C_KL) * nc + cc], Kf);
+                double kr = q(P, P->cell_slots[(size_t)(B + HF_C_KR) * nc + cc], Kf);
+                if (pr->ve_convecdiscrtype == HF_CELL_CUBISTA) {
+                    double kll = q(P, P->cell_slots[(size_t)(B + HF_C_KLL) * nc + cc], Kf);
+                    double krr = q(P, P->cell_slots[(size_t)(B + HF_C_KRR) * nc + cc], Kf);
+                    rhs -= cubista_cell(kl, kr, kll, krr, il, ir, ill, irr, vl[dim], vr[dim], K[i][j], cd[dim]);
+                } else {
+                    double dk;
+                    if ((il == 1) && (ir == 1)) dk = (kr - kl) / (2.0 * 1.0 * cd[dim]);
+                    else if (ir == 1) dk = (kr - K[i][j]) / (1.0 * cd[dim]);
+                    else dk = (K[i][j] - kl) / (1.0 * cd[dim]);
+                    rhs -= uc[dim] * dk;
+                }
+            }
+            rhs += RHS[i][j];
+            rhs *= dt;
+            rhs += K[i][j];
+            b[i * D + j] = rhs;
+        }
+    double I[3][3];
+    for (int i = 0; i < D; i++)
+        for (int j = 0; j < D; j++) I[i][j] = i == j ? 1.0 : 0.0;
+    for (int i = 0; i < D; i++)
+        for (int j = i; j < D; j++)
+            for (int k = 0; k < D; k++)
+                for (int l = 0; l < D; l++) {
+                    if (i == j) {
+                        w[i * D + k][j * D + l] = I[k][l] - dt * Om[k][l] - dt * Om[i][i] * I[k][l];
+                    } else {
+                        w[i * D + k][j * D + l] = dt * Om[j][i] * I[k][l];
+                        w[j * D + l][i * D + k] = -dt * Om[j][i] * I[k][l];
+                    }
+                }
+    for (int j = 0; j < n; j++) w[j][n] = b[j];
+    for (int k = 0; k < n - 1; k++) {
+        double mx = fabs(w[k][k]);
+        int l = k;
+        for (int i = k + 1; i < n; i++)
+            if (fabs(w[i][k]) > mx) { mx = fabs(w[i][k]); l = i; }
+        if (l != k)
+            for (int j = k; j <= n; j++) { const double aux = w[k][j]; w[k][j] = w[l][j]; w[l][j] = aux; }
+        for (int i = k + 1; i < n; i++) {
+            const double s = w[i][k] / w[k][k];
+            w[i][k] = 0;
+            for (int j = k + 1; j <= n; j++) w[i][j] -= s * w[k][j];
+        }
+    }
+    b[n - 1] = w[n - 1][n] / w[n - 1][n - 1];
+    for (int i = n - 2; i >= 0; i--) {
+        double s = 0;
+        for (int j = i + 1; j < n; j++) s += w[i][j] * b[j];
+        b[i] = (w[i][n] - s) / w[i][i];
+    }
+    for (int i = 0; i < D; i++)
+        for (int j = i; j < D; j++) {
+            knew[i * D + j][cc] = b[i * D + j];
+            if (i != j) knew[j * D + i][cc] = b[i * D + j];
+        }
+}
+
 static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew)
 {
     const int D = P->par.dim, n = P->ncell;
@@ -886,8 +966,11 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
                     KO[i][j] += K[i][k] * Om[k][j];
                 }
             }
+        const int implicit = pr->ve_discrtype == HF_VE_IMPLICIT;
         for (int i = 0; i < D; i++)
-            for (int j = 0; j < D; j++) RHS[i][j] = OK[i][j] - KO[i][j] + 2.0 * BB[i][j] + MM[i][j] / De;
+            for (int j = 0; j < D; j++)
+                RHS[i][j] = implicit ? 2.0 * BB[i][j] + MM[i][j] / De   /* hig_flow_implicit_kernel_rhs (:1956) */
+                                     : OK[i][j] - KO[i][j] + 2.0 * BB[i][j] + MM[i][j] / De;
         /* hig_flow_velocity_at_center_cell (:1879) */
         double uc[3], vl[3], vr[3];
         for (int dim = 0; dim < D; dim++) {
@@ -895,6 +978,10 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
             vl[dim] = q(P, CS(B + HF_C_UVL), F->u[dim]);
             vr[dim] = q(P, CS(B + HF_C_UVR), F->u[dim]);
             uc[dim] = 0.5 * (vl[dim] + vr[dim]);
+        }
+        if (implicit) {
+            implicit_cell(P, F, pr, cc, fl, cd, vl, vr, uc, K, RHS, Om, knew);
+            continue;
         }
         for (int i = 0; i < D; i++) {
             for (int j = i; j < D; j++) {

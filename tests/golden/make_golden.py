@@ -71,6 +71,14 @@ CASES = {
     "efene2d_log": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.E_FENE,
                                          kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, L2_fene=100.0,
                                          lambda_fene=1.0, E_fene=0.1), 3, (0.3, 0.1, 0.2)),
+    # implicit Euler constitutive step (per-cell Kronecker system in Omega)
+    "ve2d_oldroyd_implicit": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                                   ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                                   De=0.5, ve_discrtype=hp.VE_IMPLICIT), 3, (0.3, 0.1, 0.2)),
+    "ve2d_giesekus_implicit_central": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                                            ve_model=hp.GIESEKUS, kernel=hp.KERNEL_LOG, alpha=0.3,
+                                                            beta=0.1, De=0.5, ve_discrtype=hp.VE_IMPLICIT,
+                                                            ve_convecdiscrtype=hp.CELL_CENTRAL), 3, (0.3, 0.1, 0.2)),
     "sie2d_cubista": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
                       4, (0.3, 0.1, 0.0)),
     "sie2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
