@@ -269,8 +269,9 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
     g_err[0] = 0;
     if (ns->contr.spatialdiscrtype != ORDER2) return REASON(HF_ERR_UNSUPPORTED, "spatial discretisation is not second order");
     if (ns->contr.tempdiscrtype != EXPLICIT_EULER && ns->contr.tempdiscrtype != EXPLICIT_RK2 &&
-        ns->contr.tempdiscrtype != EXPLICIT_RK3 && ns->contr.tempdiscrtype != SEMI_IMPLICIT_EULER)
-        return REASON(HF_ERR_UNSUPPORTED, "time discretisation is Crank-Nicolson or BDF2");
+        ns->contr.tempdiscrtype != EXPLICIT_RK3 && ns->contr.tempdiscrtype != SEMI_IMPLICIT_EULER &&
+        ns->contr.tempdiscrtype != SEMI_IMPLICIT_CN)
+        return REASON(HF_ERR_UNSUPPORTED, "time discretisation is BDF2");
     if (ns->contr.flowtype != NEWTONIAN && ns->contr.flowtype != VISCOELASTIC) return REASON(HF_ERR_UNSUPPORTED, "flow type is neither Newtonian nor viscoelastic");
     if (ns->contr.eoflow) return REASON(HF_ERR_UNSUPPORTED, "electro-osmotic flow");
     const int ve = ns->contr.flowtype == VISCOELASTIC;
@@ -327,6 +328,7 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
      * same sfd_get_stencil queries at fcenter -/+ fdelta[dim2], here with
      * weight 1 and there with weight -dt/(Re fdelta[dim2]^2) */
     par->tempdiscrtype = ns->contr.tempdiscrtype == SEMI_IMPLICIT_EULER ? HF_SEMI_IMPLICIT_EULER
+                         : ns->contr.tempdiscrtype == SEMI_IMPLICIT_CN ? HF_SEMI_IMPLICIT_CN
                          : ns->contr.tempdiscrtype == EXPLICIT_RK2 ? HF_EXPLICIT_RK2
                          : ns->contr.tempdiscrtype == EXPLICIT_RK3 ? HF_EXPLICIT_RK3 : HF_EXPLICIT_EULER;
     if (ve) {

@@ -513,8 +513,11 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
     if (P.sie) {
         // semi-implicit Euler (hig-flow-step.c:812-829; viscoelastic
         // hig-flow-step-viscoelastic.c:1136-1147): diffusion moves to the
-        // system matrix; its boundary part is added to the right-hand side
+        // system matrix; its boundary part is added to the right-hand side.
+        // Crank-Nicolson (hig-flow-step.c:908-917, viscoelastic :1243-1257)
+        // keeps half of the diffusion here.
         double rhs = 0.0;
+        if (par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) rhs += 0.5 * diff;
         rhs += Fs;
         rhs -= pterm;
         if (VE) rhs += tens;
@@ -2681,7 +2684,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     DevFields &F = C->F;
     memset(&F, 0, sizeof F);
     const bool rk = pg->par.tempdiscrtype == HF_EXPLICIT_RK2 || pg->par.tempdiscrtype == HF_EXPLICIT_RK3;
-    if (pg->par.tempdiscrtype != HF_EXPLICIT_EULER && !rk && pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_EULER)
+    if (pg->par.tempdiscrtype != HF_EXPLICIT_EULER && !rk && pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_EULER &&
+        pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_CN)
         return cleanup(fail(HF_ERR_UNSUPPORTED, "unknown intermediate-velocity scheme"));
     for (int d = 0; d < D; d++) {
         UP(&F.u[d], (const double *)nullptr, pg->nfacet[d]);
@@ -2708,8 +2712,9 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     // weight 1); entries on one facet are added in stencil order, and each
     // stencil's boundary term (w times the row's rhs) goes to the right-hand
     // side, as sfd_get_stencil does with stn_add_to_rhs.
-    if (pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER) {
+    if (pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) {
         if (ni > 1) return cleanup(fail(HF_ERR_UNSUPPORTED, "semi-implicit Euler in a batch"));
+        const bool cn = pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN;
         C->sie = true;
         P.sie = 1;
         const double dt = pg->par.dt, Re = pg->par.Re;
@@ -2730,7 +2735,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 const double *fd = pg->delta + (size_t)pg->vel_delta[d][f] * D;
                 double alpha = 0.0, b = 0.0;
                 for (int d2 = 0; d2 < D; d2++) {
-                    const double w = -dt / (Re * fd[d2] * fd[d2]);
+                    const double w = cn ? -0.5 * dt / (Re * fd[d2] * fd[d2]) : -dt / (Re * fd[d2] * fd[d2]);
                     alpha -= 2.0 * w;
                     for (int side : {HF_V_UR, HF_V_UL}) {
                         const int32_t code = pg->vel_slots[d][(size_t)(HF_V_BLK0 + HF_V_NB * d2 + side) * nf + f];

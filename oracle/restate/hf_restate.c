@@ -238,12 +238,14 @@ static void velocity_stage(const hf_program *P, hfr_fields *F, int d)
             rhs -= conv;
             rhs += diff;
         }
-        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER) {
+        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) {
             /* higflow_semi_implicit_euler_intermediate_velocity
              * (hig-flow-step.c:812-829; viscoelastic
              * hig-flow-step-viscoelastic.c:1136-1147): the right-hand side
-             * without diffusion; the system is solved by sie_solve */
+             * without diffusion; Crank-Nicolson (hig-flow-step.c:908-917)
+             * keeps half of it; the system is solved by sie_solve */
             double r = 0.0;
+            if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) r += 0.5 * diff;
             r += Fs;
             r -= pterm;
             if (ve) {
@@ -380,7 +382,8 @@ static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
         double alpha = 0.0, b = F->us[d][f];
         int len = 0;
         for (int d2 = 0; d2 < D; d2++) {
-            const double w = -dt / (Re * fd[d2] * fd[d2]);
+            const double w = P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN ? -0.5 * dt / (Re * fd[d2] * fd[d2])
+                                                                          : -dt / (Re * fd[d2] * fd[d2]);
             alpha -= 2.0 * w;
             const int sides[2] = {HF_V_UR, HF_V_UL};
             for (int k = 0; k < 2; k++) {
@@ -1093,7 +1096,7 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
         if (P->par.tempdiscrtype == HF_EXPLICIT_RK2 || P->par.tempdiscrtype == HF_EXPLICIT_RK3) rk_stage(P, F);
         else
             for (int d = 0; d < D; d++) velocity_stage(P, F, d);
-        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER)
+        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN)
             for (int d = 0; d < D && rc == 0; d++) rc = sie_solve(P, F, d, rtol);
         if (rc) break;
         rc = pressure_stage(P, F, rtol, iters);
@@ -1108,7 +1111,7 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
 void hfr_velocity(const hf_program *P, hfr_fields *F)
 {
     for (int d = 0; d < P->par.dim; d++) velocity_stage(P, F, d);
-    if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER)
+    if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN)
         for (int d = 0; d < P->par.dim; d++) sie_solve(P, F, d, 1e-14);
 }
 

@@ -84,6 +84,11 @@ CASES = {
     "sie2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
                                                ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                                tempdiscrtype=hp.SEMI_IMPLICIT_EULER), 3, (0.3, 0.1, 0.2)),
+    "cn2d_cubista": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_CN),
+                     4, (0.3, 0.1, 0.0)),
+    "cn2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                              ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                              tempdiscrtype=hp.SEMI_IMPLICIT_CN), 3, (0.3, 0.1, 0.2)),
     "amr2d_sie_oldroyd": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
                                                ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                                tempdiscrtype=hp.SEMI_IMPLICIT_EULER,
