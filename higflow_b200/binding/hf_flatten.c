@@ -270,8 +270,8 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
     if (ns->contr.spatialdiscrtype != ORDER2) return REASON(HF_ERR_UNSUPPORTED, "spatial discretisation is not second order");
     if (ns->contr.tempdiscrtype != EXPLICIT_EULER && ns->contr.tempdiscrtype != EXPLICIT_RK2 &&
         ns->contr.tempdiscrtype != EXPLICIT_RK3 && ns->contr.tempdiscrtype != SEMI_IMPLICIT_EULER &&
-        ns->contr.tempdiscrtype != SEMI_IMPLICIT_CN)
-        return REASON(HF_ERR_UNSUPPORTED, "time discretisation is BDF2");
+        ns->contr.tempdiscrtype != SEMI_IMPLICIT_CN && ns->contr.tempdiscrtype != SEMI_IMPLICIT_BDF2)
+        return REASON(HF_ERR_UNSUPPORTED, "unknown time discretisation");
     if (ns->contr.flowtype != NEWTONIAN && ns->contr.flowtype != VISCOELASTIC) return REASON(HF_ERR_UNSUPPORTED, "flow type is neither Newtonian nor viscoelastic");
     if (ns->contr.eoflow) return REASON(HF_ERR_UNSUPPORTED, "electro-osmotic flow");
     const int ve = ns->contr.flowtype == VISCOELASTIC;
@@ -329,6 +329,7 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
      * weight 1 and there with weight -dt/(Re fdelta[dim2]^2) */
     par->tempdiscrtype = ns->contr.tempdiscrtype == SEMI_IMPLICIT_EULER ? HF_SEMI_IMPLICIT_EULER
                          : ns->contr.tempdiscrtype == SEMI_IMPLICIT_CN ? HF_SEMI_IMPLICIT_CN
+                         : ns->contr.tempdiscrtype == SEMI_IMPLICIT_BDF2 ? HF_SEMI_IMPLICIT_BDF2
                          : ns->contr.tempdiscrtype == EXPLICIT_RK2 ? HF_EXPLICIT_RK2
                          : ns->contr.tempdiscrtype == EXPLICIT_RK3 ? HF_EXPLICIT_RK3 : HF_EXPLICIT_EULER;
     if (ve) {

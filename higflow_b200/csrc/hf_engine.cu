@@ -98,6 +98,10 @@ struct DevProg {
     int sie;
     double *sie_b[3];
     const double *sie_bc[3];
+    // BDF2's second solve: its boundary part, and the source - grad p [+ div
+    // S] - conv bracket of the velocity kernel, kept for its right-hand side
+    const double *sie_bc2[3];
+    double *sie_e[3];
     const int32_t *dslots;
     const uint16_t *cdelta;
     const int32_t *cslots;
@@ -516,6 +520,22 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
         // system matrix; its boundary part is added to the right-hand side.
         // Crank-Nicolson (hig-flow-step.c:908-917, viscoelastic :1243-1257)
         // keeps half of the diffusion here.
+        if (par.tempdiscrtype == HF_SEMI_IMPLICIT_BDF2) {
+            // hig-flow-step.c:1020-1033 (viscoelastic :1349-1363): the bracket
+            // is kept for the second solve's right-hand side (k_bdf2_rhs)
+            double e = 0.0;
+            e += Fs;
+            e -= pterm;
+            if (VE) e += tens;
+            e -= conv;
+            pick<3>(P.sie_e, d)[f] = e;
+            double rhs = e;
+            rhs *= 0.5 * par.dt;
+            rhs += 0.25 * par.dt * diff;
+            rhs += ufacet;
+            pick<3>(P.sie_b, d)[f] = rhs + __ldg(pick<3>(P.sie_bc, d) + f);
+            return;
+        }
         double rhs = 0.0;
         if (par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) rhs += 0.5 * diff;
         rhs += Fs;
@@ -1015,6 +1035,22 @@ __global__ void __launch_bounds__(kBlock) k_rk_combine(DevProg P, DevFields F, i
     else pick<3>(F.us, d)[f] = u / 3.0 + 2.0 * ustar / 3.0;
 }
 
+// BDF2's second right-hand side (hig-flow-step.c:1119-1120, viscoelastic
+// hig-flow-step-viscoelastic.c:1452-1453): bracket * (dt/3)
+// + (4 uaux - u)/3, plus the second system's boundary part; facets of one
+// direction
+__global__ void __launch_bounds__(kBlock) k_bdf2_rhs(int n, double dt, const double *__restrict__ e,
+                                                   const double *__restrict__ ua, const double *__restrict__ u,
+                                                   const double *__restrict__ bc2, double *__restrict__ b)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+    double rhs = e[f];
+    rhs *= 1.0 / 3.0 * dt;
+    rhs += (4.0 * ua[f] - u[f]) / 3.0;
+    b[f] = rhs + bc2[f];
+}
+
 // CFL number of every instance (higflow_compute_CFL, hig-flow-timestep.c:7-40):
 // per cell, sum over d of |(u_l + u_r) / 2| / (the cell's face area normal to d),
 // u_l and u_r the face velocities (the divergence's own queries, on u); the
@@ -1171,7 +1207,10 @@ struct hf_case {
     // semi-implicit Euler: per direction (I - dt/Re Lap_h) as CSR, solved by
     // BiCGStab into u* (scratch Vu shared by the directions)
     bool sie = false;
+    bool bdf2 = false;
     DevMat Mu[3] = {};
+    DevMat Mu2[3] = {};             // BDF2: the second solve's systems
+    double *ua[3] = {};             // BDF2: the first solve's velocity (dpuaux)
     BiVec Vu{};
     int64_t vel_iters = 0;          // their BiCGStab iterations, all steps
     int64_t sie_launches = 0;       // their kernels, all steps
@@ -2031,55 +2070,75 @@ void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, 
     }
 }
 
-// The semi-implicit velocity systems of one step (after the velocity kernel
-// wrote their right-hand sides): per direction BiCGStab with Jacobi scaling,
-// from u as the initial guess, into u*, to the Poisson solve's tolerances (the
-// reference hands both systems to the same solver engine).  Host-driven: the
-// host reads the scalars between chunks of iterations.
-int sie_solves(hf_case *C, int64_t &launches)
+// One semi-implicit velocity system: BiCGStab with Jacobi scaling on Mu from
+// x0 into x, right-hand side b
+int sie_solve_dir(hf_case *C, const DevMat &Mu, double *x, const double *x0, double *b, int d, int64_t &launches)
 {
     cudaStream_t st = C->stream;
     const double rtol = C->opt.poisson_rtol, atol = C->opt.poisson_atol;
-    for (int d = 0; d < C->D; d++) {
-        const DevMat &Mu = C->Mu[d];
-        const int n = Mu.n;
-        BiVec V = C->Vu;
-        V.x = C->F.us[d];
-        V.b = C->P.sie_b[d];
-        HF_CK(cudaMemcpyAsync(V.x, C->F.u[d], sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
-        Scal h{};
-        h.maxit = C->opt.poisson_maxit;
-        *C->h_scal = h;
-        HF_CK(cudaMemcpyAsync(V.sc, C->h_scal, sizeof(Scal), cudaMemcpyHostToDevice, st));
-        int restarts = 0, first = 1;
+    const int n = Mu.n;
+    BiVec V = C->Vu;
+    V.x = x;
+    V.b = b;
+    HF_CK(cudaMemcpyAsync(V.x, x0, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    Scal h{};
+    h.maxit = C->opt.poisson_maxit;
+    *C->h_scal = h;
+    HF_CK(cudaMemcpyAsync(V.sc, C->h_scal, sizeof(Scal), cudaMemcpyHostToDevice, st));
+    int restarts = 0, first = 1;
+    for (;;) {
+        k_slv_init<<<blocks(n), kBlock, 0, st>>>(Mu, V, rtol, atol, first);
+        launches++;
+        first = 0;
+        int chunk = 4;
         for (;;) {
-            k_slv_init<<<blocks(n), kBlock, 0, st>>>(Mu, V, rtol, atol, first);
-            launches++;
-            first = 0;
-            int chunk = 4;
-            for (;;) {
-                for (int k = 0; k < chunk; k++) {
-                    k_bi_p<<<blocks(n), kBlock, 0, st>>>(Mu, V);
-                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.ph, V.v, 0);
-                    k_bi_s<<<blocks(n), kBlock, 0, st>>>(Mu, V);
-                    k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.sh, V.t, 1);
-                    k_bi_update<<<blocks(n), kBlock, 0, st>>>(Mu, V);
-                    launches += 5;
-                }
-                HF_CK(cudaMemcpyAsync(C->h_scal, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-                HF_CK(cudaStreamSynchronize(st));
-                if (C->h_scal->done) break;
-                chunk = std::min(chunk * 2, 32);
+            for (int k = 0; k < chunk; k++) {
+                k_bi_p<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.ph, V.v, 0);
+                k_bi_s<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(Mu, V, V.sh, V.t, 1);
+                k_bi_update<<<blocks(n), kBlock, 0, st>>>(Mu, V);
+                launches += 5;
             }
-            if (C->h_scal->status == 1 && restarts++ < 50) continue;   // breakdown: restart from x
-            break;
+            HF_CK(cudaMemcpyAsync(C->h_scal, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+            HF_CK(cudaStreamSynchronize(st));
+            if (C->h_scal->done) break;
+            chunk = std::min(chunk * 2, 32);
         }
-        HF_CK(cudaGetLastError());
-        const int status = C->h_scal->status;
-        if (status)
-            return fail(status == 1 ? HF_ERR_NOT_CONVERGED : status,
-                        "semi-implicit velocity BiCGStab failed in direction " + std::to_string(d));
-        C->vel_iters += C->h_scal->iters;
+        if (C->h_scal->status == 1 && restarts++ < 50) continue;   // breakdown: restart from x
+        break;
+    }
+    HF_CK(cudaGetLastError());
+    const int status = C->h_scal->status;
+    if (status)
+        return fail(status == 1 ? HF_ERR_NOT_CONVERGED : status,
+                    "semi-implicit velocity BiCGStab failed in direction " + std::to_string(d));
+    C->vel_iters += C->h_scal->iters;
+    return HF_OK;
+}
+
+// The semi-implicit velocity systems of one step (after the velocity kernel
+// wrote their right-hand sides): per direction BiCGStab with Jacobi scaling,
+// from u as the initial guess, into u*, to the Poisson solve's tolerances (the
+// reference hands both systems to the same solver engine).  BDF2 solves twice:
+// into uaux, then (right-hand sides from k_bdf2_rhs) into u*.  Host-driven:
+// the host reads the scalars between chunks of iterations.
+int sie_solves(hf_case *C, int64_t &launches)
+{
+    const int D = C->D;
+    for (int d = 0; d < D; d++) {
+        double *x = C->bdf2 ? C->ua[d] : C->F.us[d];
+        int rc = sie_solve_dir(C, C->Mu[d], x, C->F.u[d], C->P.sie_b[d], d, launches);
+        if (rc) return rc;
+    }
+    if (!C->bdf2) return HF_OK;
+    for (int d = 0; d < D; d++) {
+        const int n = C->Mu2[d].n;
+        k_bdf2_rhs<<<blocks(n), kBlock, 0, C->stream>>>(n, C->par.dt, C->P.sie_e[d], C->ua[d], C->F.u[d],
+                                                         C->P.sie_bc2[d], C->P.sie_b[d]);
+        launches++;
+        int rc = sie_solve_dir(C, C->Mu2[d], C->F.us[d], C->ua[d], C->P.sie_b[d], d, launches);
+        if (rc) return rc;
     }
     return HF_OK;
 }
@@ -2685,7 +2744,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     memset(&F, 0, sizeof F);
     const bool rk = pg->par.tempdiscrtype == HF_EXPLICIT_RK2 || pg->par.tempdiscrtype == HF_EXPLICIT_RK3;
     if (pg->par.tempdiscrtype != HF_EXPLICIT_EULER && !rk && pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_EULER &&
-        pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_CN)
+        pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_CN && pg->par.tempdiscrtype != HF_SEMI_IMPLICIT_BDF2)
         return cleanup(fail(HF_ERR_UNSUPPORTED, "unknown intermediate-velocity scheme"));
     for (int d = 0; d < D; d++) {
         UP(&F.u[d], (const double *)nullptr, pg->nfacet[d]);
@@ -2712,13 +2771,23 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     // weight 1); entries on one facet are added in stencil order, and each
     // stencil's boundary term (w times the row's rhs) goes to the right-hand
     // side, as sfd_get_stencil does with stn_add_to_rhs.
-    if (pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) {
-        if (ni > 1) return cleanup(fail(HF_ERR_UNSUPPORTED, "semi-implicit Euler in a batch"));
-        const bool cn = pg->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN;
+    const int scheme = pg->par.tempdiscrtype;
+    if (scheme == HF_SEMI_IMPLICIT_EULER || scheme == HF_SEMI_IMPLICIT_CN || scheme == HF_SEMI_IMPLICIT_BDF2) {
+        if (ni > 1) return cleanup(fail(HF_ERR_UNSUPPORTED, "semi-implicit velocity in a batch"));
         C->sie = true;
+        C->bdf2 = scheme == HF_SEMI_IMPLICIT_BDF2;
         P.sie = 1;
         const double dt = pg->par.dt, Re = pg->par.Re;
+        // the weights as the reference writes them: -dt/(Re d^2) (Euler,
+        // hig-flow-step.c:837), - 0.5*dt/(..) (Crank-Nicolson, :939), - 0.25*dt/(..)
+        // then - 1.0/3.0*dt/(..) (BDF2, :1042, :1129)
+        auto weight = [&](int stage, double fd) {
+            if (scheme == HF_SEMI_IMPLICIT_CN) return -0.5 * dt / (Re * fd * fd);
+            if (scheme == HF_SEMI_IMPLICIT_BDF2) return stage == 0 ? -0.25 * dt / (Re * fd * fd) : -1.0 / 3.0 * dt / (Re * fd * fd);
+            return -dt / (Re * fd * fd);
+        };
         int maxnf = 0;
+        for (int stage = 0; stage < (C->bdf2 ? 2 : 1); stage++)
         for (int d = 0; d < D; d++) {
             const int nf = pg->nfacet[d];
             maxnf = std::max(maxnf, nf);
@@ -2735,7 +2804,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 const double *fd = pg->delta + (size_t)pg->vel_delta[d][f] * D;
                 double alpha = 0.0, b = 0.0;
                 for (int d2 = 0; d2 < D; d2++) {
-                    const double w = cn ? -0.5 * dt / (Re * fd[d2] * fd[d2]) : -dt / (Re * fd[d2] * fd[d2]);
+                    const double w = weight(stage, fd[d2]);
                     alpha -= 2.0 * w;
                     for (int side : {HF_V_UR, HF_V_UL}) {
                         const int32_t code = pg->vel_slots[d][(size_t)(HF_V_BLK0 + HF_V_NB * d2 + side) * nf + f];
@@ -2766,14 +2835,22 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 bc[f] = b;
             }
             for (int f = 0; f < nf; f++) dg[f] = dg[f] != 0.0 ? 1.0 / dg[f] : 1.0;
-            DevMat &Mu = C->Mu[d];
+            DevMat &Mu = stage == 0 ? C->Mu[d] : C->Mu2[d];
             Mu.n = nf;
             UP((int32_t **)&Mu.ptr, ptr.data(), ptr.size());
             UP((int32_t **)&Mu.col, col.data(), col.size());
             UP((double **)&Mu.val, val.data(), val.size());
             UP((double **)&Mu.dinv, dg.data(), dg.size());
-            UP((double **)&P.sie_bc[d], bc.data(), bc.size());
-            UP(&P.sie_b[d], (const double *)nullptr, nf);
+            if (stage == 0) {
+                UP((double **)&P.sie_bc[d], bc.data(), bc.size());
+                UP(&P.sie_b[d], (const double *)nullptr, nf);
+                if (C->bdf2) {
+                    UP(&P.sie_e[d], (const double *)nullptr, nf);
+                    UP(&C->ua[d], (const double *)nullptr, nf);
+                }
+            } else {
+                UP((double **)&P.sie_bc2[d], bc.data(), bc.size());
+            }
         }
         BiVec &V = C->Vu;
         UP(&V.r, (const double *)nullptr, maxnf);

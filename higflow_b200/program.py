@@ -21,7 +21,7 @@ import numpy as np
 NEWTONIAN, VISCOELASTIC = 0, 3
 FENE_P, E_FENE = 4, 5
 VE_EXPLICIT, VE_IMPLICIT = 0, 1
-EXPLICIT_EULER, EXPLICIT_RK2, EXPLICIT_RK3, SEMI_IMPLICIT_EULER, SEMI_IMPLICIT_CN = 0, 1, 2, 3, 4
+EXPLICIT_EULER, EXPLICIT_RK2, EXPLICIT_RK3, SEMI_IMPLICIT_EULER, SEMI_IMPLICIT_CN, SEMI_IMPLICIT_BDF2 = 0, 1, 2, 3, 4, 5
 NON_INCREMENTAL, INCREMENTAL = 0, 1
 CENTRAL, FIRST_ORDER, SECOND_ORDER = 0, 1, 2
 MCU, CUBISTA, QUICK = 0, 1, 2

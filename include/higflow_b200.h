@@ -69,7 +69,8 @@ enum { HF_KERNEL_IDENTITY = 0, HF_KERNEL_LOG = 1, HF_KERNEL_SQRT = 2 };
  * (sources - grad p - conv [+ div S]) per direction (hig-flow-step.c:788-883,
  * hig-flow-step-viscoelastic.c:1108-1210) */
 enum { HF_EXPLICIT_EULER = 0, HF_EXPLICIT_RK2 = 1, HF_EXPLICIT_RK3 = 2, HF_SEMI_IMPLICIT_EULER = 3,
-       HF_SEMI_IMPLICIT_CN = 4 };   /* Crank-Nicolson: weights -dt/(2 Re delta^2), half the diffusion explicit */
+       HF_SEMI_IMPLICIT_CN = 4,     /* Crank-Nicolson: weights -dt/(2 Re delta^2), half the diffusion explicit */
+       HF_SEMI_IMPLICIT_BDF2 = 5 }; /* two solves: weights -dt/(4 Re delta^2), then -dt/(3 Re delta^2) */
 
 /* precision forms */
 enum {
@@ -196,7 +197,7 @@ typedef struct hf_params {
     int32_t kernel;               /* HF_KERNEL_*                             */
     double Re, dt;
     double De, beta, kernel_tol, alpha, epsilon, xi;
-    int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / _RK2 / _RK3 / HF_SEMI_IMPLICIT_EULER / _CN */
+    int32_t tempdiscrtype;        /* HF_EXPLICIT_EULER / _RK2 / _RK3 / HF_SEMI_IMPLICIT_EULER / _CN / _BDF2 */
     int32_t pad_;
     double L2_fene, lambda_fene, E_fene;   /* e-FENE (ve_parameters, hig-flow-kernel.h:443-445) */
     int32_t ve_discrtype;         /* HF_VE_EXPLICIT / HF_VE_IMPLICIT (constitutive step) */

@@ -190,6 +190,7 @@ int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
     ns->contr.eoflow = false;
     ns->contr.tempdiscrtype = p->tempdiscrtype == HF_SEMI_IMPLICIT_EULER ? SEMI_IMPLICIT_EULER
                               : p->tempdiscrtype == HF_SEMI_IMPLICIT_CN ? SEMI_IMPLICIT_CN
+                              : p->tempdiscrtype == HF_SEMI_IMPLICIT_BDF2 ? SEMI_IMPLICIT_BDF2
                               : p->tempdiscrtype == HF_EXPLICIT_RK2 ? EXPLICIT_RK2
                               : p->tempdiscrtype == HF_EXPLICIT_RK3 ? EXPLICIT_RK3 : EXPLICIT_EULER;
     ns->contr.spatialdiscrtype = ORDER2;

@@ -48,7 +48,9 @@ static double q(const hf_program *P, int32_t code, const double *f)
 /* terms (hig-flow-terms.c), explicit Euler (hig-flow-step.c:613-660,       */
 /* hig-flow-step-viscoelastic.c:931-980)                                    */
 /* ------------------------------------------------------------------ */
-static void velocity_stage(const hf_program *P, hfr_fields *F, int d)
+/* ebr: BDF2 only, receives the bracket (source - pressure [+ tensor] -
+ * convection) of every facet for the second solve */
+static void velocity_stage_e(const hf_program *P, hfr_fields *F, int d, double *ebr)
 {
     const int D = P->par.dim;
     const int nf = P->nfacet[d];
@@ -238,6 +240,27 @@ static void velocity_stage(const hf_program *P, hfr_fields *F, int d)
             rhs -= conv;
             rhs += diff;
         }
+        if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_BDF2) {
+            /* higflow_semi_implicit_bdf2_intermediate_velocity, first solve
+             * (hig-flow-step.c:1021-1033; viscoelastic
+             * hig-flow-step-viscoelastic.c:1349-1363) */
+            double br = 0.0;
+            br += Fs;
+            br -= pterm;
+            if (ve) {
+                double tens = 0.0;
+                for (int d2 = 0; d2 < D; d2++) tens += dSdx[d2];
+                br += tens;
+            }
+            br -= conv;
+            ebr[f] = br;
+            double r = br;
+            r *= 0.5 * P->par.dt;
+            r += 0.25 * P->par.dt * diff;
+            r += ufacet;
+            F->us[d][f] = r;
+            continue;
+        }
         if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) {
             /* higflow_semi_implicit_euler_intermediate_velocity
              * (hig-flow-step.c:812-829; viscoelastic
@@ -272,6 +295,8 @@ static void velocity_stage(const hf_program *P, hfr_fields *F, int d)
 /* (w times the row's rhs) join the right-hand side held in us[d].      */
 /* Solved by BiCGStab with Jacobi scaling from u.                       */
 /* ------------------------------------------------------------------ */
+static void velocity_stage(const hf_program *P, hfr_fields *F, int d) { velocity_stage_e(P, F, d, NULL); }
+
 typedef struct csr { int n; int64_t *ptr; int32_t *col; double *val; } csr;
 
 static double dot(int n, const double *a, const double *b);
@@ -355,7 +380,10 @@ static void row_add(int32_t *cols, double *vals, int *len, int32_t c, double v)
     (*len)++;
 }
 
-static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
+/* stage: 0 for Euler and Crank-Nicolson and BDF2's first solve, 1 for BDF2's
+ * second (hig-flow-step.c:1129); the right-hand side comes in x (us[d]) and
+ * the solution leaves there, from the initial guess x0 */
+static int sie_solve_x(const hf_program *P, int d, int stage, double *x, const double *x0, double rtol)
 {
     const int D = P->par.dim, nf = P->nfacet[d];
     const double dt = P->par.dt, Re = P->par.Re;
@@ -372,18 +400,19 @@ static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
     A.col = malloc(sizeof(int32_t) * (size_t)nf * cap);
     A.val = malloc(sizeof(double) * (size_t)nf * cap);
     double *bvec = malloc(sizeof(double) * (size_t)nf);
-    double *x = F->us[d];
     int32_t *rc = malloc(sizeof(int32_t) * cap);
     double *rv = malloc(sizeof(double) * cap);
     int64_t nz = 0;
     A.ptr[0] = 0;
     for (int f = 0; f < nf; f++) {
         const double *fd = P->delta + (size_t)P->vel_delta[d][f] * D;
-        double alpha = 0.0, b = F->us[d][f];
+        double alpha = 0.0, b = x[f];
         int len = 0;
         for (int d2 = 0; d2 < D; d2++) {
-            const double w = P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN ? -0.5 * dt / (Re * fd[d2] * fd[d2])
-                                                                          : -dt / (Re * fd[d2] * fd[d2]);
+            double w = -dt / (Re * fd[d2] * fd[d2]);
+            if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN) w = -0.5 * dt / (Re * fd[d2] * fd[d2]);
+            if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_BDF2)
+                w = stage == 0 ? -0.25 * dt / (Re * fd[d2] * fd[d2]) : -1.0 / 3.0 * dt / (Re * fd[d2] * fd[d2]);
             alpha -= 2.0 * w;
             const int sides[2] = {HF_V_UR, HF_V_UL};
             for (int k = 0; k < 2; k++) {
@@ -404,11 +433,46 @@ static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
         A.ptr[f + 1] = nz;
         bvec[f] = b;
     }
-    /* initial guess u */
-    memcpy(x, F->u[d], sizeof(double) * (size_t)nf);
+    memcpy(x, x0, sizeof(double) * (size_t)nf);
     const int status = csr_bicgstab(&A, bvec, x, rtol);
     free(A.ptr); free(A.col); free(A.val); free(bvec); free(rc); free(rv);
     return status;
+}
+
+static int sie_solve(const hf_program *P, hfr_fields *F, int d, double rtol)
+{
+    return sie_solve_x(P, d, 0, F->us[d], F->u[d], rtol);
+}
+
+/* BDF2 (hig-flow-step.c:992-1179; viscoelastic
+ * hig-flow-step-viscoelastic.c:1320-1513): every direction's first solve
+ * into uaux, then the second with right-hand side bracket * dt/3 +
+ * (4 uaux - u)/3 (hig-flow-step.c:1119-1120) into u* */
+static int bdf2_velocity(const hf_program *P, hfr_fields *F, double rtol)
+{
+    const int D = P->par.dim;
+    double *ebr[3] = {0}, *ua[3] = {0};
+    int rc = 0;
+    for (int d = 0; d < D; d++) {
+        ebr[d] = malloc(sizeof(double) * (size_t)P->nfacet[d]);
+        ua[d] = malloc(sizeof(double) * (size_t)P->nfacet[d]);
+        velocity_stage_e(P, F, d, ebr[d]);
+    }
+    for (int d = 0; d < D && rc == 0; d++) {
+        memcpy(ua[d], F->us[d], sizeof(double) * (size_t)P->nfacet[d]);
+        rc = sie_solve_x(P, d, 0, ua[d], F->u[d], rtol);
+    }
+    for (int d = 0; d < D && rc == 0; d++) {
+        for (int f = 0; f < P->nfacet[d]; f++) {
+            double r = ebr[d][f];
+            r *= 1.0 / 3.0 * P->par.dt;
+            r += (4.0 * ua[d][f] - F->u[d][f]) / 3.0;
+            F->us[d][f] = r;
+        }
+        rc = sie_solve_x(P, d, 1, F->us[d], ua[d], rtol);
+    }
+    for (int d = 0; d < D; d++) { free(ebr[d]); free(ua[d]); }
+    return rc;
 }
 
 /* ------------------------------------------------------------------ */
@@ -1094,6 +1158,7 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
             polymeric_stage(P, F);
         }
         if (P->par.tempdiscrtype == HF_EXPLICIT_RK2 || P->par.tempdiscrtype == HF_EXPLICIT_RK3) rk_stage(P, F);
+        else if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_BDF2) rc = bdf2_velocity(P, F, rtol);
         else
             for (int d = 0; d < D; d++) velocity_stage(P, F, d);
         if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN)
@@ -1110,6 +1175,10 @@ int hfr_step(const hf_program *P, hfr_fields *F, int nsteps, double rtol, int *i
 /* individual stages, for stage-by-stage parity tests */
 void hfr_velocity(const hf_program *P, hfr_fields *F)
 {
+    if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_BDF2) {
+        bdf2_velocity(P, F, 1e-14);
+        return;
+    }
     for (int d = 0; d < P->par.dim; d++) velocity_stage(P, F, d);
     if (P->par.tempdiscrtype == HF_SEMI_IMPLICIT_EULER || P->par.tempdiscrtype == HF_SEMI_IMPLICIT_CN)
         for (int d = 0; d < P->par.dim; d++) sie_solve(P, F, d, 1e-14);

@@ -89,6 +89,12 @@ CASES = {
     "cn2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                               tempdiscrtype=hp.SEMI_IMPLICIT_CN), 3, (0.3, 0.1, 0.2)),
+    # semi-implicit BDF2 (two solves per direction: into uaux, then into u*)
+    "bdf2_cav2d": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
+                   4, (0.3, 0.1, 0.0)),
+    "bdf2_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
+                                              ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
+                                              tempdiscrtype=hp.SEMI_IMPLICIT_BDF2), 3, (0.3, 0.1, 0.2)),
     "amr2d_sie_oldroyd": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
                                                ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                                tempdiscrtype=hp.SEMI_IMPLICIT_EULER,

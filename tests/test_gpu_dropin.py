@@ -35,6 +35,8 @@ CASES = {
     "oldroyd_sie": lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC, ve_model=hp.OLDROYD_B,
                                         kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                         tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
+    # semi-implicit BDF2 (two solves per direction)
+    "newtonian_bdf2": lambda: refpy.cavity(2, 12, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
 }
 
 

@@ -188,10 +188,11 @@ def test_semi_implicit_velocity_refused_in_a_batch():
     assert e.value.code == -2 and "semi-implicit" in str(e.value)   # HF_ERR_UNSUPPORTED
 
 
-def test_semi_implicit_velocity_iterates_and_counts_launches():
+@pytest.mark.parametrize("name", ["sie2d_cubista", "bdf2_cav2d"])
+def test_semi_implicit_velocity_iterates_and_counts_launches(name):
     """A semi-implicit step runs eagerly and its velocity solves' kernels are
     counted in the step statistics."""
-    prog, data = load_golden("sie2d_cubista")
+    prog, data = load_golden(name)
     case = engine.Case(prog, _opts())
     load_init(case, prog, data)
     case.step(2)
