@@ -285,8 +285,13 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
         if (ns->ed.ve.contr.model == FENE_P)
             return REASON(HF_ERR_UNSUPPORTED, "FENE-P (the reference's stress for it reads an unassigned xi)");
         if (ns->ed.ve.contr.model != OLDROYD_B && ns->ed.ve.contr.model != GIESEKUS &&
-            ns->ed.ve.contr.model != LPTT && ns->ed.ve.contr.model != E_FENE)
-            return REASON(HF_ERR_UNSUPPORTED, "viscoelastic model other than Oldroyd-B, Giesekus, LPTT, e-FENE");
+            ns->ed.ve.contr.model != LPTT && ns->ed.ve.contr.model != GPTT && ns->ed.ve.contr.model != E_FENE)
+            return REASON(HF_ERR_UNSUPPORTED, "viscoelastic model other than Oldroyd-B, Giesekus, LPTT, GPTT, e-FENE");
+        /* the Mittag-Leffler evaluation takes 0 < alpha <= 5 and beta <= 5
+         * (hig-flow-mittag-leffler.c:143-153 reports the others as errors) */
+        if (ns->ed.ve.contr.model == GPTT &&
+            !(ns->ed.ve.par.alpha_gptt > 0.0 && ns->ed.ve.par.alpha_gptt <= 5.0 && ns->ed.ve.par.beta_gptt <= 5.0))
+            return REASON(HF_ERR_INVALID, "GPTT needs 0 < alpha_gptt <= 5 and beta_gptt <= 5");
         if (detect_kernel(ns, &kernel)) return REASON(HF_ERR_UNSUPPORTED, "kernel transform callbacks are not identity, log or sqrt");
     }
 
@@ -345,6 +350,9 @@ int hf_flatten(higflow_solver *ns, hf_program **out)
         par->L2_fene = ns->ed.ve.par.L2_fene;
         par->lambda_fene = ns->ed.ve.par.lambda_fene;
         par->E_fene = ns->ed.ve.par.E_fene;
+        par->alpha_gptt = ns->ed.ve.par.alpha_gptt;
+        par->beta_gptt = ns->ed.ve.par.beta_gptt;
+        par->gamma_gptt = tgamma(ns->ed.ve.par.beta_gptt);
         par->ve_discrtype = ns->ed.ve.contr.discrtype == IMPLICIT ? HF_VE_IMPLICIT : HF_VE_EXPLICIT;
     }
 

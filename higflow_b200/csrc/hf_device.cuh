@@ -11,6 +11,10 @@
 #define HF_EPSMACH 1.0e-12
 #define HF_FLT_EQ(x, y) (fabs((x) - (y)) < HF_EPSMACH)  // higtree/src/utils.h:40
 
+// pi to double precision (the reference's pi, hig-flow-mittag-leffler.h:8,
+// rounds to the same double)
+#define HF_PI 3.141592653589793238462643383279502884
+
 namespace hf {
 
 // General stencil rows, in FP64 or FP32 storage.
@@ -348,6 +352,185 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
         }
     }
     return ((conv1 - conv2) / cdelta);
+}
+
+// ---------------------------------------------------------------------------
+// Mittag-Leffler function E_{a,b}(z) for the GPTT model (hig_flow_calculate_m_
+// gptt, hig-flow-step-viscoelastic.c:1771-1830; the reference evaluates it with
+// mlfv, hig-flow-mittag-leffler.c:117-366).  The published algorithm of
+// Gorenflo, Loutchko and Luchko (Fract. Calc. Appl. Anal. 5, 2002): power
+// series near the origin, the integral representation (ray integral of K, arc
+// integral of P, Romberg's rule) in the middle, the asymptotic series far out
+// for a <= 1, and for a > 1 the reduction to smaller a over roots of z.  rho =
+// 10^-fi sets the region bounds and the arc's Romberg levels (the ray takes
+// six, as the reference's rombint does, :53-56).  Powers of z are polar,
+// |z|^p e^{i p arg z}.  Only real parts enter the model; the leading term's
+// imaginary part is the true one (the reference's differs in sign, which never
+// reaches a real part).  The recursion depth is static: a >= 2 reduces to
+// [1, 2), which halves to below 1, where nothing recurses (level L = 2 at the
+// top).  Every loop is bounded.
+// ---------------------------------------------------------------------------
+struct Cx { double re, im; };
+
+__device__ inline Cx cx_make(double re, double im) { Cx z; z.re = re; z.im = im; return z; }
+__device__ inline Cx cx_polar(double r, double t) { return cx_make(r * cos(t), r * sin(t)); }
+__device__ inline Cx cx_add(Cx a, Cx b) { return cx_make(a.re + b.re, a.im + b.im); }
+__device__ inline Cx cx_div(Cx a, Cx b)
+{
+    const double d = b.re * b.re + b.im * b.im;
+    return cx_make((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d);
+}
+
+struct MlArgs { double a, b, eps; Cx z; };
+
+// ray integrand: r^((1-b)/a) e^(-r^(1/a)) / (pi a)
+//   * (r sin(pi(1-b)) - z sin(pi(1-b+a))) / (r^2 - 2 r z cos(pi a) + z^2)
+__device__ inline Cx ml_ray(const MlArgs &c, double r)
+{
+    const double a = c.a, b = c.b;
+    const double A = pow(r, (1.0 - b) / a) * exp(-pow(r, 1.0 / a)) / (HF_PI * a);
+    const double s1 = r * sin(HF_PI * (1.0 - b)), s2 = sin(HF_PI * (1.0 - b + a));
+    const double e = 2.0 * r * cos(HF_PI * a);
+    const Cx num = cx_make(s1 - s2 * c.z.re, -s2 * c.z.im);
+    const Cx den = cx_make(r * r - e * c.z.re + (c.z.re * c.z.re - c.z.im * c.z.im), -e * c.z.im + 2.0 * c.z.re * c.z.im);
+    const Cx q = cx_div(num, den);
+    return cx_make(A * q.re, A * q.im);
+}
+
+// arc integrand on |zeta| = eps: eps^(1+(1-b)/a) e^(eps^(1/a) cos(phi/a))
+//   e^{i w} / (2 pi a (eps e^{i phi} - z)), w = eps^(1/a) sin(phi/a) + phi (1+(1-b)/a)
+__device__ inline Cx ml_arc(const MlArgs &c, double phi)
+{
+    const double a = c.a, b = c.b, eps = c.eps;
+    const double p = 1.0 + (1.0 - b) / a, er = pow(eps, 1.0 / a);
+    const double A = pow(eps, p) * exp(er * cos(phi / a)) / (2.0 * HF_PI * a);
+    const double w = er * sin(phi / a) + phi * p;
+    return cx_div(cx_polar(A, w), cx_make(eps * cos(phi) - c.z.re, eps * sin(phi) - c.z.im));
+}
+
+// Romberg's rule, one row kept in place: R[k] of the new row needs R[k-1] of
+// the new row and R[k-1] of the old one.  At most eight levels (the
+// reference's table holds eight, rombint :46-50)
+template <bool RAY>
+__device__ __noinline__ Cx ml_romberg(MlArgs c, double lo, double hi, int n)
+{
+    if (RAY) n = 6;
+    n = n < 1 ? 1 : (n > 8 ? 8 : n);
+    Cx R[8];
+    for (int k = 0; k < 8; k++) R[k] = cx_make(0.0, 0.0);
+    double h = hi - lo;
+    const Cx fa = RAY ? ml_ray(c, lo) : ml_arc(c, lo);
+    const Cx fb = RAY ? ml_ray(c, hi) : ml_arc(c, hi);
+    R[0] = cx_make(h * (fa.re + fb.re) / 2.0, h * (fa.im + fb.im) / 2.0);
+    int npts = 1;
+    for (int i = 1; i < n; i++) {
+        Cx s = cx_make(0.0, 0.0);
+        for (int j = 1; j <= npts; j++) s = cx_add(s, RAY ? ml_ray(c, lo + h * (j - 0.5)) : ml_arc(c, lo + h * (j - 0.5)));
+        Cx old = R[0];
+        R[0] = cx_make((R[0].re + h * s.re) / 2.0, (R[0].im + h * s.im) / 2.0);
+        double q = 1.0;
+        for (int k = 1; k <= i; k++) {
+            q *= 4.0;
+            const Cx ok = R[k];
+            R[k] = cx_make((q * R[k - 1].re - old.re) / (q - 1.0), (q * R[k - 1].im - old.im) / (q - 1.0));
+            old = ok;
+        }
+        npts *= 2;
+        h /= 2.0;
+    }
+    return R[n - 1];
+}
+
+// z^((1-b)/a) e^(z^(1/a)) / a
+__device__ inline Cx ml_lead(double a, double b, double az, double th)
+{
+    const double ra = pow(az, 1.0 / a);
+    const double mag = (pow(az, (1.0 - b) / a) / a) * exp(ra * cos(th / a));
+    return cx_polar(mag, th * (1.0 - b) / a + ra * sin(th / a));
+}
+
+template <int L>
+__device__ __noinline__ Cx mittag_leffler(double a, double b, Cx z, int fi)
+{
+    const double az = sqrt(z.re * z.re + z.im * z.im);
+    const double th = atan2(z.im, z.re), ath = fabs(th);
+    const double rho = pow(10.0, (double)-fi);
+    const bool series = (a < 1.0 && az <= 1.0) ||
+                        (1.0 <= a && a < 2.0 && az <= floor(20.0 / pow(2.1 - a, 5.5 - 2.0 * a))) ||
+                        (a >= 2.0 && az <= 50.0);
+    if (series) {
+        int k = 0;
+        while (a * k + b <= 0.0 && k < 1000000) k++;
+        Cx s = cx_make(pow(az, (double)k) * cos(th * k) / tgamma(a * k + b),
+                       pow(az, (double)k) * sin(th * k) / tgamma(a * k + b));
+        for (int it = 0; it < 100000; it++) {
+            const Cx old = s;
+            for (int t = 0; t < 2; t++) {
+                k++;
+                const double g = tgamma(a * k + b), pk = pow(az, (double)k);
+                s = cx_make(s.re + pk * cos(th * k) / g, s.im + pk * sin(th * k) / g);
+            }
+            if (s.re == old.re && s.im == old.im) break;
+        }
+        return s;
+    }
+    if (a <= 1.0 && az <= floor(5.0 * a + 10.0)) {
+        const double r0 = fmax(fmax(1.0, 2.0 * az), pow(-2.0 * log(rho * HF_PI / 6.0), a));
+        MlArgs c;
+        c.a = a; c.b = b; c.eps = 0.0; c.z = z;
+        const double pa = HF_PI * a;
+        if (ath > pa && fabs(ath - pa) > rho) {
+            if (b <= 1.0) return ml_romberg<true>(c, 0.0, r0, fi);
+            c.eps = 1.0;
+            return cx_add(ml_romberg<true>(c, c.eps, r0, fi), ml_romberg<false>(c, -pa, pa, fi));
+        }
+        if (ath < pa && fabs(ath - pa) > rho) {
+            if (b <= 1.0) return cx_add(ml_romberg<true>(c, 0.0, r0, fi), ml_lead(a, b, az, th));
+            c.eps = az / 2.0;
+            const Cx arc = ml_romberg<false>(c, -pa, pa, fi);
+            return cx_add(cx_add(arc, ml_romberg<true>(c, c.eps, r0, fi)), ml_lead(a, b, az, th));
+        }
+        c.eps = az + 0.5;
+        return cx_add(ml_romberg<true>(c, c.eps, r0, fi), ml_romberg<false>(c, -pa, pa, fi));
+    }
+    if (a <= 1.0) {
+        Cx s = cx_make(0.0, 0.0);
+        if (ath < (HF_PI * a / 2.0 + fmin(HF_PI, HF_PI * a)) / 2.0) s = ml_lead(a, b, az, th);
+        const double kmax = floor(fi / log10(az));
+        for (int k = 1; k <= kmax && k <= 64; k++) {
+            const double g = b - a * k;
+            if (ceil(g) == floor(g)) continue;
+            const double pk = pow(az, (double)-k);
+            s = cx_make(s.re - pk * cos(th * k) / tgamma(g), s.im - (-(pk * sin(th * k))) / tgamma(g));
+        }
+        return s;
+    }
+    if constexpr (L > 0) {
+        if (a >= 2.0) {
+            const int m = (int)floor(a / 2.0);
+            Cx s = cx_make(0.0, 0.0);
+            for (int h = 0; h <= m && h < 64; h++) {
+                const double r = pow(az, 1.0 / (m + 1.0));
+                s = cx_add(s, mittag_leffler<L - 1>(a / (m + 1), b, cx_polar(r, (2.0 * HF_PI * h + th) / (m + 1.0)), fi));
+            }
+            const double w = 1.0 / (m + 1.0);
+            return cx_make(w * s.re, w * s.im);
+        }
+        const double r = sqrt(az);
+        const Cx z1 = cx_make(r * cos(th / 2.0), r * sin(th / 2.0));
+        const Cx e1 = mittag_leffler<L - 1>(a / 2.0, b, z1, fi);
+        const Cx e2 = mittag_leffler<L - 1>(a / 2.0, b, cx_make(-z1.re, -z1.im), fi);
+        return cx_make((e1.re + e2.re) / 2.0, (e1.im + e2.im) / 2.0);
+    } else {
+        // unreachable: at the last level a < 1
+        return cx_make(nan(""), nan(""));
+    }
+}
+
+// E_{a_g,b_g}(z) for real z with fi = 6, as the GPTT M term takes it (:1805)
+__device__ __noinline__ double gptt_ml(double alpha_g, double beta_g, double z)
+{
+    return mittag_leffler<2>(alpha_g, beta_g, cx_make(z, 0.0), 6).re;
 }
 
 }  // namespace hf

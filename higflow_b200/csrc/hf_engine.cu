@@ -102,6 +102,9 @@ struct DevProg {
     // S] - conv bracket of the velocity kernel, kept for its right-hand side
     const double *sie_bc2[3];
     double *sie_e[3];
+    // GPTT: E_{alpha,beta}(eps Re De tr S / (1 - beta)) per cell, written by
+    // k_gptt_ml ahead of k_ve_cell (null when no instance is GPTT)
+    double *gptt_e;
     const int32_t *dslots;
     const uint16_t *cdelta;
     const int32_t *cslots;
@@ -572,6 +575,23 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 // 8: 1.22, 16 at 32 registers: 1.19 with far more spill traffic)
 constexpr int kVeBlock = 128;
 
+// The GPTT model's Mittag-Leffler factor of every GPTT cell, from the stress
+// that k_ve_cell then reads (trace summed in its order).  A kernel of its own:
+// the out-of-line evaluation inside k_ve_cell would spill that kernel's
+// registers for every model.
+template <int D>
+__global__ void __launch_bounds__(kBlock) k_gptt_ml(DevProg P, DevFields F)
+{
+    const int cc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cc >= P.ncell) return;
+    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    if (pr.ve_model != HF_GPTT) return;
+    double trS = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; i++) trS += F.S[i * D + i][cc];
+    P.gptt_e[cc] = hf::gptt_ml(pr.alpha_gptt, pr.beta_gptt, pr.epsilon * pr.Re * pr.De * trS / (1.0 - pr.beta));
+}
+
 // IMPL: the implicit constitutive step (hf_params.ve_discrtype, the same for
 // every instance of a case), a separate instantiation so that the explicit
 // kernel carries none of its code
@@ -662,7 +682,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
         for (int j = 0; j < D; j++) {
             Mt[i][j] = Du[i][j];
-            if (pr.ve_model == HF_LPTT) Mt[i][j] -= pr.xi * 0.5 * (Du[i][j] + Du[j][i]);
+            if (pr.ve_model == HF_LPTT || pr.ve_model == HF_GPTT) Mt[i][j] -= pr.xi * 0.5 * (Du[i][j] + Du[j][i]);
         }
     hf::mprod<D>(Mt, Rm, M);
     double Oa[D][D], Om[D][D];
@@ -690,6 +710,11 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
         const double b = pr.L2_fene, lf = pr.lambda_fene, E = pr.E_fene;
         fA = b / (b - trA) - E * sqrt(b) * exp(-sqrt(trA) / lf) * (1.0 / (trA * lf) + 1 / (trA * sqrt(trA)));
     }
+    // GPTT (hig_flow_calculate_m_gptt, :1771-1830): Gamma(beta_g) times the
+    // Mittag-Leffler E_{alpha_g,beta_g}(eps Re De tr S / (1 - beta)) in place of
+    // LPTT's linear factor
+    double mlv = 0.0;
+    if (pr.ve_model == HF_GPTT) mlv = P.gptt_e[cc];
 #pragma unroll
     for (int i = 0; i < D; i++) {
 #pragma unroll
@@ -703,6 +728,8 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
             Ma[i][i] = (aux - pr.alpha * aux * aux) * jl[i];
         } else if (pr.ve_model == HF_LPTT) {
             Ma[i][i] = (1.0 - lam[i]) * (1.0 + (pr.epsilon * Re * De * trS) / (1.0 - pr.beta)) * jl[i];
+        } else if (pr.ve_model == HF_GPTT) {
+            Ma[i][i] = (1.0 - lam[i]) * pr.gamma_gptt * mlv * jl[i];
         } else if (pr.ve_model == HF_E_FENE) {
             Ma[i][i] = (1.0 - fA * lam[i]) * jl[i];
         } else {
@@ -848,11 +875,11 @@ __global__ void __launch_bounds__(kBlock) k_ve_stress(DevProg P, DevFields F)
         Bk[i][i] = hf::kernel_inverse(pr.kernel, lam2[i]);
     }
     hf::mtprod<D>(Bk, R2, A);
-    // the model switch of hig-flow-step-viscoelastic.c:274-309: LPTT sets xi;
+    // the model switch of hig-flow-step-viscoelastic.c:274-309: LPTT and GPTT set xi;
     // e-FENE computes its fA there but falls through to the default, so its
     // stress is formed with fA = a = 1, xi = 0 like Oldroyd-B and Giesekus
     const double fA = 1.0, aa = 1.0, beta = pr.beta;
-    const double xi = pr.ve_model == HF_LPTT ? pr.xi : 0.0;
+    const double xi = pr.ve_model == HF_LPTT || pr.ve_model == HF_GPTT ? pr.xi : 0.0;
 #pragma unroll
     for (int i = 0; i < D; i++) {
         double Si[D];
@@ -1208,6 +1235,7 @@ struct hf_case {
     // BiCGStab into u* (scratch Vu shared by the directions)
     bool sie = false;
     bool bdf2 = false;
+    bool gptt = false;              // some instance uses the GPTT model
     DevMat Mu[3] = {};
     DevMat Mu2[3] = {};             // BDF2: the second solve's systems
     double *ua[3] = {};             // BDF2: the first solve's velocity (dpuaux)
@@ -2190,6 +2218,10 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     if (ve) {
         record(C, HF_PHASE_VE_CELL, 0);
+        if (C->gptt) {
+            k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
+            fixed++;
+        }
         if (C->par.ve_discrtype == HF_VE_IMPLICIT)
             k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
         else
@@ -2417,6 +2449,10 @@ int bicg_step(hf_case *C)
     int64_t launches = 0;
     if (ve) {
         PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
+        if (C->gptt) {
+            k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
+            launches++;
+        }
         if (C->par.ve_discrtype == HF_VE_IMPLICIT)
             k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
         else
@@ -2603,6 +2639,16 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     }
     const int ni = C->ninst;
     if (C->coff[0] != 0 || C->coff[ni] != pg->ncell) return cleanup(fail(HF_ERR_INVALID, "cell offsets"));
+    for (const hf_params &q : ipar) {
+        if (q.flowtype != HF_VISCOELASTIC) continue;
+        if (q.ve_model != HF_OLDROYD_B && q.ve_model != HF_GIESEKUS && q.ve_model != HF_LPTT && q.ve_model != HF_GPTT &&
+            q.ve_model != HF_E_FENE)
+            return cleanup(fail(HF_ERR_UNSUPPORTED, "viscoelastic model other than Oldroyd-B, Giesekus, LPTT, GPTT, e-FENE"));
+        // the reference's Mittag-Leffler evaluation takes 0 < alpha <= 5 and
+        // beta <= 5 (hig-flow-mittag-leffler.c:143-153)
+        if (q.ve_model == HF_GPTT && !(q.alpha_gptt > 0.0 && q.alpha_gptt <= 5.0 && q.beta_gptt <= 5.0))
+            return cleanup(fail(HF_ERR_INVALID, "GPTT needs 0 < alpha_gptt <= 5 and beta_gptt <= 5"));
+    }
     for (int d = 0; d < D; d++)
         if (C->foff[d][0] != 0 || C->foff[d][ni] != pg->nfacet[d]) return cleanup(fail(HF_ERR_INVALID, "facet offsets"));
     for (int i = 0; i < ni; i++) {
@@ -2634,6 +2680,8 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         for (int i = 0; i < ni; i++) C->dt0[i] = ipar[i].dt;
         UP(&C->cfl_max, (const unsigned long long *)nullptr, ni);
         UP((double **)&P.ipinv, pinv.data(), pinv.size());
+        for (const hf_params &q : ipar) C->gptt |= q.flowtype == HF_VISCOELASTIC && q.ve_model == HF_GPTT;
+        if (C->gptt) UP(&P.gptt_e, (const double *)nullptr, pg->ncell);
     }
     UP((double **)&P.delta, pg->delta, (size_t)pg->ndelta * D);
     UP((int32_t **)&P.rows.tmpl, pg->row_tmpl, pg->nrows);
@@ -3492,6 +3540,43 @@ __global__ void k_na_begin(Scal *sc, int maxit)
 }
 
 }  // namespace
+
+namespace {
+
+__global__ void __launch_bounds__(kBlock) k_mittag_leffler(int n, double a, double b, int fi,
+                                                           const double *__restrict__ z, double *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const hf::Cx e = hf::mittag_leffler<2>(a, b, hf::cx_make(z[2 * i], z[2 * i + 1]), fi);
+    out[2 * i] = e.re;
+    out[2 * i + 1] = e.im;
+}
+
+}  // namespace
+
+extern "C" int hf_mittag_leffler(double alpha, double beta, const double *z, int64_t n, int32_t fi, double *out)
+{
+    if (n < 0 || n > (int64_t)1 << 30 || (n > 0 && (!z || !out))) return fail(HF_ERR_INVALID, "bad argument");
+    if (!(alpha > 0.0 && alpha <= 5.0) || !(beta <= 5.0))
+        return fail(HF_ERR_INVALID, "Mittag-Leffler needs 0 < alpha <= 5 and beta <= 5");
+    if (fi < 1 || fi > 8) return fail(HF_ERR_INVALID, "Mittag-Leffler accuracy digits fi must be 1..8");
+    if (n == 0) return HF_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HF_ERR_NO_DEVICE, "no CUDA device");
+    double *d = nullptr;
+    const size_t bytes = sizeof(double) * 2 * (size_t)n;
+    HF_CK(cudaMalloc(&d, 2 * bytes));
+    cudaError_t e = cudaMemcpy(d, z, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_mittag_leffler<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock>>>((int)n, alpha, beta, fi, d, d + 2 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(HF_ERR_CUDA, std::string("Mittag-Leffler evaluation: ") + cudaGetErrorString(e));
+    return HF_OK;
+}
 
 extern "C" int hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const int32_t *col, const double *val,
                                            const double *b, double *x, double rtol, double atol, int32_t maxit,

@@ -57,6 +57,7 @@ def lib() -> C.CDLL:
                                           P(C.c_int64), P(C.c_int64), C.c_int32]
         L.hf_case_profile.argtypes = [V, C.c_int32]
         L.hf_case_phase_times.argtypes = [V, P(C.c_double), P(C.c_int64), C.c_int32]
+        L.hf_mittag_leffler.argtypes = [C.c_double, C.c_double, P(C.c_double), C.c_int64, C.c_int32, P(C.c_double)]
         _lib = L
     return _lib
 
@@ -191,6 +192,18 @@ class Case:
         la = (C.c_int64 * n)()
         _check(lib().hf_case_phase_times(self.h, ms, la, n))
         return {p: (ms[i], la[i]) for i, p in enumerate(self.PHASES)}
+
+
+def mittag_leffler(alpha: float, beta: float, z, fi: int = 6) -> np.ndarray:
+    """E_{alpha,beta}(z) on the GPU at every point of ``z`` (the evaluation the
+    GPTT model takes; the reference's ``mlfv``, hig-flow-mittag-leffler.c:117).
+    Returns a complex array of the shape of ``z``."""
+    zc = np.ascontiguousarray(np.asarray(z, dtype=np.complex128))
+    zi = zc.reshape(-1).view(np.float64)
+    out = np.empty_like(zi)
+    _check(lib().hf_mittag_leffler(alpha, beta, zi.ctypes.data_as(C.POINTER(C.c_double)), zc.size, fi,
+                                   out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out.view(np.complex128).reshape(zc.shape)
 
 
 def device_bytes(prog: hp.Program, opts: Optional[hp.HFOptions] = None) -> int:

@@ -19,7 +19,7 @@ import numpy as np
 
 # enumerations (include/higflow_b200.h)
 NEWTONIAN, VISCOELASTIC = 0, 3
-FENE_P, E_FENE = 4, 5
+GPTT, FENE_P, E_FENE = 3, 4, 5
 VE_EXPLICIT, VE_IMPLICIT = 0, 1
 EXPLICIT_EULER, EXPLICIT_RK2, EXPLICIT_RK3, SEMI_IMPLICIT_EULER, SEMI_IMPLICIT_CN, SEMI_IMPLICIT_BDF2 = 0, 1, 2, 3, 4, 5
 NON_INCREMENTAL, INCREMENTAL = 0, 1
@@ -86,6 +86,7 @@ class HFParams(C.Structure):
         ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
         ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
         ("ve_discrtype", C.c_int32), ("pad2_", C.c_int32),
+        ("alpha_gptt", C.c_double), ("beta_gptt", C.c_double), ("gamma_gptt", C.c_double),
     ]
 
 
@@ -145,7 +146,7 @@ class HFStats(C.Structure):
 _PARAM_NAMES = [n for n, _ in HFParams._fields_]
 # parameters that programs written before they existed do not carry
 _PARAM_DEFAULTS = {"tempdiscrtype": 0, "pad_": 0, "L2_fene": 0.0, "lambda_fene": 0.0, "E_fene": 0.0,
-                   "ve_discrtype": 0, "pad2_": 0}
+                   "ve_discrtype": 0, "pad2_": 0, "alpha_gptt": 1.0, "beta_gptt": 1.0, "gamma_gptt": 1.0}
 _INT_PARAMS = ("dim", "flowtype", "projtype", "convecdiscrtype", "secondconvecdiscrtype", "ve_model",
                "ve_convecdiscrtype", "kernel", "tempdiscrtype", "pad_", "ve_discrtype", "pad2_")
 

@@ -55,7 +55,7 @@ enum { HF_NON_INCREMENTAL = 0, HF_INCREMENTAL = 1 };            /* projection   
 enum { HF_CENTRAL = 0, HF_FIRST_ORDER = 1, HF_SECOND_ORDER = 2 };/* convecdiscr   */
 enum { HF_MCU = 0, HF_CUBISTA = 1, HF_QUICK = 2 };              /* second order   */
 enum { HF_OLDROYD_B = 0, HF_GIESEKUS = 1, HF_LPTT = 2,           /* VE model       */
-       HF_FENE_P = 4, HF_E_FENE = 5 };
+       HF_GPTT = 3, HF_FENE_P = 4, HF_E_FENE = 5 };
 enum { HF_CELL_CENTRAL = 0, HF_CELL_CUBISTA = 1 };              /* VE convection  */
 /* constitutive step (hig-flow-kernel.h:305-308): explicit Euler, or the
  * implicit form that solves (I - dt (Omega x I - I x Omega)) K = K + dt (-conv
@@ -202,6 +202,11 @@ typedef struct hf_params {
     double L2_fene, lambda_fene, E_fene;   /* e-FENE (ve_parameters, hig-flow-kernel.h:443-445) */
     int32_t ve_discrtype;         /* HF_VE_EXPLICIT / HF_VE_IMPLICIT (constitutive step) */
     int32_t pad2_;
+    /* GPTT (ve_parameters, hig-flow-kernel.h:439-441): the Mittag-Leffler
+     * E_{alpha,beta} parameters and gamma = Gamma(beta_gptt), which the
+     * reference recomputes with tgamma every constitutive step
+     * (hig-flow-step-viscoelastic.c:359-362) */
+    double alpha_gptt, beta_gptt, gamma_gptt;
 } hf_params;
 
 /* A flattened step program (host memory, read-only for the engine). */
@@ -454,6 +459,16 @@ void hf_slv_destroy(hf_slv *s);                                                /
 int  hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const int32_t *col, const double *val,
                                  const double *b, double *x, double rtol, double atol, int32_t maxit,
                                  void *stream, int32_t *iterations, double *residual);
+
+/* The Mittag-Leffler function E_{alpha,beta}(z) that the GPTT model's M term
+ * takes (replaces mlfv, hig-flow-mittag-leffler.h:22 / .c:117), evaluated on
+ * the current device at n points: z and out are host arrays of 2n doubles,
+ * real and imaginary parts interleaved.  fi: accuracy digits, 1..8 (the model
+ * passes 6).  0 < alpha <= 5, beta <= 5 (the range the reference's evaluation
+ * accepts); otherwise HF_ERR_INVALID.  Real parts follow the reference; the
+ * imaginary part of the asymptotic form's leading term is the true one (the
+ * reference's has the wrong sign there). */
+int  hf_mittag_leffler(double alpha, double beta, const double *z, int64_t n, int32_t fi, double *out);
 
 #ifdef __cplusplus
 }

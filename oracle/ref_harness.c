@@ -51,6 +51,7 @@ typedef struct hfref_params {
     double L2_fene, lambda_fene, E_fene;
     int32_t ve_discrtype;       /* HF_VE_EXPLICIT / HF_VE_IMPLICIT */
     int32_t pad2_;
+    double alpha_gptt, beta_gptt;
 } hfref_params;
 
 typedef struct hfref_case {
@@ -209,6 +210,8 @@ int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
         ns->ed.ve.par.L2_fene = p->L2_fene;
         ns->ed.ve.par.lambda_fene = p->lambda_fene;
         ns->ed.ve.par.E_fene = p->E_fene;
+        ns->ed.ve.par.alpha_gptt = p->alpha_gptt;
+        ns->ed.ve.par.beta_gptt = p->beta_gptt;
     }
 
     higflow_set_external_functions(ns, cb_get_pressure, cb_get_velocity, cb_get_source_term,

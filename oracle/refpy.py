@@ -40,6 +40,7 @@ class RefParams(C.Structure):
         ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
         ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
         ("ve_discrtype", C.c_int32), ("pad2_", C.c_int32),
+        ("alpha_gptt", C.c_double), ("beta_gptt", C.c_double),
     ]
 
 
@@ -94,6 +95,22 @@ def lib(dim: int) -> C.CDLL:
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class _Numc(C.Structure):
+    _fields_ = [("real", C.c_double), ("imag", C.c_double)]
+
+
+def mlfv(alpha: float, beta: float, z: complex, fi: int = 6) -> complex:
+    """The reference's own Mittag-Leffler evaluation (hig-flow-mittag-leffler.c:117),
+    from the 2D build."""
+    L = lib(2)
+    if not getattr(L, "_mlfv_set", False):
+        L.mlfv.argtypes = [C.c_double, C.c_double, _Numc, C.c_int]
+        L.mlfv.restype = _Numc
+        L._mlfv_set = True
+    r = L.mlfv(alpha, beta, _Numc(z.real, z.imag), fi)
+    return complex(r.real, r.imag)
 
 
 class RefCase:
@@ -319,6 +336,8 @@ class CaseSpec:
         p.lambda_fene = g("lambda_fene", 1.0)
         p.E_fene = g("E_fene", 0.0)
         p.ve_discrtype = g("ve_discrtype", hp.VE_EXPLICIT)
+        p.alpha_gptt = g("alpha_gptt", 1.0)
+        p.beta_gptt = g("beta_gptt", 1.0)
         for b, face in enumerate(self.faces):
             for d, v in enumerate(face.get("uval", [0.0] * self.dim)):
                 p.bc_u[b][d] = v

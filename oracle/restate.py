@@ -40,12 +40,25 @@ def lib():
         L.hfr_divergence_rhs.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields), _D]
         L.hfr_cfl.argtypes = [C.POINTER(hp.HFProgram), C.POINTER(Fields)]
         L.hfr_cfl.restype = C.c_double
+        L.hfr_mittag_leffler.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _D]
+        L.hfr_mittag_leffler.restype = None
         _lib = L
     return _lib
 
 
 def available() -> bool:
     return os.path.exists(LIB)
+
+
+def mittag_leffler(alpha: float, beta: float, z, fi: int = 6) -> np.ndarray:
+    """The restated E_{alpha,beta} (hf_restate.c, ml_eval) at every point of z."""
+    zc = np.asarray(z, dtype=np.complex128)
+    out = np.empty(zc.shape, dtype=np.complex128)
+    r = (C.c_double * 2)()
+    for i, v in np.ndenumerate(zc):
+        lib().hfr_mittag_leffler(alpha, beta, v.real, v.imag, fi, r)
+        out[i] = complex(r[0], r[1])
+    return out
 
 
 class State:

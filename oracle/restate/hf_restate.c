@@ -867,8 +867,192 @@ static void du_stage(const hf_program *P, hfr_fields *F)
     }
 }
 
-/* explicit constitutive step (hig-flow-step-viscoelastic.c:352-544); the new
- * kernel goes to knew[] (the reference stores it in dpS, then copies) */
+/* ------------------------------------------------------------------ */
+/* Mittag-Leffler function E_{alpha,beta}(z), the GPTT model's         */
+/* generalised exponential (hig_flow_calculate_m_gptt,                 */
+/* hig-flow-step-viscoelastic.c:1771-1830, evaluated by mlfv,          */
+/* hig-flow-mittag-leffler.c:117-366).  The algorithm is the published */
+/* one of Gorenflo, Loutchko and Luchko (Fract. Calc. Appl. Anal. 5,   */
+/* 2002): the power series near the origin, the integral               */
+/* representation (a ray integral of K and an arc integral of P, each  */
+/* by a six-level Romberg rule) in the middle, the asymptotic series   */
+/* far out for alpha <= 1, and for alpha > 1 the reduction to smaller  */
+/* alpha (roots of z).  rho = 10^-fi is the accuracy the region bounds */
+/* and the Romberg order derive from (the reference passes fi = 6).    */
+/* Powers of z are taken in polar form, |z|^p e^{i p arg z}, as the    */
+/* reference does.  Only the real part enters the model; the imaginary */
+/* part of the asymptotic leading term is the true one here (the       */
+/* reference's sine there has the wrong sign, :287-288, :317-318,      */
+/* which never reaches a real part).                                   */
+/* ------------------------------------------------------------------ */
+typedef struct hfr_cx { double re, im; } hfr_cx;
+
+static hfr_cx cx_make(double re, double im) { hfr_cx z = {re, im}; return z; }
+static hfr_cx cx_polar(double r, double t) { return cx_make(r * cos(t), r * sin(t)); }
+static hfr_cx cx_add(hfr_cx a, hfr_cx b) { return cx_make(a.re + b.re, a.im + b.im); }
+static hfr_cx cx_scale(hfr_cx a, double s) { return cx_make(s * a.re, s * a.im); }
+static hfr_cx cx_div(hfr_cx a, hfr_cx b)
+{
+    const double d = b.re * b.re + b.im * b.im;
+    return cx_make((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d);
+}
+
+typedef struct ml_ctx { double a, b, eps; hfr_cx z; } ml_ctx;
+
+/* the ray integrand K(r) = r^((1-b)/a) e^(-r^(1/a)) / (pi a)
+ *   * (r sin(pi (1-b)) - z sin(pi (1-b+a))) / (r^2 - 2 r z cos(pi a) + z^2) */
+static hfr_cx ml_ray(const ml_ctx *c, double r)
+{
+    const double a = c->a, b = c->b;
+    const double A = pow(r, (1.0 - b) / a) * exp(-pow(r, 1.0 / a)) / (M_PI * a);
+    const double s1 = r * sin(M_PI * (1.0 - b)), s2 = sin(M_PI * (1.0 - b + a));
+    const double e = 2.0 * r * cos(M_PI * a);
+    const hfr_cx z = c->z;
+    const hfr_cx num = cx_make(s1 - s2 * z.re, -s2 * z.im);
+    const hfr_cx den = cx_make(r * r - e * z.re + (z.re * z.re - z.im * z.im), -e * z.im + 2.0 * z.re * z.im);
+    return cx_scale(cx_div(num, den), A);
+}
+
+/* the arc integrand P(phi) on |zeta| = eps:
+ *   eps^(1+(1-b)/a) e^(eps^(1/a) cos(phi/a)) e^(i w) / (2 pi a (eps e^(i phi) - z)),
+ *   w = eps^(1/a) sin(phi/a) + phi (1 + (1-b)/a) */
+static hfr_cx ml_arc(const ml_ctx *c, double phi)
+{
+    const double a = c->a, b = c->b, eps = c->eps;
+    const double p = 1.0 + (1.0 - b) / a, er = pow(eps, 1.0 / a);
+    const double A = pow(eps, p) * exp(er * cos(phi / a)) / (2.0 * M_PI * a);
+    const double w = er * sin(phi / a) + phi * p;
+    const hfr_cx den = cx_make(eps * cos(phi) - c->z.re, eps * sin(phi) - c->z.im);
+    return cx_div(cx_polar(A, w), den);
+}
+
+/* Romberg's rule with n levels (trapezoid sums of 1, 2, 4, ... panels,
+ * Richardson-extrapolated); the ray integral always takes six levels, the
+ * arc integral fi (rombint, hig-flow-mittag-leffler.c:53-56) */
+static hfr_cx ml_romberg(hfr_cx (*f)(const ml_ctx *, double), const ml_ctx *c, double lo, double hi, int n)
+{
+    if (f == ml_ray) n = 6;
+    if (n > 8) n = 8;   /* the reference's table holds eight levels (:46-50) */
+    if (n < 1) n = 1;
+    hfr_cx prev[16], cur[16];
+    double h = hi - lo;
+    const hfr_cx fa = f(c, lo), fb = f(c, hi);
+    prev[0] = cx_make(h * (fa.re + fb.re) / 2.0, h * (fa.im + fb.im) / 2.0);
+    int npts = 1;
+    for (int i = 1; i < n; i++) {
+        hfr_cx s = cx_make(0.0, 0.0);
+        for (int j = 1; j <= npts; j++) s = cx_add(s, f(c, lo + h * (j - 0.5)));
+        cur[0] = cx_make((prev[0].re + h * s.re) / 2.0, (prev[0].im + h * s.im) / 2.0);
+        double q = 1.0;
+        for (int k = 1; k <= i; k++) {
+            q *= 4.0;
+            cur[k] = cx_make((q * cur[k - 1].re - prev[k - 1].re) / (q - 1.0),
+                             (q * cur[k - 1].im - prev[k - 1].im) / (q - 1.0));
+        }
+        for (int k = 0; k <= i; k++) prev[k] = cur[k];
+        npts *= 2;
+        h /= 2.0;
+    }
+    return prev[n - 1];
+}
+
+/* z^((1-b)/a) e^(z^(1/a)) / a, the leading term of the integral and
+ * asymptotic forms */
+static hfr_cx ml_lead(double a, double b, double az, double th)
+{
+    const double ra = pow(az, 1.0 / a);
+    const double mag = (pow(az, (1.0 - b) / a) / a) * exp(ra * cos(th / a));
+    return cx_polar(mag, th * (1.0 - b) / a + ra * sin(th / a));
+}
+
+static hfr_cx ml_eval(double a, double b, hfr_cx z, int fi)
+{
+    const double az = sqrt(z.re * z.re + z.im * z.im);
+    const double th = atan2(z.im, z.re), ath = fabs(th);
+    const double rho = pow(10.0, -fi);
+    const int series = (a < 1.0 && az <= 1.0) ||
+                       (1.0 <= a && a < 2.0 && az <= floor(20.0 / pow(2.1 - a, 5.5 - 2.0 * a))) ||
+                       (a >= 2.0 && az <= 50.0);
+    if (series) {
+        /* sum z^k / Gamma(a k + b) from the first k with a k + b > 0, two
+         * terms at a time, until the sum stops changing */
+        int k = 0;
+        while (a * k + b <= 0.0) k++;
+        hfr_cx s = cx_make(pow(az, k) * cos(th * k) / tgamma(a * k + b), pow(az, k) * sin(th * k) / tgamma(a * k + b));
+        for (int it = 0; it < 100000; it++) {
+            const hfr_cx old = s;
+            for (int t = 0; t < 2; t++) {
+                k++;
+                const double g = tgamma(a * k + b), pk = pow(az, k);
+                s = cx_make(s.re + pk * cos(th * k) / g, s.im + pk * sin(th * k) / g);
+            }
+            if (s.re == old.re && s.im == old.im) break;
+        }
+        return s;
+    }
+    if (a <= 1.0 && az <= floor(5.0 * a + 10.0)) {
+        const double r0 = fmax(fmax(1.0, 2.0 * az), pow(-2.0 * log(rho * M_PI / 6.0), a));
+        ml_ctx c = {a, b, 0.0, z};
+        const double pa = M_PI * a;
+        if (ath > pa && fabs(ath - pa) > rho) {
+            if (b <= 1.0) return ml_romberg(ml_ray, &c, 0.0, r0, fi);
+            c.eps = 1.0;
+            return cx_add(ml_romberg(ml_ray, &c, c.eps, r0, fi), ml_romberg(ml_arc, &c, -pa, pa, fi));
+        }
+        if (ath < pa && fabs(ath - pa) > rho) {
+            if (b <= 1.0) return cx_add(ml_romberg(ml_ray, &c, 0.0, r0, fi), ml_lead(a, b, az, th));
+            c.eps = az / 2.0;
+            const hfr_cx arc = ml_romberg(ml_arc, &c, -pa, pa, fi);
+            return cx_add(cx_add(arc, ml_romberg(ml_ray, &c, c.eps, r0, fi)), ml_lead(a, b, az, th));
+        }
+        c.eps = az + 0.5;
+        return cx_add(ml_romberg(ml_ray, &c, c.eps, r0, fi), ml_romberg(ml_arc, &c, -pa, pa, fi));
+    }
+    if (a <= 1.0) {
+        /* asymptotic: the leading term inside the sector, minus
+         * sum_k z^-k / Gamma(b - a k) (terms with b - a k an integer skipped) */
+        hfr_cx s = cx_make(0.0, 0.0);
+        if (ath < (M_PI * a / 2.0 + fmin(M_PI, M_PI * a)) / 2.0) s = ml_lead(a, b, az, th);
+        for (int k = 1; k <= floor(fi / log10(az)); k++) {
+            const double g = b - a * k;
+            if (ceil(g) == floor(g)) continue;
+            const double pk = pow(az, -k);
+            s = cx_make(s.re - pk * cos(th * k) / tgamma(g), s.im - (-(pk * sin(th * k))) / tgamma(g));
+        }
+        return s;
+    }
+    if (a >= 2.0) {
+        /* E_{a,b}(z) = 1/(m+1) sum_h E_{a/(m+1),b}(z^(1/(m+1)) e^(2 pi i h/(m+1))) */
+        const int m = (int)floor(a / 2.0);
+        hfr_cx s = cx_make(0.0, 0.0);
+        for (int h = 0; h <= m; h++) {
+            const double r = pow(az, 1.0 / (m + 1.0));
+            s = cx_add(s, ml_eval(a / (m + 1), b, cx_polar(r, (2.0 * M_PI * h + th) / (m + 1.0)), fi));
+        }
+        return cx_scale(s, 1.0 / (m + 1.0));
+    }
+    /* 1 < a < 2: E_{a,b}(z) = (E_{a/2,b}(sqrt z) + E_{a/2,b}(-sqrt z)) / 2 */
+    const double r = sqrt(az);
+    const hfr_cx z1 = cx_make(r * cos(th / 2.0), r * sin(th / 2.0));
+    const hfr_cx e1 = ml_eval(a / 2.0, b, z1, fi), e2 = ml_eval(a / 2.0, b, cx_make(-z1.re, -z1.im), fi);
+    return cx_make((e1.re + e2.re) / 2.0, (e1.im + e2.im) / 2.0);
+}
+
+/* the GPTT factor Gamma(beta_g) E_{alpha_g,beta_g}(eps Re De tr(S) / (1 - beta)) */
+static double gptt_factor(const hf_params *pr, double trS)
+{
+    const hfr_cx z = cx_make(pr->epsilon * pr->Re * pr->De * trS / (1.0 - pr->beta), 0.0);
+    return ml_eval(pr->alpha_gptt, pr->beta_gptt, z, 6).re;
+}
+
+/* the evaluation alone, for the tests of the device form */
+void hfr_mittag_leffler(double alpha, double beta, double zr, double zi, int fi, double *out)
+{
+    const hfr_cx e = ml_eval(alpha, beta, cx_make(zr, zi), fi);
+    out[0] = e.re;
+    out[1] = e.im;
+}
+
 /* implicit Euler constitutive step of one cell (higflow_implicit_euler_
  * constitutive_equation, hig-flow-step-viscoelastic.c:841-877): right-hand
  * side for every (i, j), the Kronecker system of hig_flow_kernel_system_matrix
@@ -949,6 +1133,8 @@ static void implicit_cell(const hf_program *P, hfr_fields *F, const hf_params *p
         }
 }
 
+/* explicit constitutive step (hig-flow-step-viscoelastic.c:352-544); the new
+ * kernel goes to knew[] (the reference stores it in dpS, then copies) */
 static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew)
 {
     const int D = P->par.dim, n = P->ncell;
@@ -976,7 +1162,7 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
         for (int i = 0; i < D; i++)
             for (int j = 0; j < D; j++) {
                 Mt[i][j] = Du[i][j];
-                if (pr->ve_model == HF_LPTT) Mt[i][j] -= pr->xi * 0.5 * (Du[i][j] + Du[j][i]);
+                if (pr->ve_model == HF_LPTT || pr->ve_model == HF_GPTT) Mt[i][j] -= pr->xi * 0.5 * (Du[i][j] + Du[j][i]);
             }
         mprod(D, Mt, R, M);
         /* hig_flow_calculate_omega (:1667) */
@@ -1008,6 +1194,8 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
             const double b = pr->L2_fene, lf = pr->lambda_fene, E = pr->E_fene;
             fA = b / (b - trA) - E * sqrt(b) * exp(-sqrt(trA) / lf) * (1.0 / (trA * lf) + 1 / (trA * sqrt(trA)));
         }
+        /* GPTT (:1771-1830): Gamma(beta_g) E_{alpha_g,beta_g}(eps Re De tr S / (1 - beta)) */
+        const double mlv = pr->ve_model == HF_GPTT ? gptt_factor(pr, trS) : 0.0;
         for (int i = 0; i < D; i++) {
             for (int j = i + 1; j < D; j++) { Ma[i][j] = 0.0; Ma[j][i] = 0.0; }
             if (pr->ve_model == HF_GIESEKUS) {
@@ -1015,6 +1203,8 @@ static void constitutive_stage(const hf_program *P, hfr_fields *F, double **knew
                 Ma[i][i] = (aux - pr->alpha * aux * aux) * jl[i];
             } else if (pr->ve_model == HF_LPTT) {
                 Ma[i][i] = (1.0 - lam[i]) * (1.0 + (pr->epsilon * Re * De * trS) / (1.0 - pr->beta)) * jl[i];
+            } else if (pr->ve_model == HF_GPTT) {
+                Ma[i][i] = (1.0 - lam[i]) * pr->gamma_gptt * mlv * jl[i];
             } else if (pr->ve_model == HF_E_FENE) {
                 Ma[i][i] = (1.0 - fA * lam[i]) * jl[i];
             } else {
@@ -1103,10 +1293,10 @@ static void polymeric_stage(const hf_program *P, hfr_fields *F)
             B[i][i] = kinv(pr->kernel, lam[i]);
         }
         mtprod(D, B, R, A);
-        /* the model switch of :274-309: LPTT sets xi; e-FENE computes its fA
+        /* the model switch of :274-309: LPTT and GPTT set xi; e-FENE computes its fA
          * there but falls through to the default (fA = a = 1, xi = 0) */
         double fA = 1.0, a = 1.0, xi = 0.0;
-        if (pr->ve_model == HF_LPTT) xi = pr->xi;
+        if (pr->ve_model == HF_LPTT || pr->ve_model == HF_GPTT) xi = pr->xi;
         for (int i = 0; i < D; i++) {
             for (int j = 0; j < D; j++)
                 F->S[i * D + j][cc] = (1.0 - beta) * (fA * A[i][j]) / (Re * De * (1.0 - xi)) - (1.0 - beta) * Du[i][j] / Re;

@@ -89,6 +89,16 @@ CASES = {
     "cn2d_oldroyd_log": (lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC,
                                               ve_model=hp.OLDROYD_B, kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                               tempdiscrtype=hp.SEMI_IMPLICIT_CN), 3, (0.3, 0.1, 0.2)),
+    # GPTT: Gamma(beta_g) E_{alpha_g,beta_g}(eps Re De tr S / (1 - beta)) in M;
+    # the first steps' tr S reaches both sides of the Mittag-Leffler series /
+    # integral boundary (|z| up to 1.5 and 3), beta_g > 1 takes the arc integral
+    "gptt2d_log": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GPTT,
+                                        kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, epsilon=0.15, xi=0.1,
+                                        alpha_gptt=0.5, beta_gptt=1.0), 3, (0.3, 0.1, 0.2)),
+    "gptt2d_b12_implicit": (lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GPTT,
+                                                 kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, epsilon=0.3, xi=0.1,
+                                                 alpha_gptt=0.8, beta_gptt=1.2, ve_discrtype=hp.VE_IMPLICIT),
+                            3, (0.3, 0.1, 0.2)),
     # semi-implicit BDF2 (two solves per direction: into uaux, then into u*)
     "bdf2_cav2d": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
                    4, (0.3, 0.1, 0.0)),

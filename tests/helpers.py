@@ -36,6 +36,15 @@ def load_init(target, prog: hp.Program, data: dict) -> None:
         target.set(fid, comp, data["init_" + key])
 
 
+# Mittag-Leffler parameters and points reaching every region of the
+# evaluation: series near 0, the integral form's three sectors with beta <= 1
+# and > 1, the asymptotic series, and the reductions for alpha >= 1
+ML_ALPHAS = (0.3, 0.5, 0.8, 1.0, 1.3, 1.7, 2.0, 2.5, 3.7, 4.6)
+ML_BETAS = (0.4, 1.0, 1.5, 2.2)
+ML_POINTS = tuple(complex(x) for x in (-80, -30, -12, -5, -2.5, -1.0, -0.3, 0.0, 0.4, 1.0, 1.7, 3.0, 6.0, 9.0,
+                                      14.0, 20.0, 40.0, 70.0)) + (3 + 4j, -2 + 1j, 0.5 - 0.7j, -9 - 9j, 12j)
+
+
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     na = np.linalg.norm(a)
     return float(np.linalg.norm(a - b) / (na if na > 0 else 1.0))

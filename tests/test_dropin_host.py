@@ -13,11 +13,11 @@ refpy = pytest.importorskip("oracle.refpy")
 def test_attach_refuses_an_unsupported_model_without_a_gpu():
     if not refpy.available(2):
         pytest.skip("oracle build of the reference not present")
-    gptt = 3   # visc_model_type GPTT (hig-flow-kernel.h:300): not on the GPU path
-    case = refpy.RefCase(refpy.cavity(2, 8, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=gptt))
+    # FENE-P (visc_model_type 4, hig-flow-kernel.h:301): not on the GPU path
+    case = refpy.RefCase(refpy.cavity(2, 8, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.FENE_P))
     L = case.L
     assert L.hf_attach(case.ns, None) == -2   # HF_ERR_UNSUPPORTED
-    assert b"viscoelastic model" in L.hfref_flatten_error()
+    assert b"FENE-P" in L.hfref_flatten_error()
     assert L.hf_step(case.ns) == -2            # stepping attaches first, and refuses the same way
     assert L.hf_sync_to_host(case.ns) == -1    # never attached
     case.close()

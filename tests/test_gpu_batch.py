@@ -14,7 +14,9 @@ from tests.helpers import compare, field_keys, load_golden, load_init
 
 pytestmark = pytest.mark.gpu
 
-VE_NAMES = ["ve2d_oldroyd_log", "ve2d_giesekus_log", "ve2d_lptt_sqrt", "ve2d_oldroyd_central"]
+# the models differ per instance (Oldroyd-B, Giesekus, LPTT, GPTT, e-FENE)
+VE_NAMES = ["ve2d_oldroyd_log", "ve2d_giesekus_log", "ve2d_lptt_sqrt", "ve2d_oldroyd_central", "gptt2d_log",
+            "efene2d_log"]
 NEWT_NAMES = ["cav2d_cubista", "cav2d_quick", "cav2d_central", "chan2d_cubista", "cav2d_lid"]
 
 

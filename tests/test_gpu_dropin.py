@@ -35,6 +35,10 @@ CASES = {
     "oldroyd_sie": lambda: refpy.cavity(2, 12, Re=0.01, dt=1e-3, flowtype=hp.VISCOELASTIC, ve_model=hp.OLDROYD_B,
                                         kernel=hp.KERNEL_LOG, beta=1.0 / 9.0,
                                         tempdiscrtype=hp.SEMI_IMPLICIT_EULER),
+    # GPTT (the Mittag-Leffler factor; gamma_gptt from the flattener's tgamma)
+    "gptt_log": lambda: refpy.cavity(2, 12, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GPTT,
+                                     kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, epsilon=0.3, xi=0.1,
+                                     alpha_gptt=0.8, beta_gptt=1.2),
     # semi-implicit BDF2 (two solves per direction)
     "newtonian_bdf2": lambda: refpy.cavity(2, 12, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
 }

@@ -11,7 +11,8 @@ import pytest
 from higflow_b200 import engine
 from higflow_b200 import program as hp
 from oracle import restate
-from tests.helpers import compare, field_keys, golden_names, load_golden, load_init
+from tests.helpers import (ML_ALPHAS, ML_BETAS, ML_POINTS, compare, field_keys, golden_names, load_golden,
+                           load_init)
 
 pytestmark = pytest.mark.gpu
 
@@ -271,3 +272,64 @@ def test_adaptive_timestep_refused_for_semi_implicit():
     with pytest.raises(engine.EngineError):
         case.adjust_timestep()
     case.close()
+
+
+def _ml_series_region(a, az):
+    """The region where the evaluation sums the power series (the same bounds
+    as hf::mittag_leffler and the reference's mlfv)."""
+    return (a < 1 and az <= 1) or (1 <= a < 2 and az <= np.floor(20 / (2.1 - a) ** (5.5 - 2 * a))) or \
+        (a >= 2 and az <= 50)
+
+
+def _ml_scale(a, b, z):
+    """Rounding scale of the evaluation at z: in the power-series region the
+    sum of the terms' moduli, E_{a,b}(|z|); in the integral and asymptotic
+    forms |E(z)|; through the reductions for a > 1 the mean over the reduced
+    points, as the value itself is formed."""
+    az = abs(z)
+    if _ml_series_region(a, az):
+        return abs(restate.mittag_leffler(a, b, [az])[0])
+    if a <= 1:
+        return abs(restate.mittag_leffler(a, b, [z])[0])
+    th = np.angle(z)
+    if a >= 2:
+        m = int(np.floor(a / 2))
+        pts = [az ** (1 / (m + 1)) * np.exp(1j * (2 * np.pi * h + th) / (m + 1)) for h in range(m + 1)]
+        return float(np.mean([_ml_scale(a / (m + 1), b, p) for p in pts]))
+    r = np.sqrt(az) * np.exp(1j * th / 2)
+    return 0.5 * (_ml_scale(a / 2, b, r) + _ml_scale(a / 2, b, -r))
+
+
+def test_mittag_leffler_device_matches_restatement():
+    """hf_mittag_leffler (the GPTT model's E_{alpha,beta}, hf::mittag_leffler) on
+    the GPU against the restatement over every region of the evaluation: real
+    and imaginary parts to 1e-12 of the evaluation's rounding scale (CUDA's and
+    the host's libm differ in the last bits), infinities where the restatement
+    overflows.  The scale is |E|, and in the power-series region (also where
+    the reductions for alpha > 1 land in it) the sum of the terms' moduli,
+    E_{alpha,beta}(|z|): for z off the positive axis the series cancels terms
+    up to that size (E_{1,0.4}(-12) = -0.027 from terms near 1e5), so the last
+    bits of each term set the result's accuracy there, the reference's too."""
+    pts = np.array(ML_POINTS)
+    nfinite = 0
+    for a in ML_ALPHAS:
+        for b in ML_BETAS:
+            got = engine.mittag_leffler(a, b, pts)
+            want = restate.mittag_leffler(a, b, pts)
+            for z, g, w in zip(ML_POINTS, got, want):
+                if not np.isfinite(w.real):
+                    assert np.isinf(g.real) and np.sign(g.real) == np.sign(w.real), (a, b, z, g, w)
+                    continue
+                scale = max(abs(w), _ml_scale(a, b, z))
+                assert abs(g.real - w.real) <= 1e-12 * scale and abs(g.imag - w.imag) <= 1e-12 * scale, (a, b, z, g, w)
+                nfinite += 1
+    assert nfinite > 800
+
+
+def test_mittag_leffler_rejects_out_of_range_arguments():
+    with pytest.raises(engine.EngineError) as e:
+        engine.mittag_leffler(6.0, 1.0, [1.0])
+    assert e.value.code == -1
+    with pytest.raises(engine.EngineError):
+        engine.mittag_leffler(0.5, 1.0, [1.0], fi=0)
+    assert engine.mittag_leffler(0.5, 1.0, np.zeros(0)).size == 0

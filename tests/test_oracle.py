@@ -9,7 +9,8 @@ import pytest
 
 from higflow_b200 import program as hp
 from oracle import restate
-from tests.helpers import compare, field_keys, golden_names, load_golden, load_init
+from tests.helpers import (ML_ALPHAS, ML_BETAS, ML_POINTS, compare, field_keys, golden_names, load_golden,
+                           load_init)
 
 NAMES = golden_names()
 
@@ -181,6 +182,43 @@ def test_cfl_matches_reference(dim, ve):
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not present")
+@pytest.mark.skipif(not HAVE_REF, reason="oracle build of the reference not present")
+def test_mittag_leffler_restatement_matches_reference():
+    """E_{alpha,beta}(z) of the restatement (hf_restate.c, ml_eval) against the
+    reference's own mlfv (hig-flow-mittag-leffler.c:117) over every region of
+    the evaluation, fi = 6 as the GPTT model passes: real parts to 1e-13
+    relative, overflow to inf on both sides together.  (Imaginary parts are
+    not compared: the reference's asymptotic leading term has the sign of its
+    sine wrong, which never reaches a real part.)"""
+    pts = np.array(ML_POINTS)
+    n_region = {"finite": 0, "inf": 0}
+    for a in ML_ALPHAS:
+        for b in ML_BETAS:
+            mine = restate.mittag_leffler(a, b, pts)
+            for z, m in zip(ML_POINTS, mine):
+                r = refpy.mlfv(a, b, z)
+                if not np.isfinite(r.real):
+                    assert m.real == r.real, (a, b, z, r, m)
+                    n_region["inf"] += 1
+                    continue
+                assert abs(m.real - r.real) <= 1e-13 * abs(r.real), (a, b, z, r, m)
+                n_region["finite"] += 1
+    assert n_region["finite"] > 800
+
+
+def test_gptt_out_of_range_parameters_are_refused():
+    """GPTT with alpha_gptt outside (0, 5] (the range the reference's
+    Mittag-Leffler evaluation accepts) is refused at flatten with the reason."""
+    if not HAVE_REF:
+        pytest.skip("oracle build of the reference not present")
+    c = refpy.RefCase(refpy.cavity(2, 8, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GPTT,
+                                   kernel=hp.KERNEL_LOG, alpha_gptt=6.0, beta_gptt=1.0))
+    with pytest.raises(Exception) as e:
+        c.flatten()
+    assert "alpha_gptt" in str(e.value)
+    c.close()
+
+
 def test_fene_p_is_refused_with_its_reason():
     """FENE-P stays off the GPU path: the reference's polymeric tensor reads xi
     without assigning it for this model, so there is no defined stress to match."""
