@@ -99,6 +99,12 @@ CASES = {
                                                  kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, epsilon=0.3, xi=0.1,
                                                  alpha_gptt=0.8, beta_gptt=1.2, ve_discrtype=hp.VE_IMPLICIT),
                             3, (0.3, 0.1, 0.2)),
+    # the same in 3D (D = 3 forms of the GPTT cell kernel and of BDF2)
+    "gptt3d_log": (lambda: refpy.cavity(3, 5, Re=1.0, dt=1e-4, flowtype=hp.VISCOELASTIC, ve_model=hp.GPTT,
+                                        kernel=hp.KERNEL_LOG, beta=1.0 / 9.0, De=0.5, epsilon=0.3, xi=0.1,
+                                        alpha_gptt=0.8, beta_gptt=1.2), 3, (0.3, 0.1, 0.2)),
+    "bdf2_cav3d": (lambda: refpy.cavity(3, 6, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
+                   3, (0.3, 0.1, 0.0)),
     # semi-implicit BDF2 (two solves per direction: into uaux, then into u*)
     "bdf2_cav2d": (lambda: refpy.cavity(2, 16, Re=0.1, dt=1e-3, tempdiscrtype=hp.SEMI_IMPLICIT_BDF2),
                    4, (0.3, 0.1, 0.0)),
