@@ -395,7 +395,6 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
     const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
     const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
-    const double a = 1.7500, b = 0.3750, c = 0.7500, dd = 0.1250, ee = 0.2500;
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
     double conv1 = 0.0, conv2 = 0.0;
