@@ -38,8 +38,8 @@ WORKLOADS = {
     "c4": dict(
         name="batched 2D Giesekus lid-driven cavities: 256 instances, side N log-uniform in [32,256] "
              "(seed 0), Wi uniform [0.1,2.0], alpha uniform [0,0.5], beta 0.1, Re 1, log-conformation "
-             "kernel from identity, explicit Euler at 0.2x the explicit bound, CUBISTA, AMG-CG Poisson "
-             "to 1e-10; one batch program, one CUDA graph launch per step",
+             "kernel from identity, explicit Euler at 0.2x the explicit bound, CUBISTA, AMG-CG Poisson; "
+             "programs recorded by HigTree (bit-exact stencils); one batch, one CUDA graph launch per step",
         batch="c4", precision="mixed", dim=2,
     ),
     "c4_64": dict(
@@ -50,41 +50,33 @@ WORKLOADS = {
     "c1": dict(
         name="2D Newtonian lid-driven cavity 64x64 (uniform quadtree, unit square), Re=100, lid u=1, "
              "explicit Euler dt=1e-4, CUBISTA, incremental projection, Poisson CG to 1e-10 relative residual, "
-             "zero initial fields",
-        program="c1_cavity2d_64.prog.npz", dim=2, n=64, Re=100.0, dt=1e-4, precision="fp64",
+             "zero initial fields; program recorded by HigTree",
+        dim=2, n=64, Re=100.0, dt=1e-4, precision="fp64",
     ),
-    "cav3d_128": dict(
-        name="3D Newtonian lid-driven cavity 128^3 (uniform octree, unit cube), Re=400, lid u=1, explicit "
-             "Euler dt=1e-4, CUBISTA, incremental projection, AMG-CG Poisson to 1e-10 relative residual with "
-             "the V-cycle in FP32 (FP64 CG), zero initial fields; program tiled from the recorded 16^3 seed",
-        tiled=True, dim=3, n=128, Re=400.0, dt=1e-4, precision="mixed",
-    ),
-    "cav2d_1024": dict(
-        name="2D Newtonian lid-driven cavity 1024x1024 (uniform quadtree, unit square), Re=100, lid u=1, "
-             "explicit Euler dt=1e-5, CUBISTA, incremental projection, Poisson CG to 1e-10 relative residual, "
-             "zero initial fields; program tiled from the recorded 18x18 seed",
-        tiled=True, dim=2, n=1024, Re=100.0, dt=1e-5, precision="fp64",
+    "c3_48": dict(
+        name="3D Newtonian lid-driven cavity 48^3 (uniform octree, unit cube), Re=400, lid u=1, explicit "
+             "Euler dt=1e-4, CUBISTA, incremental projection, AMG-CG Poisson, zero initial fields; program "
+             "recorded by HigTree (the configured 128^3 needs about 3 hours of host stencil recording and "
+             "24 GB of stencils, so this line runs the largest cube recorded in about a minute)",
+        dim=3, n=48, Re=400.0, dt=1e-4, precision="mixed",
     ),
 }
 
 
-def rank_seed(rank):
-    """Seed of rank r's batch: every GPU draws its own population (shards of
-    independent instances, the per-GPU work fixed as the GPU count grows)."""
-    return rank
+def shard(draws, rank, world):
+    """This rank's instances of one population: greedy longest-processing-time
+    partition by cost N^2 x steps (each instance to the least-loaded rank, the
+    largest first); every instance lands on exactly one rank."""
+    from higflow_b200 import workloads
+    return [draws[i] for i in workloads.partition([d.cells * d.steps for d in draws], world)[rank]]
 
 
-def load_program(wl, rank=0):
-    from higflow_b200 import program as hp
-    from higflow_b200 import tiling, workloads
+def load_program(wl, rank=0, world=1):
+    from higflow_b200 import host, workloads
     if wl.get("batch") == "c4":
-        return workloads.batch(workloads.batched_giesekus(seed=rank_seed(rank))[:wl.get("count", 256)])
-    if wl.get("tiled"):
-        prog = tiling.cavity(wl["dim"], wl["n"])
-    else:
-        prog = hp.Program.load(os.path.join(REPO, "higflow_b200", "seeds", wl["program"]))
-    prog.par["Re"], prog.par["dt"] = wl["Re"], wl["dt"]
-    return prog
+        draws = workloads.batched_giesekus()[:wl.get("count", 256)]
+        return workloads.batch(shard(draws, rank, world))
+    return host.record(host.cavity(wl["dim"], wl["n"], Re=wl["Re"], dt=wl["dt"]))
 
 
 # ---------------------------------------------------------------------------
@@ -277,7 +269,7 @@ def run_b200(args, rank, world, device):
 
     wl = WORKLOADS[args.workload]
     t0 = time.perf_counter()
-    prog = load_program(wl, rank)
+    prog = load_program(wl, rank, world)
     t_program = time.perf_counter() - t0
     mixed = wl["precision"] == "mixed"
     prec = hp.PREC_MIXED if mixed else hp.PREC_FP64
@@ -375,7 +367,7 @@ def run_b200(args, rank, world, device):
                    "poisson": f"{sinfo['method']}, rtol 1e-10 on ||b - A x|| per instance",
                    "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write, outside the step events)",
                    "parallelism": f"replicas x{world}",
-                   "program": "tiled from recorded seeds" if (wl.get("tiled") or wl.get("batch")) else "recorded from the reference"},
+                   "program": "recorded by the HigFlow host (HigTree's own stencils, ids and weights)"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "bytes_per_launch": pb[dom] / dom_launch, "launch_us": per_launch_s * 1e6,
@@ -587,7 +579,7 @@ def main():
                                 device_id=torch.device(f"cuda:{local}"))
     line = run_b200(args, rank, world, local)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline and not WORKLOADS[args.workload].get("tiled"):
+        if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(WORKLOADS[args.workload])
         print(json.dumps(line))
     if world > 1:

@@ -110,6 +110,48 @@ static int copy_fields(hf_binding *b, const int (*list)[2], int nlist, int to_de
     return rc;
 }
 
+/* The source fields (cell F and facet FU[d]) as the reference computes them
+ * at time t, appended to out (grown as needed). */
+static int sources_at(higflow_solver *ns, real t, double **out, size_t *len)
+{
+    const real t0 = ns->par.t;
+    ns->par.t = t;
+    higflow_calculate_source_term(ns);
+    higflow_calculate_facet_source_term(ns);
+    ns->par.t = t0;
+    size_t n = 0;
+    for (int f = 0; f <= DIM; f++) n += f == 0 ? field_len(ns, HF_FIELD_F, 0) : field_len(ns, HF_FIELD_FU, f - 1);
+    double *v = realloc(*out, sizeof(double) * (n ? n : 1));
+    if (!v) return HF_ERR_INVALID;
+    *out = v;
+    *len = n;
+    size_t at = 0;
+    for (int f = 0; f <= DIM; f++) {
+        distributed_property *dp = f == 0 ? ns->dpF : ns->dpFU[f - 1];
+        const int m = f == 0 ? field_len(ns, HF_FIELD_F, 0) : field_len(ns, HF_FIELD_FU, f - 1);
+        for (int k = 0; k < m; k++) v[at++] = dp_get_value(dp, k);
+    }
+    return HF_OK;
+}
+
+/* Refuse source callbacks that depend on time: the sources are evaluated at
+ * the case's current time and at two later times (a step and a long span
+ * ahead) and must agree bit for bit. */
+static int check_sources_fixed(higflow_solver *ns)
+{
+    double *a = NULL, *b = NULL;
+    size_t na = 0, nb = 0;
+    const real t = ns->par.t, later[2] = {t + ns->par.dt, t + 1000.0 * ns->par.dt + 1.0};
+    int rc = sources_at(ns, t, &a, &na);
+    for (int k = 0; k < 2 && rc == HF_OK; k++) {
+        rc = sources_at(ns, later[k], &b, &nb);
+        if (rc == HF_OK && (nb != na || memcmp(a, b, sizeof(double) * na) != 0)) rc = HF_ERR_UNSUPPORTED;
+    }
+    free(a);
+    free(b);
+    return rc;
+}
+
 int hf_attach(higflow_solver *ns, const hf_options *opt)
 {
     if (!ns) return HF_ERR_INVALID;
@@ -119,6 +161,13 @@ int hf_attach(higflow_solver *ns, const hf_options *opt)
     hf_program *prog = NULL;
     int rc = hf_flatten(ns, &prog);
     if (rc) return rc;
+    /* the GPU path keeps the source terms fixed (see below): refuse source
+     * callbacks that depend on t before any device work */
+    rc = check_sources_fixed(ns);
+    if (rc) {
+        hf_program_free(prog);
+        return rc;
+    }
     hf_case *c = NULL;
     rc = hf_case_create(prog, opt, &c);
     hf_program_free(prog);   /* the engine keeps its own copy */
@@ -127,8 +176,9 @@ int hf_attach(higflow_solver *ns, const hf_options *opt)
     b->c = c;
     b->ve = ns->contr.flowtype == VISCOELASTIC;
     /* the source terms as the reference's step evaluates them before the
-     * velocity stage (hig-flow-step.c:343-606); they are time-independent on
-     * the GPU path (hf_flatten refuses time-dependent boundary data) */
+     * velocity stage (hig-flow-step.c:343-606, at ns->par.t, :359); fixed on
+     * the GPU path (time-dependent sources were refused above, time-dependent
+     * boundary data by hf_flatten) */
     higflow_calculate_source_term(ns);
     higflow_calculate_facet_source_term(ns);
     rc = copy_fields(b, k_in, (int)(sizeof k_in / sizeof k_in[0]), 1);
@@ -172,6 +222,10 @@ int hf_sync_to_device(higflow_solver *ns)
 {
     hf_binding *b = find(ns);
     if (!b) return HF_ERR_INVALID;
+    /* the time step too: a restart or a host edit may have changed it */
+    const double dt = ns->par.dt;
+    int rc = hf_case_set_timestep(b->c, &dt, 1);
+    if (rc) return rc;
     return copy_fields(b, k_in, (int)(sizeof k_in / sizeof k_in[0]), 1);
 }
 

@@ -86,12 +86,16 @@ struct DevProg {
     const uint8_t *vtag;
     int nvrows;
     double *rowval;
-    // the same pairs for k_vrows: per pair ((first entry << vlenbits) | count,
-    // base), and the template entries packed as (weight, column) in 16 bytes;
-    // vdesc is null when a program's templates do not fit the packing
-    const uint2 *vdesc;
-    const int4 *vent;
-    int vlenbits;
+    // the same pairs for k_vrows in a sliced layout (SELL-32): pair u is lane
+    // u % 32 of slice u / 32, and its entry k sits at sptr[u / 32] + 32 k +
+    // u % 32, so a warp's k-th entries are one coalesced load; the column is
+    // absolute (row base added), plen[u] is the pair's entry count.  The
+    // weights are FP64 (plain) or FP32 (mixed: sw32, FP32 accumulation).
+    const int64_t *sptr;
+    const uint8_t *plen;
+    const int32_t *scol;
+    const double *sw;
+    const float *sw32;
     // semi-implicit Euler: the velocity kernel writes each direction's
     // right-hand side, u + dt (sources - grad p [+ div S] - conv) plus the
     // system's boundary part sie_bc, into sie_b instead of u*
@@ -269,30 +273,30 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
     }
 }
 
-// The general rows the velocity stage reads, one thread per row: the long
-// interpolation stencils (tens of entries) run here, coalesced and without
-// divergence, instead of inside the per-facet kernel.
-// Each entry is one 16-byte load of (weight, column) and one gather; the sum
-// is hf::query's: -rhs, then the entries in template order.
+// The general rows the velocity stage reads, one thread per (row, field)
+// pair: the long interpolation stencils (tens of entries) run here, coalesced
+// and without divergence, instead of inside the per-facet kernel.  Entry k of
+// the 32 pairs of a warp is one 128-byte column load and one 256-byte (FP64)
+// or 128-byte (FP32) weight load; the sum is dp_interpolate_from_stencil's
+// (pdomain.c:1026-1053): -rhs, then the entries in stencil order.  W = float
+// is the mixed form: FP32 weights and field values, FP32 accumulation.
+template <typename W>
 __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= P.nvrows) return;
-    if (!P.vdesc) {
-        P.rowval[u] = hf::query(P.vrow, -u - 1, vtag_field(F, __ldg(P.vtag + u)));
-        return;
-    }
-    const uint2 d = __ldg(P.vdesc + u);
-    const double *__restrict__ fb = vtag_field(F, __ldg(P.vtag + u)) + d.y;
-    double res = 0.0;
-    res += -__ldg(P.vrow.rhs + u);
-    const int k0 = (int)(d.x >> P.vlenbits), e = k0 + (int)(d.x & ((1u << P.vlenbits) - 1));
+    const double *__restrict__ fb = vtag_field(F, __ldg(P.vtag + u));
+    const int n = __ldg(P.plen + u);
+    const int64_t e0 = __ldg(P.sptr + (u >> 5)) + (u & 31);
+    const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)P.sw32 : (const W *)P.sw;
+    W res = (W)0;
+    res += -(W)__ldg(P.vrow.rhs + u);
 #pragma unroll 4
-    for (int k = k0; k < e; k++) {
-        const int4 t = __ldg(P.vent + k);
-        res += __ldg(fb + t.z) * __hiloint2double(t.y, t.x);
+    for (int k = 0; k < n; k++) {
+        const int64_t at = e0 + 32 * (int64_t)k;
+        res += (W)__ldg(fb + __ldg(P.scol + at)) * __ldg(w + at);
     }
-    P.rowval[u] = res;
+    P.rowval[u] = (double)res;
 }
 
 // CUBISTA convective flux of the facet velocity along one direction
@@ -1272,6 +1276,7 @@ struct hf_case {
     cudaGraph_t graph[2] = {};
     cudaGraphExec_t exec[2] = {};
     int64_t ntemplates = 0;         // row templates of the finest Poisson operator
+    int64_t vel_entries = 0;        // stored entries of the velocity-stage rows (padded slices)
     bool graph_profile = false;     // graphs were captured with phase events
     bool phase_pending = false;     // a profiled step's events are not read yet
     bool capturing = false;         // a step graph is being captured
@@ -2194,7 +2199,8 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     int n = 0;
     if (C->P.nvrows) {
-        k_vrows<<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
+        if (C->P.sw32) k_vrows<float><<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
+        else k_vrows<double><<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
         n++;
     }
     if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
@@ -2748,28 +2754,48 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             UP((uint16_t **)&P.vdelta[d], pg->vel_delta[d], pg->nfacet[d]);
         }
         P.nvrows = (int)ptmpl.size();
-        // the packed form: the count field is as wide as the longest template
-        // needs, the rest of the word holds the first entry
-        int64_t maxlen = 0;
-        for (int64_t t = 0; t < pg->ntmpl; t++) maxlen = std::max(maxlen, pg->tmpl_ptr[t + 1] - pg->tmpl_ptr[t]);
-        int lb = 1;
-        while (((int64_t)1 << lb) <= maxlen) lb++;
-        P.vlenbits = lb;
-        if (!ptmpl.empty() && lb < 32 && pg->nnz < ((int64_t)1 << (32 - lb))) {
-            std::vector<uint2> vdesc(ptmpl.size());
-            for (size_t u = 0; u < ptmpl.size(); u++) {
-                const int64_t a = pg->tmpl_ptr[ptmpl[u]], len = pg->tmpl_ptr[ptmpl[u] + 1] - a;
-                vdesc[u] = make_uint2(((uint32_t)a << lb) | (uint32_t)len, (uint32_t)pbase[u]);
+        {
+            // sliced layout (see DevProg): a slice holds 32 consecutive pairs,
+            // padded to its longest; consecutive pairs are consecutive elements
+            // of one slot, so lengths within a slice rarely differ
+            const size_t np = ptmpl.size(), nsl = (np + 31) / 32;
+            std::vector<int64_t> sptr(nsl + 1, 0);
+            std::vector<uint8_t> plen(np);
+            for (size_t sl = 0; sl < nsl; sl++) {
+                int64_t mx = 0;
+                for (size_t u = sl * 32; u < std::min(np, sl * 32 + 32); u++) {
+                    const int64_t len = pg->tmpl_ptr[ptmpl[u] + 1] - pg->tmpl_ptr[ptmpl[u]];
+                    if (len > 255) return cleanup(fail(HF_ERR_UNSUPPORTED, "velocity-stage stencil longer than 255 entries"));
+                    plen[u] = (uint8_t)len;
+                    mx = std::max(mx, len);
+                }
+                sptr[sl + 1] = sptr[sl] + 32 * mx;
             }
-            UP((uint2 **)&P.vdesc, vdesc.data(), vdesc.size());
-            std::vector<int4> vent((size_t)pg->nnz);
-            for (int64_t k = 0; k < pg->nnz; k++) {
-                const double w = pg->tmpl_w[k];
-                int64_t bits;
-                memcpy(&bits, &w, sizeof bits);
-                vent[k] = make_int4((int)(uint32_t)(bits & 0xffffffff), (int)(uint32_t)((uint64_t)bits >> 32), pg->tmpl_col[k], 0);
+            const size_t ne = (size_t)sptr[nsl];
+            std::vector<int32_t> scol(ne, 0);
+            std::vector<double> sw;
+            std::vector<float> sw32;
+            if (opt.precision == HF_PREC_MIXED) sw32.assign(ne, 0.f);
+            else sw.assign(ne, 0.0);
+            for (size_t u = 0; u < np; u++) {
+                const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
+                int64_t at = sptr[u / 32] + (int64_t)(u % 32);
+                for (int k = 0; k < plen[u]; k++, at += 32) {
+                    const int64_t c = (int64_t)pbase[u] + pg->tmpl_col[a0 + k];
+                    if (c < 0 || c > INT32_MAX) return cleanup(fail(HF_ERR_INVALID, "velocity-stage column out of range"));
+                    scol[at] = (int32_t)c;
+                    if (opt.precision == HF_PREC_MIXED) sw32[at] = (float)pg->tmpl_w[a0 + k];
+                    else sw[at] = pg->tmpl_w[a0 + k];
+                }
             }
-            UP((int4 **)&P.vent, vent.data(), vent.size());
+            UP((int64_t **)&P.sptr, sptr.data(), sptr.size());
+            UP((uint8_t **)&P.plen, plen.data(), plen.size());
+            UP((int32_t **)&P.scol, scol.data(), scol.size());
+            if (opt.precision == HF_PREC_MIXED) UP((float **)&P.sw32, sw32.data(), sw32.size());
+            else UP((double **)&P.sw, sw.data(), sw.size());
+            C->vel_entries = (int64_t)ne;
+            // wait for the uploads before the host staging vectors go away
+            if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "velocity rows"));
         }
         P.vrow.tptr = P.rows.tptr;
         P.vrow.col = P.rows.col;
@@ -3133,6 +3159,26 @@ extern "C" int hf_case_adjust_timestep(hf_case *C, double *cfl, double *dt, int3
     // graphs included), so the next step uses the new values
     HF_CK(cudaMemcpyAsync((void *)C->P.ipar, C->h_ipar.data(), sizeof(hf_params) * ni, cudaMemcpyHostToDevice, st));
     HF_CK(cudaStreamSynchronize(st));
+    C->par.dt = C->h_ipar[0].dt;
+    C->P.par.dt = C->h_ipar[0].dt;
+    return HF_OK;
+}
+
+extern "C" int hf_case_set_timestep(hf_case *C, const double *dt, int32_t n)
+{
+    if (!C || !dt) return fail(HF_ERR_INVALID, "null argument");
+    if (n != C->ninst) return fail(HF_ERR_INVALID, "array size is not the instance count");
+    bool same = true;
+    for (int i = 0; i < n; i++) {
+        if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return fail(HF_ERR_INVALID, "time step must be positive and finite");
+        same = same && dt[i] == C->h_ipar[i].dt;
+    }
+    if (same) return HF_OK;
+    if (C->sie) return fail(HF_ERR_UNSUPPORTED, "new time step with the semi-implicit velocity (its matrix holds dt)");
+    for (int i = 0; i < n; i++) C->h_ipar[i].dt = dt[i];
+    HF_CK(cudaMemcpyAsync((void *)C->P.ipar, C->h_ipar.data(), sizeof(hf_params) * n, cudaMemcpyHostToDevice,
+                          C->stream));
+    HF_CK(cudaStreamSynchronize(C->stream));
     C->par.dt = C->h_ipar[0].dt;
     C->P.par.dt = C->h_ipar[0].dt;
     return HF_OK;

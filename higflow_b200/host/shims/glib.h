@@ -1,6 +1,7 @@
 /*
  * Minimal GLib stand-in for building the reference HigTree/HigFlow C sources
- * in place (oracle build only; test infrastructure, never shipped).
+ * in place in this image, which has no GLib (the HigFlow host build,
+ * higflow_b200/host, and the oracle build of the reference).
  *
  * Only the GHashTable surface that higtree/src/{mapper,point-mapper,pdomain,
  * mapper-syncer}.c use is provided: a chained hash table with the GLib

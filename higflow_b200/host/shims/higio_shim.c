@@ -1,5 +1,5 @@
 /*
- * AMR text-format reader for the oracle build (test infrastructure).
+ * AMR text-format reader for the HigFlow host build and the oracle build.
  *
  * higtree/src/higtree-io.c cannot be compiled here (it needs HDF5), so the
  * three reader entry points the reference calls on the step-setup path are

@@ -1,5 +1,5 @@
 /*
- * Single-rank load balancer for the oracle build (test infrastructure).
+ * Single-rank load balancer for the HigFlow host build and the oracle build.
  *
  * Stands in for higtree/src/lbal.c (Zoltan-based).  On one rank every input
  * tree stays local, in insertion order, and no tree is fringe, which is what

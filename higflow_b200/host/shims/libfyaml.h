@@ -1,7 +1,8 @@
 /*
- * libfyaml stand-in for the oracle build (test infrastructure).  The oracle
- * harness fills the solver parameters directly, so the YAML readers compiled
- * in from the reference are never called; each entry point aborts if reached.
+ * libfyaml stand-in for the HigFlow host build and the oracle build.  Both
+ * fill the solver parameters directly (higflow_b200/host/hf_host.c), so the
+ * YAML readers compiled in from the reference are never called; each entry
+ * point aborts if reached.
  */
 #ifndef HF_ORACLE_LIBFYAML_SHIM_H
 #define HF_ORACLE_LIBFYAML_SHIM_H

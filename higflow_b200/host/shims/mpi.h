@@ -1,6 +1,7 @@
 /*
  * Single-rank MPI stand-in for building the reference HigTree/HigFlow C sources
- * in place (oracle build only; test infrastructure, never shipped).
+ * in place in this image, which has no MPI (the HigFlow host build that records
+ * step programs, higflow_b200/host, and the oracle build of the reference).
  *
  * COMM_WORLD has exactly one rank (rank 0, size 1).  Collectives copy the send
  * buffer to the receive buffer; point-to-point calls abort, because on one rank

@@ -1,5 +1,5 @@
 /*
- * Single-rank MPI implementation for the oracle build (test infrastructure).
+ * Single-rank MPI implementation for the HigFlow host build and the oracle build.
  * See mpi.h for the contract.
  */
 #include "mpi.h"

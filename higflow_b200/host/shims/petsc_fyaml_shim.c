@@ -1,5 +1,6 @@
 /*
- * Definitions for the PETSc and libfyaml stand-ins (oracle build only).
+ * Definitions for the PETSc and libfyaml stand-ins (HigFlow host build and
+ * oracle build; neither library is in this image).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -16,7 +17,7 @@ PetscErrorCode PetscFinalize(void) { return 0; }
 
 static void no_yaml(const char *fn)
 {
-    fprintf(stderr, "oracle build: %s is not available (YAML input is not used by the oracle)\n", fn);
+    fprintf(stderr, "single-rank build: %s is not available (cases are built without YAML input)\n", fn);
     abort();
 }
 

@@ -455,7 +455,7 @@ class Program:
         )
 
     # ------------------------------------------------------------------
-    def save(self, path: str) -> None:
+    def save(self, path: str, compress: bool = True) -> None:
         arrs = dict(
             par_keys=np.array(_PARAM_NAMES),
             par_vals=np.array([float(self.par.get(n, _PARAM_DEFAULTS.get(n, 0))) for n in _PARAM_NAMES]),
@@ -472,7 +472,7 @@ class Program:
         if self.cell_slots is not None:
             arrs["cell_slots"] = self.cell_slots
             arrs["cell_flags"] = self.cell_flags
-        np.savez_compressed(path, **arrs)
+        (np.savez_compressed if compress else np.savez)(path, **arrs)
 
     @classmethod
     def load(cls, path: str) -> "Program":

@@ -1,25 +1,27 @@
 """Synthetic case populations for the batched and served benchmark configurations.
 
-Seeded draws in a fixed order (numpy.random.default_rng(seed)); every case is a
-lid-driven cavity on the unit square, its program tiled from the recorded seed
-(higflow_b200/tiling.py).  The explicit time step of each case is a fixed
-fraction of its explicit stability bound, recorded with the case.
+Seeded draws in a fixed order (numpy.random.default_rng(seed)).  Every case is
+a lid-driven cavity on the unit square or a channel [0,8] x [-1,1] (the
+geometry of the shipped higflow/example2d_Newt case), and its step program is
+recorded by the HigFlow host (higflow_b200/host.py): HigTree's own stencils,
+ids and weights.  The explicit time step of each case is a fixed fraction of
+its explicit stability bound, recorded with the case.
 """
 from __future__ import annotations
 
 import math
 from dataclasses import dataclass
-from typing import Dict, List
+from typing import List
 
 import numpy as np
 
+from . import host
 from . import program as hp
-from . import tiling
 
 
 @dataclass
 class CaseDraw:
-    n: int                 # cells per side
+    n: int                 # cells per side (channel: 2n x n/2 cells, the same count)
     model: int             # hp.OLDROYD_B / hp.GIESEKUS (viscoelastic) or -1 (Newtonian)
     De: float              # Weissenberg number (De in HigFlow's parameters)
     alpha: float           # Giesekus mobility
@@ -27,6 +29,7 @@ class CaseDraw:
     Re: float
     dt: float
     steps: int
+    geometry: str = "cavity"   # "cavity" or "channel"
 
     @property
     def cells(self) -> int:
@@ -96,24 +99,47 @@ def served_requests(count: int = 64, step_scale: float = 1.0 / 50.0, seed: int =
     return out
 
 
-_cache: Dict[tuple, hp.Program] = {}
+def partition(costs, parts: int) -> List[List[int]]:
+    """Indices of ``costs`` split into ``parts`` groups by greedy longest-first
+    assignment (each item, largest cost first, to the group with the smallest
+    total so far; ties to the lowest group).  Every index is in exactly one
+    group, groups keep ascending index order, and the largest group total is at
+    most 4/3 of the optimum (Graham's bound for this rule)."""
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * parts
+    groups: List[List[int]] = [[] for _ in range(parts)]
+    for i in order:
+        g = min(range(parts), key=lambda k: (load[k], k))
+        groups[g].append(i)
+        load[g] += costs[i]
+    return [sorted(g) for g in groups]
+
+
+def spec(c: CaseDraw) -> host.CaseSpec:
+    """The HigFlow case of one draw: a unit lid-driven cavity of n x n cells, or
+    a channel [0,8] x [-1,1] of 2n x n/2 square cells with the shipped case's
+    parabolic inflow (mean 1) and outflow; CUBISTA convection, incremental
+    projection, and for viscoelastic draws the log-conformation kernel from
+    identity with CUBISTA cell convection."""
+    par = dict(Re=c.Re, dt=c.dt)
+    if c.model >= 0:
+        par.update(flowtype=hp.VISCOELASTIC, ve_model=c.model, De=c.De, alpha=c.alpha, beta=c.beta,
+                   kernel=hp.KERNEL_LOG, kernel_tol=1e-2, ve_convecdiscrtype=hp.CELL_CUBISTA)
+    if c.geometry == "channel":
+        return host.channel(2 * c.n, max(2, c.n // 2), length=8.0, half=1.0, umax=1.5, **par)
+    return host.cavity(2, c.n, **par)
+
+
+def programs(draws: List[CaseDraw], procs=None) -> List[hp.Program]:
+    """Recorded programs of the draws (host processes in parallel, cached on disk)."""
+    return host.record_many([spec(c) for c in draws], procs=procs)
 
 
 def program(c: CaseDraw) -> hp.Program:
-    """The tiled cavity program of one draw, with its parameters."""
-    ve = c.model >= 0
-    key = (c.n, ve)
-    if key not in _cache:
-        _cache[key] = tiling.cavity(2, c.n, viscoelastic=ve)
-    base = _cache[key]
-    prog = hp.Program(**{k: v for k, v in base.__dict__.items() if k != "_keep"})
-    prog.par = dict(base.par)
-    prog.par.update(Re=c.Re, dt=c.dt)
-    if ve:
-        prog.par.update(ve_model=c.model, De=c.De, alpha=c.alpha, beta=c.beta, kernel=hp.KERNEL_LOG,
-                        kernel_tol=1e-2, ve_convecdiscrtype=hp.CELL_CUBISTA)
-    return prog
+    return programs([c], procs=1)[0]
 
 
-def batch(draws: List[CaseDraw]) -> hp.Program:
-    return hp.Program.concatenate([program(c) for c in draws])
+def batch(draws: List[CaseDraw], procs=None) -> hp.Program:
+    return hp.Program.concatenate(programs(draws, procs=procs))

@@ -346,6 +346,12 @@ int  hf_case_instance_iters(hf_case *c, int64_t *total_iters, int32_t n);
  * whose system matrix holds dt. */
 int  hf_case_adjust_timestep(hf_case *c, double *cfl, double *dt, int32_t n);
 
+/* Set each instance's time step (n = ninst) for the next steps, as a case main
+ * loop does when it changes ns->par.dt (higflow_adjust_timestep,
+ * hig-flow-timestep.c:115-139, or a restart); HF_ERR_UNSUPPORTED for the
+ * semi-implicit velocity when dt changes (its system matrix holds dt). */
+int  hf_case_set_timestep(hf_case *c, const double *dt, int32_t n);
+
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);
 

@@ -2,14 +2,12 @@
  * Oracle harness around the reference HigFlow library (test infrastructure:
  * used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm only).
  *
- * Builds a case the way a HigFlow main program does
- * (higflow/example2d_Newt/ns-example-2d.c:159-230), but from the legacy text
- * inputs (<name>.domain, <name>.bc, read by higflow_initialize_domain,
- * hig-flow-ic.c:11, and higflow_initialize_boundaries, hig-flow-bc.c:572) and
- * with the controllers filled directly instead of from YAML.  It then exposes
- * the reference's own time step and its fields through a small C API for
- * ctypes.  Boundary and initial values come from the callback tables below,
- * parameterised per boundary id.
+ * Cases are built by the drop-in host's builder (hfh_build,
+ * higflow_b200/host/hf_host.c), the way a HigFlow main program does
+ * (higflow/example2d_Newt/ns-example-2d.c:159-230), from legacy text inputs.
+ * This file adds what only the checker needs: the reference's own CPU time
+ * step (with the CPU Poisson engine of oracle/solver_cpu.c), its fields, its
+ * phase timers, CFL and adaptive step, through a small C API for ctypes.
  */
 #include <fcntl.h>
 #include <math.h>
@@ -29,122 +27,25 @@
 #include "higflow_b200.h"
 #include "higflow_b200_higflow.h"
 
-#define HFREF_MAXBC 16
+#include "hf_host.h"
 
-/* Case description passed from Python (all doubles/ints, no pointers). */
-typedef struct hfref_params {
-    int32_t flowtype, projtype, convecdiscrtype, secondconvecdiscrtype;
-    int32_t ve_model, ve_convecdiscrtype, kernel;  /* kernel: HF_KERNEL_* */
-    int32_t nbc;
-    double Re, dt, t0;
-    double De, beta, kernel_tol, alpha, epsilon, xi;
-    /* boundary velocity for bc id b, component d:
-     *   bc_u[b][d] + bc_upar[b][d] * (1 - ((x[bc_tdim[b]] - bc_c[b]) / bc_h[b])^2) */
-    double bc_u[HFREF_MAXBC][3];
-    double bc_upar[HFREF_MAXBC][3];
-    int32_t bc_tdim[HFREF_MAXBC];
-    double bc_c[HFREF_MAXBC], bc_h[HFREF_MAXBC];
-    double bc_p[HFREF_MAXBC];
-    double k_init[3][3];        /* initial kernel tensor (get_tensor) */
-    int32_t tempdiscrtype;      /* HF_EXPLICIT_EULER / HF_SEMI_IMPLICIT_EULER */
-    int32_t pad_;
-    double L2_fene, lambda_fene, E_fene;
-    int32_t ve_discrtype;       /* HF_VE_EXPLICIT / HF_VE_IMPLICIT */
-    int32_t pad2_;
-    double alpha_gptt, beta_gptt;
-} hfref_params;
+/* The case description is the host's (higflow_b200/host/hf_host.h): the
+ * oracle builds its cases with the drop-in host's own builder, hfh_build, and
+ * adds the reference's CPU step, field access and phase timers. */
+typedef hfh_params hfref_params;
 
 typedef struct hfref_case {
     higflow_solver *ns;
-    hfref_params par;
-    char nameload[1024];
     double t_velocity, t_pressure, t_final, t_ve, t_total;
 } hfref_case;
 
-static hfref_case *g_cur;
 extern double hfref_solve_seconds;
 extern int hfref_solve_iters;
 
-/* ---- callbacks (signatures of higflow_functions, hig-flow-kernel.h:217-234) ---- */
-static real cb_get_pressure(Point center, real t) { (void)center; (void)t; return 0.0; }
-static real cb_get_velocity(Point center, int dim, real t) { (void)center; (void)dim; (void)t; return 0.0; }
-static real cb_get_source_term(Point center, real t) { (void)center; (void)t; return 0.0; }
-static real cb_get_facet_source_term(Point center, int dim, real t) { (void)center; (void)dim; (void)t; return 0.0; }
-static real cb_get_boundary_pressure(int id, Point center, real t)
-{
-    (void)center; (void)t;
-    if (id < 0 || id >= HFREF_MAXBC) return 0.0;
-    return g_cur->par.bc_p[id];
-}
-static real cb_get_boundary_velocity(int id, Point center, int dim, real t)
-{
-    (void)t;
-    if (id < 0 || id >= HFREF_MAXBC) return 0.0;
-    const hfref_params *p = &g_cur->par;
-    real v = p->bc_u[id][dim];
-    if (p->bc_upar[id][dim] != 0.0) {
-        real s = (center[p->bc_tdim[id]] - p->bc_c[id]) / p->bc_h[id];
-        v += p->bc_upar[id][dim] * (1.0 - s * s);
-    }
-    return v;
-}
-static real cb_get_boundary_source_term(int id, Point center, real t) { (void)id; (void)center; (void)t; return 0.0; }
-static real cb_get_boundary_facet_source_term(int id, Point center, int dim, real t) { (void)id; (void)center; (void)dim; (void)t; return 0.0; }
+static void quiet_begin(void) { hfh_quiet_begin(); }
+static void quiet_end(void) { hfh_quiet_end(); }
 
-/* kernel-conformation transforms (commented variants in
- * higflow/example2d_Oldroyd/ns-example-2d.c:21-56) */
-static real cb_get_tensor(Point center, int i, int j, real t) { (void)center; (void)t; return g_cur->par.k_init[i][j]; }
-static real cb_get_kernel(int dim, real lambda, real tol)
-{
-    (void)dim;
-    switch (g_cur->par.kernel) {
-    case HF_KERNEL_LOG: return lambda < tol ? log(tol) : log(lambda);
-    case HF_KERNEL_SQRT: return lambda < tol ? sqrt(tol) : sqrt(lambda);
-    default: return lambda;
-    }
-}
-static real cb_get_kernel_inverse(int dim, real lambda, real tol)
-{
-    (void)dim; (void)tol;
-    switch (g_cur->par.kernel) {
-    case HF_KERNEL_LOG: return exp(lambda);
-    case HF_KERNEL_SQRT: return lambda * lambda;
-    default: return lambda;
-    }
-}
-static real cb_get_kernel_jacobian(int dim, real lambda, real tol)
-{
-    (void)dim;
-    switch (g_cur->par.kernel) {
-    case HF_KERNEL_LOG: return lambda < tol ? 1.0 / tol : 1.0 / lambda;
-    case HF_KERNEL_SQRT: return lambda < tol ? 0.5 / sqrt(tol) : 0.5 / sqrt(lambda);
-    default: return 1.0;
-    }
-}
-
-static int g_initialized;
-static int g_quiet = 1;
-static int g_saved_stdout = -1;
-
-static void quiet_begin(void)
-{
-    if (!g_quiet) return;
-    fflush(stdout);
-    g_saved_stdout = dup(1);
-    int devnull = open("/dev/null", O_WRONLY);
-    if (devnull >= 0) { dup2(devnull, 1); close(devnull); }
-}
-
-static void quiet_end(void)
-{
-    if (!g_quiet || g_saved_stdout < 0) return;
-    fflush(stdout);
-    dup2(g_saved_stdout, 1);
-    close(g_saved_stdout);
-    g_saved_stdout = -1;
-}
-
-void hfref_set_quiet(int on) { g_quiet = on; }
+void hfref_set_quiet(int on) { hfh_set_quiet(on); }
 
 static double now(void)
 {
@@ -157,78 +58,13 @@ int hfref_dim(void) { return DIM; }
 
 int hfref_create(const char *nameload, const hfref_params *p, hfref_case **out)
 {
-    if (!g_initialized) {
-        int argc = 1;
-        static char *argv0[] = {"hfref", NULL};
-        char **argv = argv0;
-        int myrank, ntasks;
-        higflow_initialize(&argc, &argv, &myrank, &ntasks);
-        g_initialized = 1;
-    }
     hfref_case *C = calloc(1, sizeof *C);
-    C->par = *p;
-    snprintf(C->nameload, sizeof C->nameload, "%s", nameload);
-    g_cur = C;
-    quiet_begin();
-
-    higflow_solver *ns = higflow_create();
-    memset(ns, 0, sizeof *ns);
-    C->ns = ns;
-    ns->par.nameload = C->nameload;
-    ns->par.namesave = C->nameload;
-    ns->par.nameprint = C->nameload;
-    ns->par.Re = p->Re;
-    ns->par.dt = p->dt;
-    ns->par.dt0 = p->dt;
-    ns->par.t = p->t0;
-    ns->par.step = 0;
-    ns->par.initstep = 0;
-    ns->par.finalstep = 1 << 30;
-    ns->par.ts = 1e30;
-    ns->par.tp = 1e30;
-    ns->contr.projtype = p->projtype;
-    ns->contr.flowtype = p->flowtype;
-    ns->contr.eoflow = false;
-    ns->contr.tempdiscrtype = p->tempdiscrtype == HF_SEMI_IMPLICIT_EULER ? SEMI_IMPLICIT_EULER
-                              : p->tempdiscrtype == HF_SEMI_IMPLICIT_CN ? SEMI_IMPLICIT_CN
-                              : p->tempdiscrtype == HF_SEMI_IMPLICIT_BDF2 ? SEMI_IMPLICIT_BDF2
-                              : p->tempdiscrtype == HF_EXPLICIT_RK2 ? EXPLICIT_RK2
-                              : p->tempdiscrtype == HF_EXPLICIT_RK3 ? EXPLICIT_RK3 : EXPLICIT_EULER;
-    ns->contr.spatialdiscrtype = ORDER2;
-    ns->contr.convecdiscrtype = p->convecdiscrtype;
-    ns->contr.secondconvecdiscrtype = p->secondconvecdiscrtype;
-    if (p->flowtype == VISCOELASTIC) {
-        ns->ed.ve.contr.model = p->ve_model;
-        ns->ed.ve.contr.discrtype = p->ve_discrtype == HF_VE_IMPLICIT ? IMPLICIT : EXPLICIT;
-        ns->ed.ve.contr.convecdiscrtype = p->ve_convecdiscrtype;
-        ns->ed.ve.par.De = p->De;
-        ns->ed.ve.par.beta = p->beta;
-        ns->ed.ve.par.kernel_tol = p->kernel_tol;
-        ns->ed.ve.par.alpha = p->alpha;
-        ns->ed.ve.par.epsilon = p->epsilon;
-        ns->ed.ve.par.xi = p->xi;
-        ns->ed.ve.par.L2_fene = p->L2_fene;
-        ns->ed.ve.par.lambda_fene = p->lambda_fene;
-        ns->ed.ve.par.E_fene = p->E_fene;
-        ns->ed.ve.par.alpha_gptt = p->alpha_gptt;
-        ns->ed.ve.par.beta_gptt = p->beta_gptt;
+    if (!C) return -1;
+    int rc = hfh_build(nameload, p, &C->ns);
+    if (rc != 0) {
+        free(C);
+        return rc;
     }
-
-    higflow_set_external_functions(ns, cb_get_pressure, cb_get_velocity, cb_get_source_term,
-                                   cb_get_facet_source_term, cb_get_boundary_pressure,
-                                   cb_get_boundary_velocity, cb_get_boundary_source_term,
-                                   cb_get_boundary_facet_source_term);
-    const int cache = 1, order = 2;
-    higflow_create_domain(ns, cache, order);
-    if (p->flowtype == VISCOELASTIC)
-        higflow_create_domain_viscoelastic(ns, cache, order, cb_get_tensor, cb_get_kernel,
-                                           cb_get_kernel_inverse, cb_get_kernel_jacobian);
-    higflow_initialize_domain(ns, 1, 0, order);
-    higflow_initialize_boundaries(ns);
-    higflow_create_distributed_properties(ns);
-    higflow_initialize_distributed_properties(ns);
-    higflow_create_solver(ns);
-    quiet_end();
     *out = C;
     return 0;
 }
@@ -319,7 +155,7 @@ int hfref_centers(hfref_case *C, int32_t facet_dim, double *out)
  * with the time update of the case main loop (ns-example-2d.c:246-248). */
 int hfref_step(hfref_case *C, int32_t nsteps, double *seconds)
 {
-    g_cur = C;
+    hfh_select(C->ns);
     higflow_solver *ns = C->ns;
     quiet_begin();
     double t0 = now();
@@ -343,7 +179,7 @@ int hfref_step(hfref_case *C, int32_t nsteps, double *seconds)
  * final velocity+pressure, viscoelastic (Du+constitutive+polymeric). */
 int hfref_step_phased(hfref_case *C, int32_t nsteps, double *times)
 {
-    g_cur = C;
+    hfh_select(C->ns);
     higflow_solver *ns = C->ns;
     const int ve = ns->contr.flowtype == VISCOELASTIC;
     quiet_begin();
@@ -402,20 +238,20 @@ double hfref_dt(hfref_case *C) { return C->ns->par.dt; }
 
 double hfref_cfl(hfref_case *C)
 {
-    g_cur = C;
+    hfh_select(C->ns);
     return higflow_compute_CFL(C->ns);
 }
 
 void hfref_adjust_timestep(hfref_case *C)
 {
-    g_cur = C;
+    hfh_select(C->ns);
     higflow_adjust_timestep(C->ns);
 }
 
 /* flatten through the binding (hf_flatten) and hand the program to Python */
 int hfref_flatten(hfref_case *C, hf_program **out)
 {
-    g_cur = C;
+    hfh_select(C->ns);
     quiet_begin();
     int rc = hf_flatten(C->ns, out);
     quiet_end();
@@ -428,12 +264,7 @@ const char *hfref_flatten_error(void) { return hf_flatten_error(); }
 
 void hfref_destroy(hfref_case *C)
 {
-    /* higflow_destroy releases everything the case created; the partition
-     * graph and trees are leaked by the reference itself and live until exit */
     if (!C) return;
-    g_cur = C;
-    quiet_begin();
-    higflow_destroy(C->ns);
-    quiet_end();
+    hfh_destroy(C->ns);
     free(C);
 }

@@ -17,31 +17,15 @@ from typing import Dict, Optional, Sequence
 import numpy as np
 
 from higflow_b200 import program as hp
+from higflow_b200.host import CaseSpec, HostParams, cavity, channel  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-MAXBC = 16
 
 _libs: Dict[int, C.CDLL] = {}
 
 
-class RefParams(C.Structure):
-    _fields_ = [
-        ("flowtype", C.c_int32), ("projtype", C.c_int32), ("convecdiscrtype", C.c_int32),
-        ("secondconvecdiscrtype", C.c_int32), ("ve_model", C.c_int32),
-        ("ve_convecdiscrtype", C.c_int32), ("kernel", C.c_int32), ("nbc", C.c_int32),
-        ("Re", C.c_double), ("dt", C.c_double), ("t0", C.c_double),
-        ("De", C.c_double), ("beta", C.c_double), ("kernel_tol", C.c_double),
-        ("alpha", C.c_double), ("epsilon", C.c_double), ("xi", C.c_double),
-        ("bc_u", (C.c_double * 3) * MAXBC), ("bc_upar", (C.c_double * 3) * MAXBC),
-        ("bc_tdim", C.c_int32 * MAXBC), ("bc_c", C.c_double * MAXBC), ("bc_h", C.c_double * MAXBC),
-        ("bc_p", C.c_double * MAXBC),
-        ("k_init", (C.c_double * 3) * 3),
-        ("tempdiscrtype", C.c_int32), ("pad_", C.c_int32),
-        ("L2_fene", C.c_double), ("lambda_fene", C.c_double), ("E_fene", C.c_double),
-        ("ve_discrtype", C.c_int32), ("pad2_", C.c_int32),
-        ("alpha_gptt", C.c_double), ("beta_gptt", C.c_double),
-    ]
+RefParams = HostParams
 
 
 def available(dim: int = 2) -> bool:
@@ -122,7 +106,7 @@ class RefCase:
         self.L = lib(self.dim)
         self.tmp = tempfile.mkdtemp(prefix="hfref_")
         name = spec.write(self.tmp)
-        p = spec.ref_params()
+        p = spec.host_params()
         h = C.c_void_p()
         rc = self.L.hfref_create(name.encode(), C.byref(p), C.byref(h))
         if rc != 0:
@@ -243,148 +227,5 @@ class RefCase:
         return out
 
 
-# ----------------------------------------------------------------------
-# case descriptions (text inputs in the reference's legacy formats)
-# ----------------------------------------------------------------------
-class CaseSpec:
-    """A box domain with per-face boundary conditions, in the reference's
-    legacy .domain/.bc text formats (hig-flow-ic.c:11-56, hig-flow-bc.c:572-614)
-    and its .amr format (higtree-io.c:269-293)."""
-
-    def __init__(self, dim: int, n: Sequence[int], lo: Sequence[float], hi: Sequence[float],
-                 faces: Sequence[dict], **par):
-        self.dim = dim
-        self.n = list(n)
-        self.lo = list(lo)
-        self.hi = list(hi)
-        self.faces = list(faces)   # per face: dict(axis, side, p='N'|'D', u='D'|'N', uval=[..], upar=.., p_val=)
-        self.flowtype = par.get("flowtype", hp.NEWTONIAN)
-        self.par = dict(par)
-        self.refine: list = par.get("refine", [])   # extra levels: list of (delta, [(init, size)])
-
-    def _amr(self, lo, hi, n, levels=()) -> str:
-        s = " ".join(f"{lo[d]!r} {hi[d]!r}" for d in range(self.dim)) + "\n"
-        s += f"{1 + len(levels)}\n"
-        delta = [(hi[d] - lo[d]) / n[d] if n[d] > 0 else 0.0 for d in range(self.dim)]
-        s += " ".join(repr(x) for x in delta) + " 1\n"
-        s += " ".join("0" for _ in range(self.dim)) + " " + " ".join(str(x) for x in n) + "\n"
-        for (ldelta, patches) in levels:
-            s += " ".join(repr(x) for x in ldelta) + f" {len(patches)}\n"
-            for (init, size) in patches:
-                s += " ".join(str(x) for x in init) + " " + " ".join(str(x) for x in size) + "\n"
-        return s
-
-    def write(self, d: str) -> str:
-        name = os.path.join(d, "case")
-        with open(os.path.join(d, "dom0.amr"), "w") as f:
-            f.write(self._amr(self.lo, self.hi, self.n, self.refine))
-        with open(name + ".domain", "w") as f:
-            f.write("1\n" + os.path.join(d, "dom0.amr") + "\n")
-        lines = [str(len(self.faces))]
-        for b, face in enumerate(self.faces):
-            ax, side = face["axis"], face["side"]
-            lo = list(self.lo)
-            hi = list(self.hi)
-            n = list(self.n)
-            if side == 0:
-                hi[ax] = lo[ax]
-            else:
-                lo[ax] = hi[ax]
-            n[ax] = 1
-            nb = [n[k] if k != ax else 1 for k in range(self.dim)]
-            # degenerate axis: delta 0 (as in higflow/example2d_Newt/amrs/bc/*.amr)
-            s = " ".join(f"{lo[k]!r} {hi[k]!r}" for k in range(self.dim)) + "\n1\n"
-            delta = [0.0 if k == ax else (hi[k] - lo[k]) / nb[k] for k in range(self.dim)]
-            s += " ".join(repr(x) for x in delta) + " 1\n"
-            s += " ".join("0" for _ in range(self.dim)) + " " + " ".join(str(x) for x in nb) + "\n"
-            path = os.path.join(d, f"bc{b}.amr")
-            with open(path, "w") as f:
-                f.write(s)
-            ptype = 0 if face.get("p", "N") == "D" else 1
-            lines.append(str(b))
-            lines.append(path)
-            lines.append(f"{ptype} 0")
-            utype = 0 if face.get("u", "D") == "D" else 1
-            for _ in range(self.dim):
-                lines.append(f"{utype} 0")
-        with open(name + ".bc", "w") as f:
-            f.write("\n".join(lines) + "\n")
-        return name
-
-    def ref_params(self) -> RefParams:
-        p = RefParams()
-        g = self.par.get
-        p.flowtype = self.flowtype
-        p.projtype = g("projtype", hp.INCREMENTAL)
-        p.convecdiscrtype = g("convecdiscrtype", hp.SECOND_ORDER)
-        p.secondconvecdiscrtype = g("secondconvecdiscrtype", hp.CUBISTA)
-        p.ve_model = g("ve_model", hp.OLDROYD_B)
-        p.ve_convecdiscrtype = g("ve_convecdiscrtype", hp.CELL_CUBISTA)
-        p.kernel = g("kernel", hp.KERNEL_LOG)
-        p.nbc = len(self.faces)
-        p.Re = g("Re", 100.0)
-        p.dt = g("dt", 1e-4)
-        p.t0 = g("t0", 0.0)
-        p.De = g("De", 1.0)
-        p.beta = g("beta", 1.0 / 9.0)
-        p.kernel_tol = g("kernel_tol", 1e-2)
-        p.alpha = g("alpha", 0.2)
-        p.epsilon = g("epsilon", 0.25)
-        p.xi = g("xi", 0.0)
-        p.tempdiscrtype = g("tempdiscrtype", hp.EXPLICIT_EULER)
-        p.L2_fene = g("L2_fene", 100.0)
-        p.lambda_fene = g("lambda_fene", 1.0)
-        p.E_fene = g("E_fene", 0.0)
-        p.ve_discrtype = g("ve_discrtype", hp.VE_EXPLICIT)
-        p.alpha_gptt = g("alpha_gptt", 1.0)
-        p.beta_gptt = g("beta_gptt", 1.0)
-        for b, face in enumerate(self.faces):
-            for d, v in enumerate(face.get("uval", [0.0] * self.dim)):
-                p.bc_u[b][d] = v
-            for d, v in enumerate(face.get("upar", [0.0] * self.dim)):
-                p.bc_upar[b][d] = v
-            p.bc_tdim[b] = face.get("tdim", 0)
-            p.bc_c[b] = face.get("c", 0.0)
-            p.bc_h[b] = face.get("h", 1.0)
-            p.bc_p[b] = face.get("p_val", 0.0)
-        kin = g("k_init", None)
-        if kin is None:
-            # kernel of A = I: log -> 0, identity/sqrt -> I
-            ident = p.kernel != hp.KERNEL_LOG
-            for i in range(3):
-                for j in range(3):
-                    p.k_init[i][j] = 1.0 if (ident and i == j) else 0.0
-        else:
-            for i in range(3):
-                for j in range(3):
-                    p.k_init[i][j] = kin[i][j]
-        return p
-
-
-def cavity(dim: int = 2, n: int = 16, lid: float = 1.0, **par) -> CaseSpec:
-    """Lid-driven cavity on the unit square/cube: no-slip walls, lid velocity
-    u_0 = ``lid`` on the top face (y = 1 in 2D, z = 1 in 3D), Neumann pressure
-    everywhere (so the pressure is pinned, hig-flow-bc.c:597-602)."""
-    faces = []
-    top = dim - 1
-    for ax in range(dim):
-        for side in (0, 1):
-            uval = [0.0] * dim
-            if ax == top and side == 1:
-                uval[0] = lid
-            faces.append(dict(axis=ax, side=side, p="N", u="D", uval=uval))
-    return CaseSpec(dim, [n] * dim, [0.0] * dim, [1.0] * dim, faces, **par)
-
-
-def channel(nx: int = 32, ny: int = 8, length: float = 8.0, half: float = 1.0, umax: float = 1.5,
-            **par) -> CaseSpec:
-    """2D channel [0,L] x [-h,h]: parabolic inflow umax*(1-(y/h)^2) at x = 0,
-    no-slip walls, Dirichlet pressure / Neumann velocity outflow at x = L
-    (the shipped higflow/example2d_Newt channel)."""
-    faces = [
-        dict(axis=0, side=0, p="N", u="D", uval=[0.0, 0.0], upar=[umax, 0.0], tdim=1, c=0.0, h=half),
-        dict(axis=0, side=1, p="D", u="N", uval=[0.0, 0.0]),
-        dict(axis=1, side=0, p="N", u="D", uval=[0.0, 0.0]),
-        dict(axis=1, side=1, p="N", u="D", uval=[0.0, 0.0]),
-    ]
-    return CaseSpec(2, [nx, ny], [0.0, -half], [length, half], faces, **par)
+# case descriptions are the drop-in host's (higflow_b200/host.py)
+__all__ = ["CaseSpec", "cavity", "channel", "RefCase", "available", "mlfv"]

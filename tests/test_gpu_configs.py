@@ -1,0 +1,78 @@
+"""The benchmark configurations against the reference itself, at their own sizes.
+
+Programs are recorded by the HigFlow host (higflow_b200/host.py) exactly as the
+benchmark records them; the reference fields come from the reference's own
+step (tests/golden/make_configs.py).  Tolerances, relative L2 per field:
+plain FP64 1e-10 (the parity bar), mixed form 1e-6 (the precision bar of the
+mixed form against the FP64 oracle).
+
+* C1: the 64x64 Newtonian lid-driven cavity, Re 100, dt 1e-4, 200 steps from
+  rest (the whole configuration).
+* C4 subset: six instances of the batched Giesekus population (sides 32 to
+  129), 20 steps from rest with the conformation at the identity, run as one
+  batch.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from higflow_b200 import engine, host, workloads
+from higflow_b200 import program as hp
+from tests.helpers import GOLDEN, rel_l2
+
+PLAIN_TOL = 1e-10
+MIXED_TOL = 1e-6
+
+
+def _c1():
+    prog = host.record(host.cavity(2, 64, Re=100.0, dt=1e-4))
+    ref = dict(np.load(os.path.join(GOLDEN, "c1_64_200.npz")))
+    return prog, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision, tol", [(hp.PREC_FP64, PLAIN_TOL), (hp.PREC_MIXED, MIXED_TOL)])
+def test_c1_whole_configuration_matches_reference(precision, tol):
+    prog, ref = _c1()
+    case = engine.Case(prog, engine.options(rtol=1e-13 if precision == hp.PREC_FP64 else 1e-10, atol=1e-300,
+                                            precision=precision))
+    case.step(int(ref["steps"]))
+    err = {"u0": rel_l2(ref["ref_u0"], case.get(hp.FIELD_U, 0)), "u1": rel_l2(ref["ref_u1"], case.get(hp.FIELD_U, 1)),
+           "p": rel_l2(ref["ref_p"], case.get(hp.FIELD_P))}
+    case.close()
+    assert max(err.values()) < tol, err
+
+
+def _c4_sub():
+    ref = dict(np.load(os.path.join(GOLDEN, "c4_sub_20.npz")))
+    draws = workloads.batched_giesekus()
+    idx = [int(i) for i in ref["index"]]
+    progs = [host.record(workloads.spec(draws[i])) for i in idx]
+    return idx, progs, ref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision, tol", [(hp.PREC_FP64, PLAIN_TOL), (hp.PREC_MIXED, MIXED_TOL)])
+def test_c4_subset_batch_matches_reference(precision, tol):
+    idx, progs, ref = _c4_sub()
+    batch = hp.Program.concatenate(progs)
+    case = engine.Case(batch, engine.options(rtol=1e-13 if precision == hp.PREC_FP64 else 1e-10, atol=1e-300,
+                                             precision=precision))
+    case.step(int(ref["steps"]))
+    worst = {}
+    for j, i in enumerate(idx):
+        got = {f"u{d}": case.get_instance(hp.FIELD_U, d, j) for d in range(2)}
+        got["p"] = case.get_instance(hp.FIELD_P, 0, j)
+        for k in range(4):
+            got[f"K{k}"] = case.get_instance(hp.FIELD_KERNEL, k, j)
+        err = {k: rel_l2(ref[f"ref{i}_{k}"], v) for k, v in got.items()}
+        worst[i] = max(err.values())
+        assert worst[i] < tol, (i, err)
+    case.close()
+
+
+def test_fixture_instances_are_the_generator_selection():
+    from tests.golden.make_configs import c4_subset
+    ref = np.load(os.path.join(GOLDEN, "c4_sub_20.npz"))
+    assert [int(i) for i in ref["index"]] == c4_subset()

@@ -6,7 +6,7 @@ import pytest
 
 from higflow_b200 import engine
 from higflow_b200 import program as hp
-from higflow_b200 import tiling
+from higflow_b200 import host
 
 pytestmark = pytest.mark.gpu
 
@@ -18,11 +18,11 @@ def _requests():
     rng = np.random.default_rng(3)
     for k, (n, ve, steps) in enumerate([(24, False, 7), (40, True, 5), (32, True, 9), (56, False, 4),
                                         (28, True, 6), (48, False, 8)]):
-        prog = tiling.cavity(2, n, viscoelastic=ve)
-        prog.par.update(Re=1.0 if ve else 100.0, dt=1e-4 if ve else 2e-4)
+        par = dict(Re=1.0 if ve else 100.0, dt=1e-4 if ve else 2e-4)
         if ve:
-            prog.par.update(ve_model=hp.GIESEKUS if k % 2 else hp.OLDROYD_B, De=0.3 + 0.1 * k, alpha=0.2,
-                            beta=0.1, kernel=hp.KERNEL_LOG, kernel_tol=1e-2)
+            par.update(flowtype=hp.VISCOELASTIC, ve_model=hp.GIESEKUS if k % 2 else hp.OLDROYD_B, De=0.3 + 0.1 * k,
+                       alpha=0.2, beta=0.1, kernel=hp.KERNEL_LOG, kernel_tol=1e-2)
+        prog = host.record(host.cavity(2, n, **par))
         fields = {(hp.FIELD_U, d): 0.05 * rng.standard_normal(prog.nfacet[d]) for d in range(2)}
         out.append((prog, engine.options(rtol=1e-10, atol=1e-300, precision=hp.PREC_MIXED if ve else hp.PREC_FP64),
                     steps, fields))
