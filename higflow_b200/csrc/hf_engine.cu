@@ -1258,6 +1258,7 @@ struct hf_case {
     bool mixed = false;
     PcgFine G{};
     double *pa = nullptr, *pb = nullptr;   // CG directions (alternating)
+    float *pa32 = nullptr, *pb32 = nullptr;   // the mixed form's inner directions
     int nlev = 1;                   // multigrid levels including the finest
     VLev<double> L64[kMaxLevels] = {};
     VLev<float> L32[kMaxLevels] = {};
@@ -1943,6 +1944,16 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     const size_t o_r = ar.zeros<double>(n), o_z = ar.zeros<double>(n), o_q = ar.zeros<double>(n);
     const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n), o_xprev = ar.zeros<double>(n);
     const size_t o_part = ar.zeros<double>((size_t)LH[0].ablk.size() * 2);
+    // mixed form: the inner solve's FP32 vectors
+    size_t o_r32 = 0, o_z32 = 0, o_q32 = 0, o_e32 = 0, o_pa32 = 0, o_pb32 = 0;
+    if (mixed) {
+        o_r32 = ar.zeros<float>(n);
+        o_z32 = ar.zeros<float>(n);
+        o_q32 = ar.zeros<float>(n);
+        o_e32 = ar.zeros<float>(n);
+        o_pa32 = ar.zeros<float>(n);
+        o_pb32 = ar.zeros<float>(n);
+    }
     std::vector<IScal> S(ni);
     for (int i = 0; i < ni; i++) {
         memset(&S[i], 0, sizeof(IScal));
@@ -1996,6 +2007,17 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     G.maxit = C->opt.poisson_maxit;
     C->pa = (double *)(base + o_pa);
     C->pb = (double *)(base + o_pb);
+    if (mixed) {
+        G.A32 = TRows<float>{G.A.rd, G.A.toff, (const float *)(base + o_tval32)};
+        G.r32 = (float *)(base + o_r32);
+        G.z32 = (float *)(base + o_z32);
+        G.q32 = (float *)(base + o_q32);
+        G.e32 = (float *)(base + o_e32);
+        G.eta = kInnerEta;
+        G.inner_maxit = kInnerMaxit;
+        C->pa32 = (float *)(base + o_pa32);
+        C->pb32 = (float *)(base + o_pb32);
+    }
     if (amg) {
         for (int l = 0; l < nlev; l++) {
             if (mixed) {
@@ -2048,17 +2070,16 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
 // ---------------------------------------------------------------------------
 // one time step as a CUDA graph
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, typename R>
 void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T> *H, const TailInst<T> *ti,
-                    int &kernels)
+                    const R *r0, int &kernels)
 {
     const IScal *S = C->G.S;
-    const double *r0 = C->G.r;
     // the large levels, every instance at once, down to each instance's tail
     for (int l = 0; l < C->nreg; l++) {
         if (L[l].nsblk) {
-            if (l == 0) k_vc_down<T, true><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
-            else k_vc_down<T, false><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
+            if (l == 0) k_vc_down<T, true, R><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
+            else k_vc_down<T, false, R><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
             kernels++;
         }
         if (L[l + 1].nablk) {
@@ -2067,7 +2088,7 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T>
         }
     }
     // the small levels: one CTA per instance
-    k_vc_tail<T><<<C->ninst, kTailThreads, 0, st>>>(H, ti, r0, S);
+    k_vc_tail<T, R><<<C->ninst, kTailThreads, 0, st>>>(H, ti, r0, S);
     kernels++;
     for (int l = C->nreg - 1; l >= 0; l--) {
         if (!L[l].nsblk) continue;
@@ -2078,7 +2099,6 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T>
             kernels++;
         }
     }
-    k_pcg_z<T, false><<<C->G.nblk, kBlock, 0, st>>>(C->G, L[0]);
     kernels++;
 }
 
@@ -2087,17 +2107,27 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T>
 void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, int &kernels)
 {
     for (int it = 0; it < 2; it++) {
+        const int set = it == 1 ? (cond ? 1 : 2) : 0;
+        if (C->mixed) {
+            // the inner FP32 iteration of the mixed form
+            enqueue_vcycle<float, float>(C, st, C->L32, C->h32, C->t32, C->G.r32, kernels);
+            k_pcg_z32<<<C->G.nblk, kBlock, 0, st>>>(C->G, C->L32[0]);
+            float *po = it == 0 ? C->pa32 : C->pb32, *pn = it == 0 ? C->pb32 : C->pa32;
+            k_pcg_dir32<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
+            k_pcg_update32<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, set);
+            kernels += 3;
+            continue;
+        }
         if (!C->amg) {
             k_pcg_z<double, true><<<C->G.nblk, kBlock, 0, st>>>(C->G, VLev<double>{});
-            kernels++;
-        } else if (C->mixed) {
-            enqueue_vcycle<float>(C, st, C->L32, C->h32, C->t32, kernels);
         } else {
-            enqueue_vcycle<double>(C, st, C->L64, C->h64, C->t64, kernels);
+            enqueue_vcycle<double, double>(C, st, C->L64, C->h64, C->t64, C->G.r, kernels);
+            k_pcg_z<double, false><<<C->G.nblk, kBlock, 0, st>>>(C->G, C->L64[0]);
         }
+        kernels++;
         double *po = it == 0 ? C->pa : C->pb, *pn = it == 0 ? C->pb : C->pa;
         k_pcg_dir<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
-        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, it == 1 ? (cond ? 1 : 2) : 0);
+        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, set);
         kernels += 2;
     }
 }
@@ -2269,13 +2299,25 @@ int eager_step(hf_case *C)
     int fixed = 0, body = 0;
     enqueue_pre<D>(C, F, fixed);
     if (C->sie_rc) return C->sie_rc;
-    for (;;) {
-        body = 0;
-        enqueue_body(C, C->stream, 0, body);
+    // the mixed form: up to kMaxSweeps inner solves, each followed by the FP64
+    // correction; the plain form: one solve
+    const int sweeps = C->mixed ? kMaxSweeps : 1;
+    for (int sw = 0; sw < sweeps; sw++) {
+        for (;;) {
+            body = 0;
+            enqueue_body(C, C->stream, 0, body);
+            HF_CK(cudaGetLastError());
+            HF_CK(cudaMemcpyAsync(C->h_ctl, C->G.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, C->stream));
+            HF_CK(cudaStreamSynchronize(C->stream));
+            if (!(C->h_ctl->active > 0 && C->h_ctl->bodies < C->h_ctl->maxbodies)) break;
+        }
+        if (!C->mixed) break;
+        k_ir_correct<<<C->G.nblk, kBlock, 0, C->stream>>>(C->G, 0, 0, sw == sweeps - 1);
+        fixed++;
         HF_CK(cudaGetLastError());
         HF_CK(cudaMemcpyAsync(C->h_ctl, C->G.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, C->stream));
         HF_CK(cudaStreamSynchronize(C->stream));
-        if (!(C->h_ctl->active > 0 && C->h_ctl->bodies < C->h_ctl->maxbodies)) break;
+        if (C->h_ctl->active == 0) break;
     }
     enqueue_post<D>(C, F, fixed);
     HF_CK(cudaGetLastError());
@@ -2294,30 +2336,54 @@ int capture_step(hf_case *C, DevFields F, cudaGraph_t *gout)
     C->capturing = true;
     enqueue_pre<D>(C, F, fixed);
 
-    // the iterations: a conditional WHILE node after everything captured so far
+    // the iterations: a conditional WHILE node after everything captured so far;
+    // the mixed form has kMaxSweeps of them, each followed by its FP64
+    // correction, which sets the next one's condition
+    const int sweeps = C->mixed ? kMaxSweeps : 1;
+    cudaError_t e = cudaSuccess;
+    cudaGraphConditionalHandle cond[kMaxSweeps] = {};
+    bool have[kMaxSweeps] = {};
     cudaGraph_t g = nullptr;
-    cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
-    cudaGraphConditionalHandle cond = 0;
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
-    cudaGraphNodeParams cp{};
-    cudaGraphNode_t node = nullptr;
-    if (e == cudaSuccess) {
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
-    }
-    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
-    if (e == cudaSuccess) {
-        cudaGraph_t bg = cp.conditional.phGraph_out[0];
-        e = cudaStreamBeginCaptureToGraph(C->body_stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    for (int sw = 0; sw < sweeps && e == cudaSuccess; sw++) {
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps);
+        if (e == cudaSuccess && !have[sw]) e = cudaGraphConditionalHandleCreate(&cond[sw], g, 1, cudaGraphCondAssignDefault);
+        have[sw] = true;
+        cudaGraphNodeParams cp{};
+        cudaGraphNode_t node = nullptr;
         if (e == cudaSuccess) {
-            enqueue_body(C, C->body_stream, cond, body);
-            e = cudaStreamEndCapture(C->body_stream, &bg);
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond[sw];
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+        }
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess) {
+            cudaGraph_t bg = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(C->body_stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                body = 0;
+                enqueue_body(C, C->body_stream, cond[sw], body);
+                e = cudaStreamEndCapture(C->body_stream, &bg);
+            }
+        }
+        if (e == cudaSuccess && C->mixed) {
+            // the correction sets the condition of the next sweep (created with
+            // the next node; a handle is a value, so it is created first here)
+            cudaGraphConditionalHandle next = 0;
+            const bool last = sw == sweeps - 1;
+            if (!last) e = cudaGraphConditionalHandleCreate(&next, g, 1, cudaGraphCondAssignDefault);
+            if (e == cudaSuccess) {
+                k_ir_correct<<<C->G.nblk, kBlock, 0, st>>>(C->G, next, last ? 0 : 1, last ? 1 : 0);
+                fixed++;
+                if (!last) {
+                    cond[sw + 1] = next;
+                    have[sw + 1] = true;
+                }
+            }
         }
     }
     enqueue_post<D>(C, F, fixed);
@@ -3084,16 +3150,18 @@ extern "C" int hf_case_stats(hf_case *C, hf_stats *out)
         s.last_iters = 0;
         s.last_residual = 0.0;
         s.total_iters = 0;
+        s.last_outer = 1;
         for (int i = 0; i < C->ninst; i++) {
             const IScal &q = C->h_S[i];
-            s.last_iters = std::max(s.last_iters, q.iters);
+            s.last_iters = std::max(s.last_iters, q.iters + q.iters_prev);
+            s.last_outer = std::max(s.last_outer, C->mixed ? q.outer + 1 : 1);
             s.last_residual = std::max(s.last_residual, q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr));
             s.total_iters += q.total_iters;
         }
         s.kernel_launches = s.steps * C->fixed_kernels + C->h_ctl->total_bodies * C->body_kernels + C->sie_launches;
     }
     *out = C->stats;
-    out->last_outer = 1;
+    if (!C->use_cg) out->last_outer = 1;
     return HF_OK;
 }
 
@@ -3118,7 +3186,8 @@ extern "C" int hf_case_instance_result(hf_case *C, int32_t inst, int32_t *iters,
     int rc = pull_state(C);
     if (rc) return rc;
     const IScal &q = C->h_S[inst];
-    if (iters) *iters = q.iters;
+    if (iters) *iters = q.iters + q.iters_prev;
+    if (outer) *outer = C->mixed ? q.outer + 1 : 1;
     if (status) *status = q.status;
     if (residual) *residual = q.bb > 0 ? sqrt(q.rr / q.bb) : sqrt(q.rr);
     return HF_OK;
@@ -3574,14 +3643,27 @@ __global__ void __launch_bounds__(kBlock) k_na_dinv(DevMat M, double *dinv)
     dinv[i] = d;
 }
 
-// fresh scalars: zero, iteration cap set; the reduction counter is left as it is
+// fresh scalars: zero (the reduction counter too, so a call that stopped on an
+// error leaves nothing behind for the next one), iteration cap set
 __global__ void k_na_begin(Scal *sc, int maxit)
 {
-    const unsigned counter = sc->counter;
     Scal z{};
     z.maxit = maxit;
-    z.counter = counter;
     *sc = z;
+}
+
+// An error inside the no-alloc solve: wait for the kernels already queued (they
+// use the shared scratch) when the stream still answers, forget the kept scratch
+// address of the device (the next call looks it up again), then report.
+int na_fail(cudaStream_t st, int dev, const std::string &msg)
+{
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    {
+        std::lock_guard<std::mutex> lock(g_na_mutex);
+        g_na_ptr[dev] = nullptr;
+    }
+    return fail(HF_ERR_CUDA, msg);
 }
 
 }  // namespace
@@ -3685,9 +3767,10 @@ extern "C" int hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const 
                 k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(M, V, V.sh, V.t, 1);
                 k_bi_update<<<blocks(n), kBlock, 0, st>>>(M, V);
             }
-            HF_CK(cudaGetLastError());
-            HF_CK(cudaMemcpyAsync(&h, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-            HF_CK(cudaStreamSynchronize(st));
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&h, V.sc, sizeof(Scal), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return na_fail(st, dev, std::string("no-alloc BiCGStab: ") + cudaGetErrorString(e));
             if (h.done) break;
             chunk = std::min(chunk * 2, 32);
         }

@@ -34,6 +34,12 @@
 #include <cstdint>
 
 constexpr int kMaxLevels = 16;       // multigrid levels including the finest
+// mixed form: inner FP32 sweeps per solve, each to eta times the FP64 residual
+// it starts from (FP32 CG reaches about 1e-6 of its start), at most
+// kInnerMaxit iterations
+constexpr int kMaxSweeps = 4;
+constexpr double kInnerEta = 1e-5;
+constexpr int kInnerMaxit = 60;
 constexpr int kMaxCoarse = 128;      // rows of the coarsest level (dense inverse)
 constexpr int kCoarseCap = 1024;     // largest coarsest level accepted (stalled coarsening)
 
@@ -63,6 +69,11 @@ struct IScal {
     int32_t iters, status, done, tail0;  // tail0: the whole V-cycle is the tail (s = 0)
     uint32_t counter, pad;
     int64_t total_iters;
+    // mixed form (FP32 inner CG inside FP64 refinement): the inner sweep's
+    // target, sweeps done, inner iterations of the step's earlier sweeps, and
+    // fin = the FP64 residual met the target (or the solve failed)
+    double tol2in;
+    int32_t outer, iters_prev, fin, pad2;
 };
 
 // loop control and error record of the whole case
@@ -191,6 +202,13 @@ struct PcgFine {
     int projtype_all;         // the projection type of every instance, or -1
     double rtol, atol;
     int maxit;
+    // mixed form: the inner solve of A e = r in FP32 (operator, vectors and
+    // V-cycle), e applied to the FP64 unknown and r updated in FP64 after
+    // each sweep (k_ir_correct); r32 is null in the plain form
+    TRows<float> A32;
+    float *r32, *z32, *q32, *e32;
+    double eta;               // inner sweep target: ||r_in|| <= eta ||r|| (or the outer target)
+    int inner_maxit;          // iterations per inner sweep
 };
 
 // The smoothing sweeps use each level's dinv array already scaled by the
@@ -409,6 +427,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
         const double ax = trow(G.A, cc, [&](int j) { return x[j]; });
         const double r = bred - ax;
         G.r[cc] = r;
+        if (G.r32) {
+            G.r32[cc] = (float)r;
+            G.e32[cc] = 0.f;
+        }
         part[0] += r * r;
         part[1] += borig * borig;
     }
@@ -419,6 +441,10 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
         s.bb = tot[1];
         const double t = fmax(G.rtol * sqrt(tot[1]), G.atol);
         s.tol2 = t * t;
+        s.tol2in = G.r32 ? fmax(s.tol2, G.eta * G.eta * tot[0]) : s.tol2;
+        s.outer = 0;
+        s.iters_prev = 0;
+        s.fin = 0;
         s.beta = 0.0;
         s.iters = 0;
         s.status = 0;
@@ -429,8 +455,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
 }
 
 // x = w D^-1 b ; r = b - A x on the smoothed rows of one level
-template <typename T, bool FINE>
-__global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const double *__restrict__ r0, const IScal *S)
+template <typename T, bool FINE, typename R = double>
+__global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const R *__restrict__ r0, const IScal *S)
 {
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
@@ -486,9 +512,9 @@ __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, c
 // output (or the CG residual when s is the finest level); level s's out is the
 // correction the regular prolongation reads.  Same arithmetic as the
 // level-synchronous kernels; the dense solve splits each row over a warp.
-template <typename T>
+template <typename T, typename R = double>
 __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, const TailInst<T> *TI,
-                                                        const double *__restrict__ r0, const IScal *S)
+                                                        const R *__restrict__ r0, const IScal *S)
 {
     __shared__ TailInst<T> ti;
     __shared__ VLev<T> L, Ln;
@@ -800,11 +826,13 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
     Ctl *c = G.ctl;
     for (int i = threadIdx.x; i < G.ninst; i += kBlock) {
         IScal &s = G.S[i];
-        if (!s.done) {   // stopped by the body cap: count as not converged
-            s.status = HF_ERR_NOT_CONVERGED;
+        // stopped by the body cap (or, mixed, by the sweep cap): not converged
+        if (G.r32 ? !s.fin : !s.done) {
+            if (s.status == 0) s.status = HF_ERR_NOT_CONVERGED;
             s.done = 1;
+            s.fin = 1;
         }
-        s.total_iters += s.iters;
+        s.total_iters += s.iters + s.iters_prev;
         if (s.status && atomicCAS(&c->err_status, 0, s.status) == 0) {
             c->err_inst = i;
             c->err_step = c->step;
@@ -816,5 +844,224 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
         c->step += 1;
         c->active = 0;
         c->bodies = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mixed form: FP32 inner CG on A e = r, FP64 refinement
+// ---------------------------------------------------------------------------
+// Each sweep runs the CG recurrences of the plain form in FP32 (vectors r32,
+// z32, q32, directions, e32; the finest operator's FP32 templates; the FP32
+// V-cycle) from e = 0 until ||r32|| <= max(eta ||r||, outer target) or the
+// sweep's iteration cap; then k_ir_correct adds e to the FP64 unknown and
+// updates the FP64 residual r -= A e with the FP64 operator, which decides
+// convergence against the plain form's test.  Dot products of FP32 vectors
+// are accumulated in FP64.
+
+// z32 from the V-cycle (finest post-smoothing or the tail's output), r.z
+__global__ void __launch_bounds__(kBlock) k_pcg_z32(PcgFine G, VLev<float> L0)
+{
+    Blk B;
+    if (pcg::load_blk(G.blk, G.S, B)) return;
+    const bool tail0 = G.S[B.inst].tail0;
+    const pcg::RowSet R = pcg::rowset(B);
+    float s[kRPT];
+    if (!tail0) pcg::trows(L0.At, R, s, [&](int j) { return L0.x[j]; });
+    double part[1] = {0.0};
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        if (q >= R.nrow) break;
+        const int i = R.row[q];
+        const float ri = G.r32[i];
+        const float z = tail0 ? L0.out[i] : L0.x[i] + L0.dinv[i] * (ri - s[q]);
+        G.z32[i] = z;
+        part[0] += (double)ri * (double)z;
+    }
+    double tot[1];
+    if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
+        IScal &s = G.S[B.inst];
+        s.beta = s.iters == 0 ? 0.0 : tot[0] / s.rz;
+        s.rz = tot[0];
+        if (!isfinite(tot[0])) { s.status = HF_ERR_NAN; pcg::finish_instance(s, G.ctl); }
+    }
+}
+
+// p = z + beta p_old ; q = A32 p ; alpha = r.z / p.q  (FP32 vectors)
+__global__ void __launch_bounds__(kBlock) k_pcg_dir32(PcgFine G, const float *__restrict__ po, float *__restrict__ pn)
+{
+    Blk B;
+    if (pcg::load_blk(G.blk, G.S, B)) return;
+    const IScal &sc = G.S[B.inst];
+    const bool first = sc.iters == 0;
+    const float beta = (float)sc.beta;
+    uint32_t d[kRPT];
+    pcg::row_descs(G.A32.rd, B, d);
+    __shared__ float sp[kStageRows];
+    const int s0 = B.row0 + B.pad0, ns = B.cnt + B.pad1 - B.pad0;
+    const bool staged = ns <= kStageRows;
+    if (staged) {
+        for (int j = threadIdx.x; j < ns; j += kBlock) sp[j] = first ? G.z32[s0 + j] : G.z32[s0 + j] + beta * po[s0 + j];
+        __syncthreads();
+    }
+    double part[1] = {0.0};
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        const int t = threadIdx.x + q * kBlock;
+        if (t >= B.cnt) break;
+        const int i = B.row0 + t;
+        float qi, p;
+        if (staged) {
+            qi = trow_d(G.A32, d[q], i, [&](int j) { return sp[j - s0]; });
+            p = sp[i - s0];
+        } else if (first) {
+            qi = trow_d(G.A32, d[q], i, [&](int j) { return G.z32[j]; });
+            p = G.z32[i];
+        } else {
+            qi = trow_d(G.A32, d[q], i, [&](int j) { return G.z32[j] + beta * po[j]; });
+            p = G.z32[i] + beta * po[i];
+        }
+        pn[i] = p;
+        G.q32[i] = qi;
+        part[0] += (double)p * (double)qi;
+    }
+    double tot[1];
+    if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
+        IScal &s = G.S[B.inst];
+        if (!isfinite(tot[0])) {
+            s.status = HF_ERR_NAN;
+            pcg::finish_instance(s, G.ctl);
+        } else if (!(tot[0] > 0.0)) {
+            // p.q <= 0: the FP32 recurrence is at its rounding level; the sweep
+            // ends and the FP64 correction decides
+            pcg::finish_instance(s, G.ctl);
+        } else {
+            s.alpha = s.rz / tot[0];
+        }
+    }
+}
+
+// e += alpha p ; r32 -= alpha q ; the sweep ends at its target or cap.  The
+// first update of a sweep overwrites e (e = alpha p): e is not cleared between
+// sweeps.  set_cond as in k_pcg_update.
+__global__ void __launch_bounds__(kBlock) k_pcg_update32(PcgFine G, const float *__restrict__ pn,
+                                                         cudaGraphConditionalHandle cond, int set_cond)
+{
+    Blk B;
+    const bool skip = pcg::load_blk(G.blk, G.S, B);
+    if (!skip) {
+        const IScal &sc = G.S[B.inst];
+        const float alpha = (float)sc.alpha;
+        const bool first = sc.iters == 0;
+        const pcg::RowSet R = pcg::rowset(B);
+        double part[1] = {0.0};
+#pragma unroll
+        for (int q = 0; q < kRPT; q++) {
+            if (q >= R.nrow) break;
+            const int i = R.row[q];
+            const float pv = pn[i], qv = G.q32[i];
+            G.e32[i] = (first ? 0.f : G.e32[i]) + alpha * pv;
+            const float r = G.r32[i] - alpha * qv;
+            G.r32[i] = r;
+            part[0] += (double)r * (double)r;
+        }
+        double tot[1];
+        if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
+            IScal &s = G.S[B.inst];
+            s.iters += 1;
+            if (!isfinite(tot[0])) { s.status = HF_ERR_NAN; pcg::finish_instance(s, G.ctl); }
+            else if (!(tot[0] > s.tol2in) || s.iters >= G.inner_maxit || s.iters + s.iters_prev >= G.maxit)
+                pcg::finish_instance(s, G.ctl);
+        }
+    }
+    if (!set_cond) return;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(&G.ctl->gcount, 1u);
+        if (t == gridDim.x - 1) {
+            __threadfence();
+            Ctl &c = *G.ctl;
+            c.gcount = 0;
+            c.bodies += 1;
+            const int active = ((volatile Ctl *)G.ctl)->active;
+            if (set_cond == 1) cudaGraphSetConditional(cond, (active > 0 && c.bodies < c.maxbodies) ? 1u : 0u);
+        }
+    }
+}
+
+// The FP64 refinement step after an inner sweep, on every instance not yet
+// finished: x += e, r -= A e (FP64 operator, FP64 arithmetic on the FP32 e),
+// ||r|| against the plain form's target; an instance above it starts another
+// sweep (last == 0) or is reported not converged (last != 0).  The last block
+// of the grid sets the next sweep's loop condition (set_next == 1) or leaves
+// the count for the host (eager launches).
+__global__ void __launch_bounds__(kBlock) k_ir_correct(PcgFine G, cudaGraphConditionalHandle next, int set_next,
+                                                       int last)
+{
+    __shared__ Blk sb;
+    __shared__ int sfin, sstat;
+    if (threadIdx.x == 0) {
+        sb = G.blk[blockIdx.x];
+        const volatile IScal &v = ((volatile IScal *)G.S)[sb.inst];
+        sfin = v.fin;
+        sstat = v.status;
+    }
+    __syncthreads();
+    const Blk B = sb;
+    if (!sfin) {
+        const int pt = G.projtype_all >= 0 ? G.projtype_all : G.ipar[B.inst].projtype;
+        double *x = pt == HF_INCREMENTAL ? G.dp : G.p;
+        const bool apply = sstat == 0;
+        double part[1] = {0.0};
+        uint32_t d[kRPT];
+        pcg::row_descs(G.A.rd, B, d);
+#pragma unroll
+        for (int q = 0; q < kRPT; q++) {
+            const int t = threadIdx.x + q * kBlock;
+            if (t >= B.cnt) break;
+            const int i = B.row0 + t;
+            double r = G.r[i];
+            if (apply) {
+                x[i] += (double)G.e32[i];
+                r -= trow_d(G.A, d[q], i, [&](int j) { return (double)G.e32[j]; });
+                G.r[i] = r;
+                G.r32[i] = (float)r;
+            }
+            part[0] += r * r;
+        }
+        double tot[1];
+        if (pcg::inst_sum<1>(part, B, G.partials, G.S, tot) && threadIdx.x == 0) {
+            IScal &s = G.S[B.inst];
+            s.rr = tot[0];
+            if (s.status != 0) {
+                s.fin = 1;
+            } else if (!isfinite(tot[0])) {
+                s.status = HF_ERR_NAN;
+                s.fin = 1;
+            } else if (!(tot[0] > s.tol2)) {
+                s.fin = 1;
+            } else if (last || s.iters + s.iters_prev >= G.maxit) {
+                s.status = HF_ERR_NOT_CONVERGED;
+                s.fin = 1;
+            } else {
+                s.outer += 1;
+                s.iters_prev += s.iters;
+                s.iters = 0;
+                s.beta = 0.0;
+                s.tol2in = fmax(s.tol2, G.eta * G.eta * tot[0]);
+                s.done = 0;
+                atomicAdd(&G.ctl->active, 1);
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(&G.ctl->gcount, 1u);
+        if (t == gridDim.x - 1) {
+            __threadfence();
+            Ctl &c = *G.ctl;
+            c.gcount = 0;
+            const int active = ((volatile Ctl *)G.ctl)->active;
+            if (set_next) cudaGraphSetConditional(next, active > 0 ? 1u : 0u);
+        }
     }
 }

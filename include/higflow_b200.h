@@ -75,10 +75,15 @@ enum { HF_EXPLICIT_EULER = 0, HF_EXPLICIT_RK2 = 1, HF_EXPLICIT_RK3 = 2, HF_SEMI_
 /* precision forms */
 enum {
     HF_PREC_FP64 = 0,   /* plain: every gather, update and Poisson iterate in FP64 */
-    HF_PREC_MIXED = 1   /* the AMG V-cycle preconditioner in FP32; the CG
-                           recurrences, the finest Poisson operator, stencil
-                           gathers, eigen/kernel transform and time update
-                           stay FP64 (same residual test as the plain form) */
+    HF_PREC_MIXED = 1   /* velocity-stage stencil rows with FP32 weights and
+                           FP32 accumulation; the Poisson solve as FP32 AMG-CG
+                           sweeps (operator, vectors, V-cycle in FP32) inside
+                           FP64 iterative refinement: after each sweep the
+                           FP64 unknown takes the correction and the FP64
+                           residual is updated with the FP64 operator, to the
+                           plain form's residual test; eigensystem, kernel
+                           transform and the velocity/pressure/conformation
+                           time updates stay FP64 */
 };
 
 /* Poisson preconditioner (CG path) */
@@ -290,7 +295,8 @@ typedef struct hf_options {
 typedef struct hf_stats {
     int64_t steps;            /* steps taken since create                      */
     int32_t last_iters;       /* Poisson iterations of the last step (inner)   */
-    int32_t last_outer;       /* refinement sweeps of the last step (mixed)    */
+    int32_t last_outer;       /* refinement sweeps of the last step (mixed:    */
+                              /* the most of any instance; plain: 1)           */
     double  last_residual;    /* relative true residual of the last solve      */
     int64_t total_iters;      /* all Poisson iterations since create           */
     int64_t kernel_launches;  /* kernels launched by hf_case_step so far       */
@@ -328,8 +334,8 @@ int  hf_case_solver_info(hf_case *c, int32_t *method, int32_t *nlev, int64_t *ro
 int  hf_case_launch_counts(hf_case *c, int32_t *per_step, int32_t *per_body);
 
 /* Batches: number of instances, and the last step's Poisson result of one
- * instance (iterations, refinement sweeps (always 1), status, relative
- * residual ||r|| / ||b||). */
+ * instance (iterations, all sweeps together; refinement sweeps (mixed form;
+ * 1 for the plain form); status; relative residual ||r|| / ||b||). */
 int  hf_case_instances(hf_case *c, int32_t *ninst);
 int  hf_case_instance_result(hf_case *c, int32_t inst, int32_t *iters, int32_t *outer, int32_t *status,
                              double *residual);
@@ -456,12 +462,14 @@ void hf_slv_destroy(hf_slv *s);                                                /
  * device buffer of 65536 rows (about 4.7 MB), for callers that cannot allocate
  * once running (an HBM budget fixed at start-up, or solves on one stream while
  * other streams of the device are busy, which cudaMalloc/cudaFree would stall).
- * Larger systems are rejected with HF_ERR_INVALID.  The first call on each
- * device looks the buffer up (cudaGetSymbolAddress, which may load the module)
- * and should come before any stream capture.  The buffer's reduction counter
- * must be zero when a call starts: it is zero at load and every call that
- * returns leaves it zero.  Calls that overlap (other threads or streams on the
- * same device) share the buffer and race: serialise them. */
+ * Larger systems are rejected with HF_ERR_INVALID.  The buffer's device address
+ * is looked up (cudaGetSymbolAddress, which may load the module) by the first
+ * call on each device and kept; that first call should come before any stream
+ * capture.  A call that fails with a CUDA error waits for its queued kernels
+ * when the stream still answers and drops the kept address; a device reset
+ * (cudaDeviceReset) between calls is not supported.  Each call clears the
+ * buffer's scalars before it starts.  Calls that overlap (other threads or
+ * streams on the same device) share the buffer and race: serialise them. */
 int  hf_slv_solve_device_noalloc(int32_t n, const int32_t *ptr, const int32_t *col, const double *val,
                                  const double *b, double *x, double rtol, double atol, int32_t maxit,
                                  void *stream, int32_t *iterations, double *residual);

@@ -10,7 +10,14 @@ mixed form against the FP64 oracle).
   rest (the whole configuration).
 * C4 subset: six instances of the batched Giesekus population (sides 32 to
   129), 20 steps from rest with the conformation at the identity, run as one
-  batch.
+  batch.  From the identity the reference's conformation is ill-conditioned
+  (its spin term divides by an eigenvalue gap plus 1e-12,
+  hig-flow-step-viscoelastic.c:1667): the fixture stores, per instance and
+  field, how far the reference's own fields move when its Poisson tolerance
+  goes from 1e-15 to 1e-13, and a field's bound is the larger of the
+  tolerance above and three times that sensitivity (it exceeds 1e-10 for the
+  side-129 instance's K, about 4e-6; every other field of every instance is
+  held to the plain bar).
 """
 import os
 
@@ -67,8 +74,9 @@ def test_c4_subset_batch_matches_reference(precision, tol):
         for k in range(4):
             got[f"K{k}"] = case.get_instance(hp.FIELD_KERNEL, k, j)
         err = {k: rel_l2(ref[f"ref{i}_{k}"], v) for k, v in got.items()}
-        worst[i] = max(err.values())
-        assert worst[i] < tol, (i, err)
+        bound = {k: max(tol, 3.0 * float(ref[f"sens{i}_{k}"])) for k in got}
+        worst[i] = max(err[k] / bound[k] for k in got)
+        assert worst[i] < 1.0, (i, err, bound)
     case.close()
 
 

@@ -3,7 +3,10 @@
 The system is a seeded sparse, non-symmetric, diagonally dominant matrix (the
 shape of a Poisson row set with convection-like asymmetry).  Both entry points
 run the same Jacobi-preconditioned BiCGStab to rtol 1e-12; the solutions must
-agree to 1e-10 relative L2, on two no-alloc calls in a row.
+agree to 1e-10 relative L2, on two no-alloc calls in a row, and the no-alloc
+solution must satisfy ||b - A x|| / ||b|| <= 1e-10 when the residual is
+recomputed on the host (scipy).  Sizes: a small system and one at the entry
+point's 65536-row limit.
 """
 import ctypes as C
 
@@ -81,10 +84,16 @@ def _allocating_solve(L, ptr, col, val, b, x0):
     return x
 
 
-def test_no_alloc_solve_matches_allocating_solver_twice():
+def _host_residual(ptr, col, val, x, b):
+    import scipy.sparse as sp
+    A = sp.csr_matrix((val, col, ptr), shape=(b.size, b.size))
+    return float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("n", [3000, 65536])
+def test_no_alloc_solve_matches_allocating_solver_twice(n):
     import torch
     L = _lib()
-    n = 3000
     ptr, col, val, b, x0 = _system(n)
     want = _allocating_solve(L, ptr, col, val, b, x0)
     dev = torch.device("cuda:0")
@@ -105,6 +114,7 @@ def test_no_alloc_solve_matches_allocating_solver_twice():
         err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err < TOL, (call, err)
         assert it.value > 0 and res.value <= 1e-11
+        assert _host_residual(ptr, col, val, got, b) <= 1e-10, call
 
 
 def test_no_alloc_rejects_oversize_system():
