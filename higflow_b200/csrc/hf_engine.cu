@@ -124,7 +124,16 @@ struct DevProg {
     const int32_t *cinst;
     const int32_t *finst[3];
     const double *ipinv;
+    // per-instance step limits (hf_case_set_step_limits): steps left, < 0 no
+    // limit; an instance at 0 is frozen: no kernel changes its fields.  Null
+    // until limits are set.
+    const int64_t *ilim;
 };
+
+__device__ __forceinline__ bool frozen(const DevProg &P, int inst)
+{
+    return P.ilim && __ldg(P.ilim + inst) == 0;
+}
 
 struct DevFields {
     double *u[3], *us[3], *p, *dp, *F, *FU[3];
@@ -398,7 +407,9 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 #define SLQ(s, fld) (val[s])
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
     const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
-    const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
+    const int inst = __ldg(pick<3>(P.finst, d) + f);
+    if (frozen(P, inst)) return;
+    const hf_params &par = P.ipar[inst];
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
     double conv1 = 0.0, conv2 = 0.0;
@@ -587,7 +598,9 @@ __global__ void __launch_bounds__(kBlock) k_gptt_ml(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     if (cc >= P.ncell) return;
-    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    const int inst = __ldg(P.cinst + cc);
+    if (frozen(P, inst)) return;
+    const hf_params &pr = P.ipar[inst];
     if (pr.ve_model != HF_GPTT) return;
     double trS = 0.0;
 #pragma unroll
@@ -608,7 +621,14 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #define CS(s) __ldg(P.cslots + (size_t)(s) * n + cc)
     const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
     const uint32_t fl = __ldg(P.cflags + cc);
-    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    const int inst = __ldg(P.cinst + cc);
+    if (frozen(P, inst)) {
+        // the stage's output replaces K after it (pointer swap): carry K over
+#pragma unroll
+        for (int k = 0; k < D * D; k++) F.Knew[k][cc] = F.K[k][cc];
+        return;
+    }
+    const hf_params &pr = P.ipar[inst];
     // The velocity values this cell reads: its face velocities (u[dim] at
     // -/+ half a cell, UVL/UVR) and the Du corner queries (HF_C_NQ per ordered
     // pair dim != dim2, on u[dim]).  All slot codes, then all values as
@@ -859,7 +879,9 @@ __global__ void __launch_bounds__(kBlock) k_ve_stress(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     if (cc >= P.ncell) return;
-    const hf_params &pr = P.ipar[__ldg(P.cinst + cc)];
+    const int inst = __ldg(P.cinst + cc);
+    if (frozen(P, inst)) return;
+    const hf_params &pr = P.ipar[inst];
     const double Re = pr.Re, De = pr.De;
     double Knew[D][D], Du[D][D];
 #pragma unroll
@@ -1060,6 +1082,7 @@ __global__ void __launch_bounds__(kBlock) k_rk_combine(DevProg P, DevFields F, i
 #pragma unroll
     for (int k = 1; k < D; k++) d += (e >= P.off[k]);
     const int f = e - pick<4>(P.off, d);
+    if (frozen(P, __ldg(pick<3>(P.finst, d) + f))) return;
     const double u = pick<3>(F.u, d)[f], ustar = pick<3>(F.us, d)[f];
     if (which == 0) pick<3>(F.us, d)[f] = 0.5 * (u + ustar);
     else pick<3>(F.us, d)[f] = u / 3.0 + 2.0 * ustar / 3.0;
@@ -1160,7 +1183,9 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
         for (int k = 1; k < D; k++) d += (e >= P.off[k]);
         const int f = e - pick<4>(P.off, d);
         const int nf = pick<3>(P.nf, d);
-        const hf_params &par = P.ipar[__ldg(pick<3>(P.finst, d) + f)];
+        const int inst = __ldg(pick<3>(P.finst, d) + f);
+        if (frozen(P, inst)) return;
+        const hf_params &par = P.ipar[inst];
         const int pt = P.projtype_all >= 0 ? P.projtype_all : par.projtype;
         const double *pp = pt == HF_INCREMENTAL ? F.dp : F.p;
         const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
@@ -1172,7 +1197,7 @@ __global__ void __launch_bounds__(kBlock) k_final(DevProg P, DevFields F)
         pick<3>(F.u, d)[f] = __ldg(pick<3>(F.us, d) + f) - par.dt * dpdx;
     } else {
         const int c = e - P.off[D];
-        if (c < P.ncell &&
+        if (c < P.ncell && !frozen(P, __ldg(P.cinst + c)) &&
             (P.projtype_all >= 0 ? P.projtype_all : P.ipar[__ldg(P.cinst + c)].projtype) == HF_INCREMENTAL)
             F.p[c] = F.p[c] + F.dp[c];
     }
@@ -1278,6 +1303,7 @@ struct hf_case {
     cudaGraphExec_t exec[2] = {};
     int64_t ntemplates = 0;         // row templates of the finest Poisson operator
     int64_t vel_entries = 0;        // stored entries of the velocity-stage rows (padded slices)
+    int64_t *ilim = nullptr;        // per-instance step limits on the device (null: none)
     bool graph_profile = false;     // graphs were captured with phase events
     bool phase_pending = false;     // a profiled step's events are not read yet
     bool capturing = false;         // a step graph is being captured
@@ -2285,8 +2311,9 @@ void enqueue_post(hf_case *C, const DevFields &F, int &fixed)
     cudaStream_t st = C->stream;
     record(C, HF_PHASE_POISSON_ITER, 1);
     record(C, HF_PHASE_FINAL, 0);
-    k_step_end<<<1, kBlock, 0, st>>>(C->G);
+    // (k_final first: k_step_end counts the instances' step limits down)
     k_final<D><<<blocks(C->nfacet_total + C->P.ncell), kBlock, 0, st>>>(C->P, F);
+    k_step_end<<<1, kBlock, 0, st>>>(C->G);
     record(C, HF_PHASE_FINAL, 1);
     fixed += 2;
 }
@@ -3250,6 +3277,30 @@ extern "C" int hf_case_set_timestep(hf_case *C, const double *dt, int32_t n)
     HF_CK(cudaStreamSynchronize(C->stream));
     C->par.dt = C->h_ipar[0].dt;
     C->P.par.dt = C->h_ipar[0].dt;
+    return HF_OK;
+}
+
+extern "C" int hf_case_set_step_limits(hf_case *C, const int64_t *steps, int32_t n)
+{
+    if (!C || !steps) return fail(HF_ERR_INVALID, "null argument");
+    if (n != C->ninst) return fail(HF_ERR_INVALID, "array size is not the instance count");
+    if (!C->use_cg || C->sie) return fail(HF_ERR_UNSUPPORTED, "step limits need the CG Poisson path and an explicit velocity");
+    std::vector<int64_t> h(steps, steps + n);
+    for (int64_t &v : h)
+        if (v < 0) v = -1;
+    HF_CK(cudaStreamSynchronize(C->stream));   // no step of this case in flight
+    if (!C->ilim) {
+        double bytes = 0;
+        int rc = upload(C->owned, &C->ilim, h.data(), h.size(), bytes, C->stream);
+        if (rc) return rc;
+        C->bytes += bytes;
+        C->P.ilim = C->ilim;
+        C->G.ilim = C->ilim;
+        destroy_graphs(C);   // the captured kernels hold the parameters without limits
+    } else {
+        HF_CK(cudaMemcpyAsync(C->ilim, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, C->stream));
+    }
+    HF_CK(cudaStreamSynchronize(C->stream));
     return HF_OK;
 }
 

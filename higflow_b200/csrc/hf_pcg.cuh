@@ -207,6 +207,9 @@ struct PcgFine {
     // each sweep (k_ir_correct); r32 is null in the plain form
     TRows<float> A32;
     float *r32, *z32, *q32, *e32;
+    // per-instance step limits (DevProg::ilim): a frozen instance (0 steps
+    // left) takes no part in the step's solve; null when no limits are set
+    int64_t *ilim;
     double eta;               // inner sweep target: ||r_in|| <= eta ||r|| (or the outer target)
     int inner_maxit;          // iterations per inner sweep
 };
@@ -397,6 +400,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
 {
     Blk B;
     pcg::load_blk(G.blk, G.S, B);   // a new solve: the done flags are reset here
+    // a frozen instance keeps done (and fin) from its last solve
+    if (G.ilim && G.ilim[B.inst] == 0) return;
     const hf_params &par = G.ipar[B.inst];
     const bool incr = par.projtype == HF_INCREMENTAL;
     const double *x = incr ? G.dp : G.p;
@@ -441,7 +446,9 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
         s.bb = tot[1];
         const double t = fmax(G.rtol * sqrt(tot[1]), G.atol);
         s.tol2 = t * t;
-        s.tol2in = G.r32 ? fmax(s.tol2, G.eta * G.eta * tot[0]) : s.tol2;
+        // the inner sweep aims at half the outer target (its FP32 recurrence
+        // drifts from the true residual), or eta of where it starts
+        s.tol2in = G.r32 ? fmax(0.25 * s.tol2, G.eta * G.eta * tot[0]) : s.tol2;
         s.outer = 0;
         s.iters_prev = 0;
         s.fin = 0;
@@ -801,6 +808,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_extrapolate(PcgFine G)
     if (i >= G.n) return;
     // (the instance lookup only when the instances differ in projection
     // type: it would delay every load behind two dependent ones)
+    if (G.ilim && G.ilim[__ldg(G.cinst + i)] == 0) return;
     const int pt = G.projtype_all >= 0 ? G.projtype_all : __ldg(&G.ipar[__ldg(G.cinst + i)].projtype);
     double *x = pt == HF_INCREMENTAL ? G.dp : G.p;
     const double xn = x[i], xpv = G.xprev[i];
@@ -826,6 +834,10 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
     Ctl *c = G.ctl;
     for (int i = threadIdx.x; i < G.ninst; i += kBlock) {
         IScal &s = G.S[i];
+        if (G.ilim) {
+            if (G.ilim[i] == 0) continue;   // frozen during this step
+            if (G.ilim[i] > 0) G.ilim[i] -= 1;
+        }
         // stopped by the body cap (or, mixed, by the sweep cap): not converged
         if (G.r32 ? !s.fin : !s.done) {
             if (s.status == 0) s.status = HF_ERR_NOT_CONVERGED;
@@ -852,8 +864,9 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
 // ---------------------------------------------------------------------------
 // Each sweep runs the CG recurrences of the plain form in FP32 (vectors r32,
 // z32, q32, directions, e32; the finest operator's FP32 templates; the FP32
-// V-cycle) from e = 0 until ||r32|| <= max(eta ||r||, outer target) or the
-// sweep's iteration cap; then k_ir_correct adds e to the FP64 unknown and
+// V-cycle) from e = 0 until ||r32|| <= max(eta ||r||, outer target / 2) or the
+// sweep's iteration cap (the sweep aims at half the outer target, so that one
+// correction usually meets it); then k_ir_correct adds e to the FP64 unknown and
 // updates the FP64 residual r -= A e with the FP64 operator, which decides
 // convergence against the plain form's test.  Dot products of FP32 vectors
 // are accumulated in FP64.
@@ -1047,7 +1060,7 @@ __global__ void __launch_bounds__(kBlock) k_ir_correct(PcgFine G, cudaGraphCondi
                 s.iters_prev += s.iters;
                 s.iters = 0;
                 s.beta = 0.0;
-                s.tol2in = fmax(s.tol2, G.eta * G.eta * tot[0]);
+                s.tol2in = fmax(0.25 * s.tol2, G.eta * G.eta * tot[0]);
                 s.done = 0;
                 atomicAdd(&G.ctl->active, 1);
             }

@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.hf_case_launch_counts.argtypes = [V, P(C.c_int32), P(C.c_int32)]
         L.hf_case_instance_iters.argtypes = [V, P(C.c_int64), C.c_int32]
         L.hf_case_adjust_timestep.argtypes = [V, P(C.c_double), P(C.c_double), C.c_int32]
+        L.hf_case_set_timestep.argtypes = [V, P(C.c_double), C.c_int32]
+        L.hf_case_set_step_limits.argtypes = [V, P(C.c_int64), C.c_int32]
         L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
         L.hf_case_synchronize.argtypes = [V]
         L.hf_case_destroy.argtypes = [V]
@@ -130,6 +132,15 @@ class Case:
         _check(lib().hf_case_adjust_timestep(self.h, cfl.ctypes.data_as(C.POINTER(C.c_double)),
                                              dt.ctypes.data_as(C.POINTER(C.c_double)), n))
         return cfl, dt
+
+    def set_step_limits(self, steps) -> None:
+        """Instance i takes steps[i] more steps, then stays as it is (< 0: no limit)."""
+        a = np.ascontiguousarray(steps, dtype=np.int64)
+        _check(lib().hf_case_set_step_limits(self.h, a.ctypes.data_as(C.POINTER(C.c_int64)), a.size))
+
+    def set_timestep(self, dt) -> None:
+        a = np.ascontiguousarray(np.atleast_1d(dt), dtype=np.float64)
+        _check(lib().hf_case_set_timestep(self.h, a.ctypes.data_as(C.POINTER(C.c_double)), a.size))
 
     def launch_counts(self):
         """(kernels per step outside the Poisson loop, kernels per loop body)."""

@@ -222,24 +222,33 @@ class CaseSpec:
                 s += " ".join(str(x) for x in init) + " " + " ".join(str(x) for x in size) + "\n"
         return s
 
+    def trees(self):
+        """(lo, hi, cells per axis, refinement levels) of each tree."""
+        return [(self.lo, self.hi, self.n, self.refine)]
+
+    def face_box(self, face):
+        """(lo, hi, cells per axis, normal axis) of a boundary: a face of the box."""
+        ax, side = face["axis"], face["side"]
+        lo = list(self.lo)
+        hi = list(self.hi)
+        if side == 0:
+            hi[ax] = lo[ax]
+        else:
+            lo[ax] = hi[ax]
+        return lo, hi, [self.n[k] if k != ax else 1 for k in range(self.dim)], ax
+
     def write(self, d: str) -> str:
         name = os.path.join(d, "case")
-        with open(os.path.join(d, "dom0.amr"), "w") as f:
-            f.write(self._amr(self.lo, self.hi, self.n, self.refine))
+        paths = []
+        for t, (lo, hi, n, refine) in enumerate(self.trees()):
+            paths.append(os.path.join(d, f"dom{t}.amr"))
+            with open(paths[-1], "w") as f:
+                f.write(self._amr(lo, hi, n, refine))
         with open(name + ".domain", "w") as f:
-            f.write("1\n" + os.path.join(d, "dom0.amr") + "\n")
+            f.write(f"{len(paths)}\n" + "".join(p + "\n" for p in paths))
         lines = [str(len(self.faces))]
         for b, face in enumerate(self.faces):
-            ax, side = face["axis"], face["side"]
-            lo = list(self.lo)
-            hi = list(self.hi)
-            n = list(self.n)
-            if side == 0:
-                hi[ax] = lo[ax]
-            else:
-                lo[ax] = hi[ax]
-            n[ax] = 1
-            nb = [n[k] if k != ax else 1 for k in range(self.dim)]
+            lo, hi, nb, ax = self.face_box(face)
             # degenerate axis: delta 0 (as in higflow/example2d_Newt/amrs/bc/*.amr)
             s = " ".join(f"{lo[k]!r} {hi[k]!r}" for k in range(self.dim)) + "\n1\n"
             delta = [0.0 if k == ax else (hi[k] - lo[k]) / nb[k] for k in range(self.dim)]
@@ -337,3 +346,66 @@ def channel(nx: int = 32, ny: int = 8, length: float = 8.0, half: float = 1.0, u
         dict(axis=1, side=1, p="N", u="D", uval=[0.0, 0.0]),
     ]
     return CaseSpec(2, [nx, ny], [0.0, -half], [length, half], faces, **par)
+
+
+class TreesSpec(CaseSpec):
+    """A domain of several trees (boxes, each with its own refinement levels)
+    and explicit boundary boxes: ``trees`` = [dict(lo, hi, n, refine=[...])],
+    ``faces`` = [dict(lo, hi, n, axis, p, u, uval, upar, tdim, c, h, p_val)]
+    with ``n`` the boundary's cells per axis (1 along its normal ``axis``)."""
+
+    def __init__(self, dim: int, trees: Sequence[dict], faces: Sequence[dict], **par):
+        t0 = trees[0]
+        super().__init__(dim, t0["n"], t0["lo"], t0["hi"], faces, **par)
+        self.tree_list = [dict(t) for t in trees]
+
+    def trees(self):
+        return [(t["lo"], t["hi"], t["n"], t.get("refine", [])) for t in self.tree_list]
+
+    def face_box(self, face):
+        return list(face["lo"]), list(face["hi"]), list(face["n"]), face["axis"]
+
+    def cells(self) -> int:
+        return int(sum(int(np.prod(t["n"])) for t in self.tree_list))
+
+    def geometry_key(self) -> str:
+        p = self.host_params()
+        for k in _PHYSICAL:
+            setattr(p, k, 0.0)
+        h = hashlib.sha256()
+        h.update(repr((self.dim, self.tree_list, self.faces)).encode())
+        h.update(bytes(p))
+        return h.hexdigest()[:32]
+
+
+def contraction(per_unit: int = 32, band: float = 0.125, refine: bool = True, umax: float = 1.5, **par) -> TreesSpec:
+    """The 2D 4:1 planar contraction of higflow/example2d_Newt_contraction (two
+    trees: upstream [-16,0] x [-4,4], downstream [0,16] x [-1,1]; its eight
+    boundaries), at ``per_unit`` cells per unit length, with a second level
+    (half the cell size) on squares of side 2 ``band`` centred on the
+    contraction corners (0, +-1) (``band`` = 1/16 of the downstream width
+    2 by default).  Parabolic inflow umax (1 - (y/4)^2) (mean umax 2/3) at
+    x = -16, no-slip walls, outflow at x = 16 (pressure Dirichlet 0,
+    velocity Neumann)."""
+    h = 1.0 / per_unit
+    up = dict(lo=[-16.0, -4.0], hi=[0.0, 4.0], n=[16 * per_unit, 8 * per_unit])
+    dn = dict(lo=[0.0, -1.0], hi=[16.0, 1.0], n=[16 * per_unit, 2 * per_unit])
+    if refine:
+        b = int(round(band * 2 * per_unit))      # band in level-2 cells
+        # level-2 patches (init, size) in level-2 cell units of each tree
+        up["refine"] = [([h / 2, h / 2], [((32 * per_unit - b, (3 * per_unit) * 2 - b), (b, 2 * b)),
+                                          ((32 * per_unit - b, (5 * per_unit) * 2 - b), (b, 2 * b))])]
+        dn["refine"] = [([h / 2, h / 2], [((0, 4 * per_unit - b), (b, b)), ((0, 0), (b, b))])]
+    wall = dict(p="N", u="D", uval=[0.0, 0.0])
+    faces = [
+        dict(lo=[-16.0, -4.0], hi=[-16.0, 4.0], n=[1, 8 * per_unit], axis=0, p="N", u="D", uval=[0.0, 0.0],
+             upar=[umax, 0.0], tdim=1, c=0.0, h=4.0),
+        dict(lo=[-16.0, 4.0], hi=[0.0, 4.0], n=[16 * per_unit, 1], axis=1, **wall),
+        dict(lo=[0.0, 1.0], hi=[0.0, 4.0], n=[1, 3 * per_unit], axis=0, **wall),
+        dict(lo=[0.0, 1.0], hi=[16.0, 1.0], n=[16 * per_unit, 1], axis=1, **wall),
+        dict(lo=[16.0, -1.0], hi=[16.0, 1.0], n=[1, 2 * per_unit], axis=0, p="D", u="N", uval=[0.0, 0.0]),
+        dict(lo=[0.0, -1.0], hi=[16.0, -1.0], n=[16 * per_unit, 1], axis=1, **wall),
+        dict(lo=[0.0, -4.0], hi=[0.0, -1.0], n=[1, 3 * per_unit], axis=0, **wall),
+        dict(lo=[-16.0, -4.0], hi=[0.0, -4.0], n=[16 * per_unit, 1], axis=1, **wall),
+    ]
+    return TreesSpec(2, [up, dn], faces, **par)

@@ -59,8 +59,11 @@ def batched_giesekus(count: int = 256, seed: int = 0) -> List[CaseDraw]:
 def served_stream(seed: int = 0, rate: float = 50.0, window_s: float = 60.0):
     """Poisson arrivals at ``rate`` per second over ``window_s``: 40% Newtonian
     cavities, 40% Oldroyd-B cavities (Wi uniform [0.1, 1.5]), 20% Giesekus
-    (alpha uniform [0, 0.5], Wi uniform [0.1, 1.5]); side N log-uniform in
-    [64, 512]; 500-5000 steps.  Inter-arrival times are drawn first."""
+    channels (alpha uniform [0, 0.5], Wi uniform [0.1, 1.5]; the channel of the
+    shipped example2d_Newt case); side N log-uniform in [64, 512] (a channel
+    has 2N x N/2 cells); 500-5000 steps.  Inter-arrival times are drawn
+    first; the time step of every draw is the cavity's explicit bound at its
+    side (the channel's cells are larger, so it is within the channel's)."""
     rng = np.random.default_rng(seed)
     t, times = 0.0, []
     while True:
@@ -82,21 +85,35 @@ def served_stream(seed: int = 0, rate: float = 50.0, window_s: float = 60.0):
         else:
             cases.append(CaseDraw(n=n, model=hp.GIESEKUS, De=float(rng.uniform(0.1, 1.5)),
                                   alpha=float(rng.uniform(0.0, 0.5)), beta=0.1, Re=1.0,
-                                  dt=explicit_dt(n, 1.0), steps=steps))
+                                  dt=explicit_dt(n, 1.0), steps=steps, geometry="channel"))
     return times, cases
 
 
-def served_requests(count: int = 64, step_scale: float = 1.0 / 50.0, seed: int = 0):
+def served_requests(count: int = 48, step_scale: float = 1.0, seed: int = 0):
     """The first ``count`` requests of the served stream, step counts scaled by
     ``step_scale`` (at least 1): [(arrival s, CaseDraw)].  The stream's offered
-    load (about 8.5e9 cell-steps/s) is far above one device; the bounded sample
-    keeps arrivals, sizes and the mix of the stream and makes the run finish."""
+    load (about 8.5e9 cell-steps/s over its 60 s window, some 5e11 cell-steps)
+    is far above one device; the bounded prefix keeps arrivals, sizes, step
+    counts and the mix of the stream and makes the run finish."""
     times, cases = served_stream(seed=seed)
     out = []
     for t, c in list(zip(times, cases))[:count]:
         c = CaseDraw(**{**c.__dict__, "steps": max(1, int(round(c.steps * step_scale)))})
         out.append((t, c))
     return out
+
+
+def contraction_c2(per_unit: int = 32) -> host.TreesSpec:
+    """The 2D Oldroyd-B 4:1 planar contraction configuration: two trees of the
+    shipped contraction case at ``per_unit`` cells per unit length (32: 163,840
+    cells plus the refined corner squares), Re 0.01, Wi 1.0, beta 1/9,
+    log-conformation from the identity, parabolic inflow of mean 1, dt 5e-5.
+    The velocity is semi-implicit Euler: explicit Euler at this dt violates the
+    explicit viscous bound dt <= Re h^2 / 4 (about 2.4e-6 at h = 1/32) and
+    diverges in the reference too."""
+    return host.contraction(per_unit, Re=0.01, dt=5e-5, flowtype=hp.VISCOELASTIC, ve_model=hp.OLDROYD_B, De=1.0,
+                            beta=1.0 / 9.0, kernel=hp.KERNEL_LOG, kernel_tol=1e-2,
+                            tempdiscrtype=hp.SEMI_IMPLICIT_EULER)
 
 
 def partition(costs, parts: int) -> List[List[int]]:

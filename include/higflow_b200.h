@@ -358,6 +358,15 @@ int  hf_case_adjust_timestep(hf_case *c, double *cfl, double *dt, int32_t n);
  * semi-implicit velocity when dt changes (its system matrix holds dt). */
 int  hf_case_set_timestep(hf_case *c, const double *dt, int32_t n);
 
+/* Per-instance step limits (no counterpart in the reference, which runs one
+ * case per job): instance i takes steps[i] more steps and is then frozen (no
+ * kernel changes its fields) while the others go on; steps[i] < 0: no limit.
+ * n = ninst.  Each frozen instance's fields stay those of its last step, so
+ * its result is the same as when it runs alone for steps[i] steps.  Needs the
+ * CG Poisson path and an explicit velocity scheme (HF_ERR_UNSUPPORTED
+ * otherwise). */
+int  hf_case_set_step_limits(hf_case *c, const int64_t *steps, int32_t n);
+
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);
 

@@ -95,3 +95,25 @@ def test_eager_launches_match_the_step_graph():
         case.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("precision", [hp.PREC_FP64, hp.PREC_MIXED])
+def test_step_limits_freeze_each_instance_at_its_count(precision):
+    """hf_case_set_step_limits: instance i takes limits[i] steps and is then
+    frozen while the batch goes on; its fields equal the instance run alone
+    for limits[i] steps (1e-10 relative L2), in both precision forms."""
+    names = VE_NAMES[:4]
+    limits = [1, 4, 2, 6]
+    progs, datas = zip(*[load_golden(n) for n in names])
+    batch = hp.Program.concatenate(progs)
+    case = engine.Case(batch, engine.options(rtol=1e-13, atol=1e-300, precision=precision))
+    for key, fid, comp in field_keys(progs[0]):
+        case.set(fid, comp, np.concatenate([d["init_" + key] for d in datas]))
+    case.set_step_limits(limits)
+    case.step(max(limits) + 2)
+    for i, (name, prog) in enumerate(zip(names, progs)):
+        alone = _run_alone(name, limits[i], precision=precision)
+        got = {k: case.get_instance(fid, comp, i) for k, fid, comp in field_keys(prog)}
+        err = compare(got, alone, _keys(prog))
+        assert max(err.values()) < 1e-10, (name, limits[i], err)
+    case.close()

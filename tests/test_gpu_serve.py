@@ -1,6 +1,8 @@
 """Serving (hf_server_*): requests admitted while others run, each one the same
 alone and in the mix, bit for bit (every request is an engine case of its own
 with deterministic kernels; tolerance 0)."""
+import time
+
 import numpy as np
 import pytest
 
@@ -78,3 +80,38 @@ def test_a_failing_request_does_not_disturb_the_others():
     for rid in ids:
         srv.release(rid)
     srv.close()
+
+
+def test_batch_server_results_are_the_same_alone_and_in_the_mix():
+    """Continuous batching (higflow_b200.serve.BatchServer): requests submitted
+    while others run are grouped into cohorts that step as one batch, each
+    request frozen at its own step count.  Every result equals the request run
+    alone as an engine case for its steps (1e-10 relative L2, plain FP64)."""
+    from higflow_b200 import serve
+    reqs = _requests()
+    opts = engine.options(rtol=1e-13, atol=1e-300)
+    srv = serve.BatchServer(opts=opts, max_cohorts=3, chunk=3)
+    ids = []
+    for k, (prog, _, steps, fields) in enumerate(reqs):
+        ids.append(srv.submit(prog, steps, fields))
+        if k == 2:
+            time.sleep(0.05)       # the later ones arrive while the first cohort runs
+    got = []
+    for rid, (prog, _, _, _) in zip(ids, reqs):
+        status, q, t = srv.wait(rid, timeout=300)
+        assert status == 0
+        got.append({k: srv.get(rid, *k) for k in _fields(lambda f, c: None, prog)})
+        srv.release(rid)
+    st = srv.stats()
+    srv.close()
+    assert st["cohorts"] >= 2
+    for (prog, _, steps, fields), mix in zip(reqs, got):
+        case = engine.Case(prog, opts)
+        for key, v in fields.items():
+            case.set(*key, v)
+        case.step(steps)
+        alone = _fields(case.get, prog)
+        case.close()
+        for k in alone:
+            err = np.linalg.norm(alone[k] - mix[k]) / max(np.linalg.norm(alone[k]), 1e-300)
+            assert err < 1e-10, (k, err)
