@@ -249,22 +249,30 @@ __device__ __noinline__ void implicit_kernel_solve(const double *Om, double dt, 
     }
 }
 
+// FLT_EQ of higtree/src/utils.h:40 in the arithmetic type
+template <typename T>
+__device__ __forceinline__ bool flt_eq(T x, T y)
+{
+    return fabs(x - y) < T(HF_EPSMACH);
+}
+
 // hig_flow_convective_cell_term_cubista (hig-flow-step.c:1185-1358).  Out of
 // line: the VE cell stage calls it D(D+1)/2 x D times, and six inlined copies
 // of its branches made that kernel instruction-fetch bound (1.74 -> 1.38 ms on
 // 4.29 M cells with one shared copy).
-__device__ __noinline__ double cubista_cell(double kl, double kr, double kll, double krr, int il, int ir,
-                                      int ill, int irr, double vl, double vr, double kc, double cdelta)
+template <typename T>
+__device__ __noinline__ T cubista_cell_t(T kl, T kr, T kll, T krr, int il, int ir, int ill, int irr, T vl, T vr, T kc,
+                                       T cdelta)
 {
-    const double a = 1.7500, b = 0.3750, c = 0.7500, d = 0.1250, e = 0.2500;
-    double vbar, fi, conv1 = 0.0, conv2 = 0.0;
+    const T a = T(1.7500), b = T(0.3750), c = T(0.7500), d = T(0.1250), e = T(0.2500);
+    T vbar, fi, conv1 = T(0), conv2 = T(0);
     vbar = vr;
-    if (vbar > 0.0) {
-        if (HF_FLT_EQ(kr, kl)) {
+    if (vbar > T(0)) {
+        if (flt_eq(kr, kl)) {
             conv1 = vbar * kc;
         } else {
             fi = (kc - kl) / (kr - kl);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv1 = vbar * kc;
             } else {
                 if (fi < b) conv1 = il == 1 ? vbar * (a * kc - c * kl) : vbar * kc;
@@ -274,11 +282,11 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
         }
     } else {
         if ((ir == 1) && (irr == 1)) {
-            if (HF_FLT_EQ(kc, krr)) {
+            if (flt_eq(kc, krr)) {
                 conv1 = vbar * kr;
             } else {
                 fi = (kr - krr) / (kc - krr);
-                if ((fi <= 0.0) || (fi >= 1.0)) {
+                if ((fi <= T(0)) || (fi >= T(1))) {
                     conv1 = vbar * kr;
                 } else {
                     if (fi < b) conv1 = vbar * (a * kr - c * krr);
@@ -287,11 +295,11 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
                 }
             }
         } else if ((ir == 1) && (irr == 0)) {
-            if (HF_FLT_EQ(kc, krr)) {
+            if (flt_eq(kc, krr)) {
                 conv1 = vbar * kr;
             } else {
                 fi = (kr - krr) / (kc - krr);
-                if ((fi <= 0.0) || (fi >= 1.0)) {
+                if ((fi <= T(0)) || (fi >= T(1))) {
                     conv1 = vbar * kr;
                 } else {
                     if (fi <= c) conv1 = vbar * kr;
@@ -301,18 +309,18 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
         } else {
             conv1 = vr * kc;
             vbar = vl;
-            conv2 = vbar > 0.0 ? vbar * kl : vbar * kc;
+            conv2 = vbar > T(0) ? vbar * kl : vbar * kc;
             return ((conv1 - conv2) / cdelta);
         }
     }
     vbar = vl;
-    if (vbar > 0.0) {
+    if (vbar > T(0)) {
         if ((il == 1) && (ill == 1)) {
-            if (HF_FLT_EQ(kc, kll)) {
+            if (flt_eq(kc, kll)) {
                 conv2 = vbar * kl;
             } else {
                 fi = (kl - kll) / (kc - kll);
-                if ((fi <= 0.0) || (fi >= 1.0)) {
+                if ((fi <= T(0)) || (fi >= T(1))) {
                     conv2 = vbar * kl;
                 } else {
                     if (fi < b) conv2 = vbar * (a * kl - c * kll);
@@ -321,11 +329,11 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
                 }
             }
         } else if ((il == 1) && (ill == 0)) {
-            if (HF_FLT_EQ(kc, kll)) {
+            if (flt_eq(kc, kll)) {
                 conv2 = vbar * kl;
             } else {
                 fi = (kl - kll) / (kc - kll);
-                if ((fi <= 0.0) || (fi >= 1.0)) {
+                if ((fi <= T(0)) || (fi >= T(1))) {
                     conv2 = vbar * kl;
                 } else {
                     if (fi <= c) conv2 = vbar * kl;
@@ -333,16 +341,16 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
                 }
             }
         } else {
-            conv1 = vr > 0.0 ? vr * kc : vr * kr;
+            conv1 = vr > T(0) ? vr * kc : vr * kr;
             conv2 = vl * kc;
             return ((conv1 - conv2) / cdelta);
         }
     } else {
-        if (HF_FLT_EQ(kl, kr)) {
+        if (flt_eq(kl, kr)) {
             conv2 = vbar * kc;
         } else {
             fi = (kc - kr) / (kl - kr);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv2 = vbar * kc;
             } else {
                 if (fi < b) conv2 = ir == 1 ? vbar * (a * kc - c * kr) : vbar * kc;
@@ -352,6 +360,14 @@ __device__ __noinline__ double cubista_cell(double kl, double kr, double kll, do
         }
     }
     return ((conv1 - conv2) / cdelta);
+}
+
+// (the FP64 instantiation is the reference's arithmetic; the mixed form
+// takes the FP32 one)
+__device__ __forceinline__ double cubista_cell(double kl, double kr, double kll, double krr, int il, int ir, int ill,
+                                               int irr, double vl, double vr, double kc, double cdelta)
+{
+    return cubista_cell_t<double>(kl, kr, kll, krr, il, ir, ill, irr, vl, vr, kc, cdelta);
 }
 
 // ---------------------------------------------------------------------------

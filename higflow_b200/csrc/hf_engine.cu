@@ -96,6 +96,12 @@ struct DevProg {
     const int32_t *scol;
     const double *sw;
     const float *sw32;
+    // the columns as 16-bit offsets from the pair's first column (pcol0), when
+    // every pair's entries lie within +-32767 of it (interpolation stencils
+    // are local: 2D meshes up to several thousand cells a side); scol16 null
+    // otherwise
+    const int16_t *scol16;
+    const int32_t *pcol0;
     // semi-implicit Euler: the velocity kernel writes each direction's
     // right-hand side, u + dt (sources - grad p [+ div S] - conv) plus the
     // system's boundary part sie_bc, into sie_b instead of u*
@@ -289,12 +295,13 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 // or 128-byte (FP32) weight load; the sum is dp_interpolate_from_stencil's
 // (pdomain.c:1026-1053): -rhs, then the entries in stencil order.  W = float
 // is the mixed form: FP32 weights and field values, FP32 accumulation.
-template <typename W>
+template <typename W, bool C16>
 __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= P.nvrows) return;
     const double *__restrict__ fb = vtag_field(F, __ldg(P.vtag + u));
+    if (C16) fb += __ldg(P.pcol0 + u);
     const int n = __ldg(P.plen + u);
     const int64_t e0 = __ldg(P.sptr + (u >> 5)) + (u & 31);
     const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)P.sw32 : (const W *)P.sw;
@@ -303,7 +310,8 @@ __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
 #pragma unroll 4
     for (int k = 0; k < n; k++) {
         const int64_t at = e0 + 32 * (int64_t)k;
-        res += (W)__ldg(fb + __ldg(P.scol + at)) * __ldg(w + at);
+        const int c = C16 ? (int)__ldg(P.scol16 + at) : __ldg(P.scol + at);
+        res += (W)__ldg(fb + c) * __ldg(w + at);
     }
     P.rowval[u] = (double)res;
 }
@@ -313,17 +321,17 @@ __global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
 // would otherwise carry one inlined copy of these branches per direction.
 // conv1 / conv2 come in with the previous direction's values, as in the
 // reference, where a NaN ratio leaves them unassigned.
-__device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double ur, double ull, double urr,
-                                              int infll, int infrr, double vcr, double vcl, double conv1,
-                                              double conv2)
+template <typename T>
+__device__ __noinline__ void cubista_facet_t(T ufacet, T ul, T ur, T ull, T urr, int infll, int infrr, T vcr, T vcl,
+                                             T &conv1, T &conv2)
 {
-    const double a = 1.7500, b = 0.3750, c = 0.7500, dd = 0.1250, ee = 0.2500;
-    if (vcr > 0.0) {
-        if (HF_FLT_EQ(ur, ul)) {
+    const T a = T(1.7500), b = T(0.3750), c = T(0.7500), dd = T(0.1250), ee = T(0.2500);
+    if (vcr > T(0)) {
+        if (hf::flt_eq(ur, ul)) {
             conv1 = vcr * ufacet;
         } else {
-            const double fi = (ufacet - ul) / (ur - ul);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            const T fi = (ufacet - ul) / (ur - ul);
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv1 = vcr * ufacet;
             } else {
                 if (fi < b) conv1 = vcr * (a * ufacet - c * ul);
@@ -332,11 +340,11 @@ __device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double u
             }
         }
     } else {
-        if (HF_FLT_EQ(ufacet, urr)) {
+        if (hf::flt_eq(ufacet, urr)) {
             conv1 = vcr * ur;
         } else {
-            const double fi = (ur - urr) / (ufacet - urr);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            const T fi = (ur - urr) / (ufacet - urr);
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv1 = vcr * ur;
             } else {
                 if (fi < b) conv1 = infrr == 1 ? vcr * (a * ur - c * urr) : vcr * ur;
@@ -345,12 +353,12 @@ __device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double u
             }
         }
     }
-    if (vcl > 0.0) {
-        if (HF_FLT_EQ(ufacet, ull)) {
+    if (vcl > T(0)) {
+        if (hf::flt_eq(ufacet, ull)) {
             conv2 = vcl * ul;
         } else {
-            const double fi = (ul - ull) / (ufacet - ull);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            const T fi = (ul - ull) / (ufacet - ull);
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv2 = vcl * ul;
             } else {
                 if (fi < b) conv2 = infll == 1 ? vcl * (a * ul - c * ull) : vcl * ul;
@@ -359,11 +367,11 @@ __device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double u
             }
         }
     } else {
-        if (HF_FLT_EQ(ul, ur)) {
+        if (hf::flt_eq(ul, ur)) {
             conv2 = vcl * ufacet;
         } else {
-            const double fi = (ufacet - ur) / (ul - ur);
-            if ((fi <= 0.0) || (fi >= 1.0)) {
+            const T fi = (ufacet - ur) / (ul - ur);
+            if ((fi <= T(0)) || (fi >= T(1))) {
                 conv2 = vcl * ufacet;
             } else {
                 if (fi < b) conv2 = vcl * (a * ufacet - c * ur);
@@ -372,14 +380,25 @@ __device__ __noinline__ double2 cubista_facet(double ufacet, double ul, double u
             }
         }
     }
-    return make_double2(conv1, conv2);
+}
+
+// (FP64: the reference's arithmetic; the mixed form takes the FP32 instantiation)
+template <typename T>
+__device__ __forceinline__ double2 cubista_facet(double ufacet, double ul, double ur, double ull, double urr, int infll,
+                                                 int infrr, double vcr, double vcl, double conv1, double conv2)
+{
+    T c1 = (T)conv1, c2 = (T)conv2;
+    cubista_facet_t<T>((T)ufacet, (T)ul, (T)ur, (T)ull, (T)urr, infll, infrr, (T)vcr, (T)vcl, c1, c2);
+    return make_double2((double)c1, (double)c2);
 }
 
 // 128-thread blocks: the prefetched slots take ~170 registers per thread, and
 // three such blocks fit an SM where one 256-thread block would
 constexpr int kVelBlock = 128;
 
-template <int D, bool VE>
+// MIX: the mixed form, whose CUBISTA fluxes are evaluated in FP32 (the time
+// update and everything else stay FP64)
+template <int D, bool VE, bool MIX>
 __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -458,7 +477,8 @@ __global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
             } else if (second == HF_CUBISTA) {
                 const double vcr = SLQ(B + HF_V_VCR, F.u[d2]);
                 const double vcl = SLQ(B + HF_V_VCL, F.u[d2]);
-                const double2 cv = cubista_facet(ufacet, ul, ur, ull, urr, infll, infrr, vcr, vcl, conv1, conv2);
+                const double2 cv = cubista_facet<typename std::conditional<MIX, float, double>::type>(
+                    ufacet, ul, ur, ull, urr, infll, infrr, vcr, vcl, conv1, conv2);
                 conv1 = cv.x;
                 conv2 = cv.y;
                 vc[d2] = ((conv1 - conv2) / fd[d]);
@@ -611,7 +631,9 @@ __global__ void __launch_bounds__(kBlock) k_gptt_ml(DevProg P, DevFields F)
 // IMPL: the implicit constitutive step (hf_params.ve_discrtype, the same for
 // every instance of a case), a separate instantiation so that the explicit
 // kernel carries none of its code
-template <int D, bool IMPL>
+// MIX: the mixed form, whose CUBISTA cell convection is evaluated in FP32 (the
+// eigensystem, kernel transform and time update stay FP64)
+template <int D, bool IMPL, bool MIX>
 __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P, DevFields F)
 {
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
@@ -814,7 +836,12 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
                 if (cub) {
                     const double kll = kv[4 * dim + 2];
                     const double krr = kv[4 * dim + 3];
-                    rhs -= hf::cubista_cell(kl, kr, kll, krr, il, ir, ill, irr, vl[dim], vr[dim], K[i][j], cd[dim]);
+                    if (MIX)
+                        rhs -= (double)hf::cubista_cell_t<float>((float)kl, (float)kr, (float)kll, (float)krr, il, ir,
+                                                                 ill, irr, (float)vl[dim], (float)vr[dim],
+                                                                 (float)K[i][j], (float)cd[dim]);
+                    else
+                        rhs -= hf::cubista_cell(kl, kr, kll, krr, il, ir, ill, irr, vl[dim], vr[dim], K[i][j], cd[dim]);
                 } else {
                     double dk;
                     if ((il == 1) && (ir == 1)) dk = (kr - kl) / (2.0 * 1.0 * cd[dim]);
@@ -2255,12 +2282,26 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     int n = 0;
     if (C->P.nvrows) {
-        if (C->P.sw32) k_vrows<float><<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
-        else k_vrows<double><<<blocks(C->P.nvrows), kBlock, 0, st>>>(C->P, F);
+        const int nb = blocks(C->P.nvrows);
+        const bool c16 = C->P.scol16 != nullptr;
+        if (C->P.sw32) {
+            if (c16) k_vrows<float, true><<<nb, kBlock, 0, st>>>(C->P, F);
+            else k_vrows<float, false><<<nb, kBlock, 0, st>>>(C->P, F);
+        } else {
+            if (c16) k_vrows<double, true><<<nb, kBlock, 0, st>>>(C->P, F);
+            else k_vrows<double, false><<<nb, kBlock, 0, st>>>(C->P, F);
+        }
         n++;
     }
-    if (ve) k_velocity<D, true><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
-    else k_velocity<D, false><<<(C->nfacet_total + kVelBlock - 1) / kVelBlock, kVelBlock, 0, st>>>(C->P, F);
+    const int nb = (C->nfacet_total + kVelBlock - 1) / kVelBlock;
+    const bool mix = C->P.sw32 != nullptr;
+    if (ve) {
+        if (mix) k_velocity<D, true, true><<<nb, kVelBlock, 0, st>>>(C->P, F);
+        else k_velocity<D, true, false><<<nb, kVelBlock, 0, st>>>(C->P, F);
+    } else {
+        if (mix) k_velocity<D, false, true><<<nb, kVelBlock, 0, st>>>(C->P, F);
+        else k_velocity<D, false, false><<<nb, kVelBlock, 0, st>>>(C->P, F);
+    }
     n++;
     const int scheme = C->par.tempdiscrtype;
     if (scheme == HF_EXPLICIT_RK2 || scheme == HF_EXPLICIT_RK3) {
@@ -2283,10 +2324,15 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
             k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
             fixed++;
         }
-        if (C->par.ve_discrtype == HF_VE_IMPLICIT)
-            k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
-        else
-            k_ve_cell<D, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, F);
+        const int nb = (C->P.ncell + kVeBlock - 1) / kVeBlock;
+        const bool mix = C->P.sw32 != nullptr;
+        if (C->par.ve_discrtype == HF_VE_IMPLICIT) {
+            if (mix) k_ve_cell<D, true, true><<<nb, kVeBlock, 0, st>>>(C->P, F);
+            else k_ve_cell<D, true, false><<<nb, kVeBlock, 0, st>>>(C->P, F);
+        } else {
+            if (mix) k_ve_cell<D, false, true><<<nb, kVeBlock, 0, st>>>(C->P, F);
+            else k_ve_cell<D, false, false><<<nb, kVeBlock, 0, st>>>(C->P, F);
+        }
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
@@ -2551,10 +2597,11 @@ int bicg_step(hf_case *C)
             k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
             launches++;
         }
+        // (the BiCGStab path is plain FP64: the mixed form needs the CG solver)
         if (C->par.ve_discrtype == HF_VE_IMPLICIT)
-            k_ve_cell<D, true><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
+            k_ve_cell<D, true, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
         else
-            k_ve_cell<D, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
+            k_ve_cell<D, false, false><<<(C->P.ncell + kVeBlock - 1) / kVeBlock, kVeBlock, 0, st>>>(C->P, C->F);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
         launches += 2;
         for (int k = 0; k < D * D; k++) std::swap(C->F.K[k], C->F.Knew[k]);
@@ -2865,7 +2912,20 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 sptr[sl + 1] = sptr[sl] + 32 * mx;
             }
             const size_t ne = (size_t)sptr[nsl];
-            std::vector<int32_t> scol(ne, 0);
+            // the columns: 16-bit offsets from the pair's first column when
+            // every pair's entries stay within +-32767 of it, else 32-bit
+            bool c16 = true;
+            std::vector<int32_t> pcol0(np, 0);
+            for (size_t u = 0; u < np && c16; u++) {
+                const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
+                pcol0[u] = plen[u] ? pbase[u] + pg->tmpl_col[a0] : 0;
+                for (int k = 0; k < plen[u]; k++) {
+                    const int64_t d = (int64_t)pbase[u] + pg->tmpl_col[a0 + k] - pcol0[u];
+                    if (d < -32767 || d > 32767) { c16 = false; break; }
+                }
+            }
+            std::vector<int32_t> scol(c16 ? 0 : ne, 0);
+            std::vector<int16_t> scol16(c16 ? ne : 0, 0);
             std::vector<double> sw;
             std::vector<float> sw32;
             if (opt.precision == HF_PREC_MIXED) sw32.assign(ne, 0.f);
@@ -2876,14 +2936,20 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
                 for (int k = 0; k < plen[u]; k++, at += 32) {
                     const int64_t c = (int64_t)pbase[u] + pg->tmpl_col[a0 + k];
                     if (c < 0 || c > INT32_MAX) return cleanup(fail(HF_ERR_INVALID, "velocity-stage column out of range"));
-                    scol[at] = (int32_t)c;
+                    if (c16) scol16[at] = (int16_t)(c - pcol0[u]);
+                    else scol[at] = (int32_t)c;
                     if (opt.precision == HF_PREC_MIXED) sw32[at] = (float)pg->tmpl_w[a0 + k];
                     else sw[at] = pg->tmpl_w[a0 + k];
                 }
             }
             UP((int64_t **)&P.sptr, sptr.data(), sptr.size());
             UP((uint8_t **)&P.plen, plen.data(), plen.size());
-            UP((int32_t **)&P.scol, scol.data(), scol.size());
+            if (c16) {
+                UP((int16_t **)&P.scol16, scol16.data(), scol16.size());
+                UP((int32_t **)&P.pcol0, pcol0.data(), pcol0.size());
+            } else {
+                UP((int32_t **)&P.scol, scol.data(), scol.size());
+            }
             if (opt.precision == HF_PREC_MIXED) UP((float **)&P.sw32, sw32.data(), sw32.size());
             else UP((double **)&P.sw, sw.data(), sw.size());
             C->vel_entries = (int64_t)ne;
