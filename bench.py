@@ -381,6 +381,7 @@ def run_b200(args, rank, world, device):
     launches = st.kernel_launches - st0.kernel_launches
     iters = st.total_iters - st0.total_iters
     phases = case.phase_times()
+    shapes = dict(zip(("k_vrows", "k_velocity", "k_ve_cell"), case.launch_shapes()))
     case.profile(False)
     t_s = _max_over_ranks(dev_ms / 1e3, world, device)
     value = cells * args.steps * world / t_s
@@ -474,6 +475,7 @@ def run_b200(args, rank, world, device):
         "poisson_iters_per_instance_step": it_step,
         "refinement_sweeps_last_step": st.last_outer,
         "phases_ms_per_step": {p: v[0] / args.steps for p, v in phases.items()},
+        "tuned_block_sizes": shapes,
         "setup_s": {"program": t_program, "create_and_time": t_create},
         "wall_s": t_wall,
         "clocks": clocks,

@@ -295,8 +295,9 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 // or 128-byte (FP32) weight load; the sum is dp_interpolate_from_stencil's
 // (pdomain.c:1026-1053): -rhs, then the entries in stencil order.  W = float
 // is the mixed form: FP32 weights and field values, FP32 accumulation.
+// (launch bounds of the largest block size the tuner tries)
 template <typename W, bool C16>
-__global__ void __launch_bounds__(kBlock) k_vrows(DevProg P, DevFields F)
+__global__ void __launch_bounds__(512) k_vrows(DevProg P, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= P.nvrows) return;
@@ -392,14 +393,15 @@ __device__ __forceinline__ double2 cubista_facet(double ufacet, double ul, doubl
     return make_double2((double)c1, (double)c2);
 }
 
-// 128-thread blocks: the prefetched slots take ~170 registers per thread, and
-// three such blocks fit an SM where one 256-thread block would
+// 128-thread blocks by default: the prefetched slots take ~170 registers per
+// thread, and three such blocks fit an SM where one 256-thread block would
+// (the tuner also tries 64 and 256)
 constexpr int kVelBlock = 128;
 
 // MIX: the mixed form, whose CUBISTA fluxes are evaluated in FP32 (the time
 // update and everything else stay FP64)
 template <int D, bool VE, bool MIX>
-__global__ void __launch_bounds__(kVelBlock) k_velocity(DevProg P, DevFields F)
+__global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= P.off[D]) return;
@@ -1331,6 +1333,10 @@ struct hf_case {
     int64_t ntemplates = 0;         // row templates of the finest Poisson operator
     int64_t vel_entries = 0;        // stored entries of the velocity-stage rows (padded slices)
     int64_t *ilim = nullptr;        // per-instance step limits on the device (null: none)
+    // launch shapes of the tuned kernels (hf_options.tuning): k_vrows,
+    // k_velocity, k_ve_cell block sizes; tuned before the first step
+    int blk_vrows = kBlock, blk_vel = kVelBlock, blk_ve = kVeBlock;
+    bool tuned = false;
     bool graph_profile = false;     // graphs were captured with phase events
     bool phase_pending = false;     // a profiled step's events are not read yet
     bool capturing = false;         // a step graph is being captured
@@ -2267,6 +2273,88 @@ void record(hf_case *C, int phase, int end)
     else cudaEventRecord(C->ev[2 * phase + end], C->stream);
 }
 
+// The viscoelastic cell stage's main kernel at the case's block size
+template <int D>
+void enqueue_ve_cell(hf_case *C, const DevFields &F, cudaStream_t st)
+{
+    const int vb = C->blk_ve, nb = (C->P.ncell + vb - 1) / vb;
+    const bool mix = C->P.sw32 != nullptr;
+    if (C->par.ve_discrtype == HF_VE_IMPLICIT) {
+        if (mix) k_ve_cell<D, true, true><<<nb, vb, 0, st>>>(C->P, F);
+        else k_ve_cell<D, true, false><<<nb, vb, 0, st>>>(C->P, F);
+    } else {
+        if (mix) k_ve_cell<D, false, true><<<nb, vb, 0, st>>>(C->P, F);
+        else k_ve_cell<D, false, false><<<nb, vb, 0, st>>>(C->P, F);
+    }
+}
+
+template <int D>
+int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st);
+
+// The launch-shape tuner (hf_options.tuning == 0): before the first step, each
+// tuned kernel runs a few times at each candidate block size on this case's
+// own data, timed with CUDA events on the case stream, and the fastest size is
+// kept.  The kernels tried write only what the step itself rewrites before
+// reading it (row values, u*, the new kernel tensor and Du), and every size
+// gives the same bits (each thread's work and order do not depend on the
+// block size), so tuning changes no result.
+template <int D>
+int autotune(hf_case *C)
+{
+    C->tuned = true;
+    if (C->opt.tuning != 0) return HF_OK;
+    cudaStream_t st = C->stream;
+    cudaEvent_t a, b;
+    HF_CK(cudaEventCreate(&a));
+    HF_CK(cudaEventCreate(&b));
+    auto time_it = [&](auto launch) -> float {
+        launch();   // warm
+        cudaEventRecord(a, st);
+        for (int r = 0; r < 3; r++) launch();
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    };
+    auto pick = [&](int &slot, std::initializer_list<int> sizes, auto launch) {
+        float best = 1e30f;
+        int keep = slot;
+        for (int bs : sizes) {
+            slot = bs;
+            const float ms = time_it(launch);
+            if (cudaGetLastError() != cudaSuccess) continue;
+            if (ms < best) {
+                best = ms;
+                keep = bs;
+            }
+        }
+        slot = keep;
+    };
+    const DevFields F = C->F;
+    // k_vrows alone (the facet kernel reads its output)
+    if (C->P.nvrows) {
+        pick(C->blk_vrows, {128, 256, 512}, [&]() {
+            const int bs = C->blk_vrows, nb = (C->P.nvrows + bs - 1) / bs;
+            const bool c16 = C->P.scol16 != nullptr;
+            if (C->P.sw32) {
+                if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(C->P, F);
+                else k_vrows<float, false><<<nb, bs, 0, st>>>(C->P, F);
+            } else {
+                if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(C->P, F);
+                else k_vrows<double, false><<<nb, bs, 0, st>>>(C->P, F);
+            }
+        });
+    }
+    if (!C->sie) pick(C->blk_vel, {64, 128, 256}, [&]() { enqueue_velocity<D>(C, F, st); });
+    if (C->par.flowtype == HF_VISCOELASTIC) pick(C->blk_ve, {64, 128}, [&]() { enqueue_ve_cell<D>(C, F, st); });
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    HF_CK(cudaStreamSynchronize(st));
+    HF_CK(cudaGetLastError());
+    return HF_OK;
+}
+
 // The velocity stage of one step: explicit Euler (k_vrows + k_velocity), and
 // for the explicit Runge-Kutta forms its combination with u.  The reference's
 // Runge-Kutta stages call higflow_explicit_euler_intermediate_velocity(ns, in,
@@ -2282,25 +2370,25 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     int n = 0;
     if (C->P.nvrows) {
-        const int nb = blocks(C->P.nvrows);
+        const int bs = C->blk_vrows, nb = (C->P.nvrows + bs - 1) / bs;
         const bool c16 = C->P.scol16 != nullptr;
         if (C->P.sw32) {
-            if (c16) k_vrows<float, true><<<nb, kBlock, 0, st>>>(C->P, F);
-            else k_vrows<float, false><<<nb, kBlock, 0, st>>>(C->P, F);
+            if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(C->P, F);
+            else k_vrows<float, false><<<nb, bs, 0, st>>>(C->P, F);
         } else {
-            if (c16) k_vrows<double, true><<<nb, kBlock, 0, st>>>(C->P, F);
-            else k_vrows<double, false><<<nb, kBlock, 0, st>>>(C->P, F);
+            if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(C->P, F);
+            else k_vrows<double, false><<<nb, bs, 0, st>>>(C->P, F);
         }
         n++;
     }
-    const int nb = (C->nfacet_total + kVelBlock - 1) / kVelBlock;
+    const int vb = C->blk_vel, nb = (C->nfacet_total + vb - 1) / vb;
     const bool mix = C->P.sw32 != nullptr;
     if (ve) {
-        if (mix) k_velocity<D, true, true><<<nb, kVelBlock, 0, st>>>(C->P, F);
-        else k_velocity<D, true, false><<<nb, kVelBlock, 0, st>>>(C->P, F);
+        if (mix) k_velocity<D, true, true><<<nb, vb, 0, st>>>(C->P, F);
+        else k_velocity<D, true, false><<<nb, vb, 0, st>>>(C->P, F);
     } else {
-        if (mix) k_velocity<D, false, true><<<nb, kVelBlock, 0, st>>>(C->P, F);
-        else k_velocity<D, false, false><<<nb, kVelBlock, 0, st>>>(C->P, F);
+        if (mix) k_velocity<D, false, true><<<nb, vb, 0, st>>>(C->P, F);
+        else k_velocity<D, false, false><<<nb, vb, 0, st>>>(C->P, F);
     }
     n++;
     const int scheme = C->par.tempdiscrtype;
@@ -2324,15 +2412,7 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
             k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
             fixed++;
         }
-        const int nb = (C->P.ncell + kVeBlock - 1) / kVeBlock;
-        const bool mix = C->P.sw32 != nullptr;
-        if (C->par.ve_discrtype == HF_VE_IMPLICIT) {
-            if (mix) k_ve_cell<D, true, true><<<nb, kVeBlock, 0, st>>>(C->P, F);
-            else k_ve_cell<D, true, false><<<nb, kVeBlock, 0, st>>>(C->P, F);
-        } else {
-            if (mix) k_ve_cell<D, false, true><<<nb, kVeBlock, 0, st>>>(C->P, F);
-            else k_ve_cell<D, false, false><<<nb, kVeBlock, 0, st>>>(C->P, F);
-        }
+        enqueue_ve_cell<D>(C, F, st);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
@@ -2555,7 +2635,9 @@ int graph_steps(hf_case *C, int nsteps, bool sync)
     // the semi-implicit form solves its velocity systems with a host-driven
     // loop, so its steps run eagerly
     const bool eager = C->opt.eager != 0 || C->sie;
-    int rc = eager ? HF_OK : ensure_graphs<D>(C);
+    int rc = C->tuned ? HF_OK : autotune<D>(C);
+    if (rc) return rc;
+    rc = eager ? HF_OK : ensure_graphs<D>(C);
     if (rc) return rc;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     auto one = [&]() -> int {
@@ -3343,6 +3425,15 @@ extern "C" int hf_case_set_timestep(hf_case *C, const double *dt, int32_t n)
     HF_CK(cudaStreamSynchronize(C->stream));
     C->par.dt = C->h_ipar[0].dt;
     C->P.par.dt = C->h_ipar[0].dt;
+    return HF_OK;
+}
+
+extern "C" int hf_case_launch_shapes(hf_case *C, int32_t *blocks, int32_t n)
+{
+    if (!C || !blocks || n < 3) return fail(HF_ERR_INVALID, "bad argument");
+    blocks[0] = C->blk_vrows;
+    blocks[1] = C->blk_vel;
+    blocks[2] = C->blk_ve;
     return HF_OK;
 }
 

@@ -46,6 +46,7 @@ def lib() -> C.CDLL:
         L.hf_case_adjust_timestep.argtypes = [V, P(C.c_double), P(C.c_double), C.c_int32]
         L.hf_case_set_timestep.argtypes = [V, P(C.c_double), C.c_int32]
         L.hf_case_set_step_limits.argtypes = [V, P(C.c_int64), C.c_int32]
+        L.hf_case_launch_shapes.argtypes = [V, P(C.c_int32), C.c_int32]
         L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
         L.hf_case_synchronize.argtypes = [V]
         L.hf_case_destroy.argtypes = [V]
@@ -71,12 +72,13 @@ def _check(rc: int) -> None:
 
 def options(precision: int = hp.PREC_FP64, poisson: int = hp.POISSON_AUTO, rtol: float = 1e-10,
             atol: float = 1e-10, maxit: int = 20000, device: int = 0,
-            precond: int = hp.PRECOND_AUTO, eager: bool = False) -> hp.HFOptions:
+            precond: int = hp.PRECOND_AUTO, eager: bool = False, tune: bool = True) -> hp.HFOptions:
     o = hp.HFOptions()
     o.precision, o.poisson = precision, poisson
     o.poisson_rtol, o.poisson_atol, o.poisson_maxit, o.device = rtol, atol, maxit, device
     o.precond = precond
     o.eager = int(bool(eager))
+    o.tuning = 0 if tune else 1
     return o
 
 
@@ -141,6 +143,12 @@ class Case:
     def set_timestep(self, dt) -> None:
         a = np.ascontiguousarray(np.atleast_1d(dt), dtype=np.float64)
         _check(lib().hf_case_set_timestep(self.h, a.ctypes.data_as(C.POINTER(C.c_double)), a.size))
+
+    def launch_shapes(self):
+        """Block sizes of the tuned kernels: (k_vrows, k_velocity, k_ve_cell)."""
+        a = (C.c_int32 * 3)()
+        _check(lib().hf_case_launch_shapes(self.h, a, 3))
+        return tuple(a)
 
     def launch_counts(self):
         """(kernels per step outside the Poisson loop, kernels per loop body)."""

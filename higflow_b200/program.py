@@ -131,7 +131,7 @@ class HFOptions(C.Structure):
         ("precision", C.c_int32), ("poisson", C.c_int32),
         ("poisson_rtol", C.c_double), ("poisson_atol", C.c_double),
         ("poisson_maxit", C.c_int32), ("device", C.c_int32), ("precond", C.c_int32),
-        ("eager", C.c_int32),
+        ("eager", C.c_int32), ("tuning", C.c_int32),
     ]
 
 

@@ -193,7 +193,7 @@ class BatchServer:
             r.t_done = time.perf_counter()
             r.done = True
             r.prog = None
-            self.cell_steps += r.steps * (c.prog.cell_off[i + 1] - c.prog.cell_off[i])
+            self.cell_steps += int(r.steps) * int(c.prog.cell_off[i + 1] - c.prog.cell_off[i])
             self.cv.notify_all()
 
     def _run(self) -> None:

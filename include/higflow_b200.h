@@ -290,6 +290,10 @@ typedef struct hf_options {
     int32_t eager;            /* 0: each step is one CUDA graph launch; 1:    */
                               /* kernels launched one by one with a host loop */
                               /* over the iterations (kernel profilers)       */
+    int32_t tuning;           /* 0: before the first step, time the velocity- */
+                              /* and cell-stage kernels at a few block sizes  */
+                              /* on this case and keep the fastest (results   */
+                              /* do not depend on it); 1: built-in sizes      */
 } hf_options;
 
 typedef struct hf_stats {
@@ -328,6 +332,11 @@ void hf_case_destroy(hf_case *c);
  * coarsest solves of all instances (rows = sum cn, nnz_a = sum cn^2). */
 int  hf_case_solver_info(hf_case *c, int32_t *method, int32_t *nlev, int64_t *rows, int64_t *nnz_a,
                          int64_t *nnz_p, int64_t *nnz_r, int32_t max_levels);
+
+/* The block sizes the case launches its tuned kernels with (see
+ * hf_options.tuning): blocks[0] velocity-stage rows (k_vrows), [1] facet
+ * kernel (k_velocity), [2] cell stage (k_ve_cell); n >= 3. */
+int  hf_case_launch_shapes(hf_case *c, int32_t *blocks, int32_t n);
 
 /* Kernels per step outside the Poisson iterations, and per loop body of the
  * iterations (one body = two CG iterations). */

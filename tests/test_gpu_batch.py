@@ -117,3 +117,27 @@ def test_step_limits_freeze_each_instance_at_its_count(precision):
         err = compare(got, alone, _keys(prog))
         assert max(err.values()) < 1e-10, (name, limits[i], err)
     case.close()
+
+
+def test_launch_shape_tuning_changes_no_result():
+    """hf_options.tuning: the tuned block sizes give the built-in sizes' fields
+    bit for bit (each thread's work and order do not depend on the block
+    size), and the sizes kept are among the candidates."""
+    names = VE_NAMES[:3]
+    progs, datas = zip(*[load_golden(n) for n in names])
+    batch = hp.Program.concatenate(progs)
+    out = []
+    for tune in (True, False):
+        case = engine.Case(batch, engine.options(rtol=1e-13, atol=1e-300, precision=hp.PREC_MIXED, tune=tune))
+        for key, fid, comp in field_keys(progs[0]):
+            case.set(fid, comp, np.concatenate([d["init_" + key] for d in datas]))
+        case.step(3)
+        out.append({k: case.get(fid, comp) for k, fid, comp in field_keys(progs[0])})
+        shapes = case.launch_shapes()
+        if tune:
+            assert shapes[0] in (128, 256, 512) and shapes[1] in (64, 128, 256) and shapes[2] in (64, 128)
+        else:
+            assert shapes == (256, 128, 128)
+        case.close()
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
