@@ -315,6 +315,47 @@ def equal_error_protocol(draws, steps, device):
     return result
 
 
+def plain_one_case_at_a_time(draws, rtol, device, steps=10, count=16):
+    """The plain FP64 path as a HigFlow case runs it through the drop-in: one
+    case per engine case, stepped alone (one CUDA graph launch per step).
+    ``count`` instances at the population's side quantiles are timed (CUDA
+    events around ``steps`` steps after warm-up); the population's time per
+    step is the sum over its instances of the sample's time per step
+    interpolated in N^2 (log-log).  Returns cell-steps/s of the whole
+    population and the sample."""
+    import torch
+    from higflow_b200 import engine, workloads
+    from higflow_b200 import program as hp
+    sub = protocol_subset(draws, count)
+    progs = workloads.programs(sub)
+    ms = []
+    for prog in progs:
+        case = engine.Case(prog, engine.options(rtol=rtol, atol=1e-300, device=device, precision=hp.PREC_FP64))
+        stream = torch.cuda.ExternalStream(case.stream(), device=device)
+        case.step(3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+        case.step(steps, sync=False)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        case.synchronize()
+        torch.cuda.synchronize(device)
+        ms.append(a.elapsed_time(b) / steps)
+        case.close()
+    x = np.log([d.cells for d in sub])
+    y = np.log(ms)
+    order = np.argsort(x)
+    per = np.exp(np.interp(np.log([d.cells for d in draws]), x[order], y[order]))
+    total_ms = float(per.sum())
+    cells = sum(d.cells for d in draws)
+    return {"value": cells / (total_ms / 1e3), "ms_per_population_step": total_ms,
+            "sample": {"N": [d.n for d in sub], "ms_per_step": ms}, "rtol": rtol,
+            "method": f"{len(sub)} instances at the population's side quantiles stepped alone ({steps} steps each "
+                      "after 3 warm-up, CUDA events), the population's step time the sum of the sample's per-step "
+                      "times interpolated in cells (log-log) over its 256 instances"}
+
+
 def time_form(prog, prec, rtol, state, args, world, device, flush, profile=True):
     """Create a case in one precision form, load the state, warm up, time
     args.steps steps; returns (case, device ms, wall s, stats deltas)."""
@@ -438,6 +479,11 @@ def run_b200(args, rank, world, device):
                                                "frac": pws["bytes"] / (p_ms / args.steps / 1e3) / 1e9 / peak},
                                 "clocks": pclk},
                  "mixed_over_plain": value / plain_value}
+    if mixed and wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras:
+        draws = workloads.batched_giesekus()
+        one = plain_one_case_at_a_time(draws, rtol["plain"], device)
+        one["mixed_batched_over_it"] = value / one["value"]
+        extra["plain_fp64_one_case_at_a_time"] = one
     if protocol is not None:
         extra["equal_error_protocol"] = protocol
         if protocol.get("mixed"):

@@ -2001,7 +2001,8 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
             inv_off[i] = mixed ? ar.vec(cast_vec<float>(IH[i].inv)) : ar.vec(IH[i].inv);
     const int n = C->P.ncell;
     const size_t o_r = ar.zeros<double>(n), o_z = ar.zeros<double>(n), o_q = ar.zeros<double>(n);
-    const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n), o_xprev = ar.zeros<double>(n);
+    const size_t o_pa = ar.zeros<double>(n), o_pb = ar.zeros<double>(n), o_xprev = ar.zeros<double>(n),
+                 o_xprev2 = ar.zeros<double>(n);
     const size_t o_part = ar.zeros<double>((size_t)LH[0].ablk.size() * 2);
     // mixed form: the inner solve's FP32 vectors
     size_t o_r32 = 0, o_z32 = 0, o_q32 = 0, o_e32 = 0, o_pa32 = 0, o_pb32 = 0;
@@ -2050,6 +2051,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
     G.p = C->F.p;
     G.dp = C->F.dp;
     G.xprev = (double *)(base + o_xprev);
+    G.xprev2 = (double *)(base + o_xprev2);
     G.cinst = C->P.cinst;
     G.r = (double *)(base + o_r);
     G.z = (double *)(base + o_z);

@@ -86,6 +86,7 @@ struct Ctl {
     int64_t err_step;
     int64_t step;         // steps completed
     int64_t total_bodies;
+    int32_t hist, pad;    // earlier solutions the initial guess can use (0..2)
 };
 
 // The finest operator as row templates: row i applies the template described
@@ -191,7 +192,7 @@ struct PcgFine {
     const int32_t *ipin;      // per instance: pinned global row or -1
     const hf_params *ipar;
     double *p, *dp;           // unknown: dp (incremental projection) or p
-    double *xprev;            // the unknown of the step before (initial-guess extrapolation)
+    double *xprev, *xprev2;   // the unknown of the steps before (initial-guess extrapolation)
     const int32_t *cinst;     // cell -> instance
     double *r, *z, *q;
     double *partials;
@@ -797,11 +798,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *
     }
 }
 
-// Initial guess of the step's solve: linear extrapolation in time of the
-// unknown, x0 = 2 x_n - x_{n-1} (x_n is the previous step's solution, the
-// reference's own initial guess, solver-petsc.c:386-399).  The solution is the
-// same to the solve's tolerance; the extrapolated start is closer to it, so
-// fewer iterations are needed.  The first step of a case keeps x_n.
+// Initial guess of the step's solve: extrapolation in time of the unknown from
+// the solutions of the steps before (x_n is the previous step's solution, the
+// reference's own initial guess, solver-petsc.c:386-399): quadratic,
+// x0 = 3 x_n - 3 x_{n-1} + x_{n-2}, once two earlier solutions are known,
+// linear, 2 x_n - x_{n-1}, with one, x_n with none (Ctl::hist counts them;
+// a restart clears it).  The solution is the same to the solve's tolerance;
+// the extrapolated start is closer to it, so fewer iterations are needed.
 __global__ void __launch_bounds__(kBlock) k_pcg_extrapolate(PcgFine G)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -811,11 +814,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg_extrapolate(PcgFine G)
     if (G.ilim && G.ilim[__ldg(G.cinst + i)] == 0) return;
     const int pt = G.projtype_all >= 0 ? G.projtype_all : __ldg(&G.ipar[__ldg(G.cinst + i)].projtype);
     double *x = pt == HF_INCREMENTAL ? G.dp : G.p;
-    const double xn = x[i], xpv = G.xprev[i];
-    // (a plain load: the step count was written by an earlier kernel)
-    const double xp = __ldg(&G.ctl->step) == 0 ? xn : xpv;
+    const double xn = x[i], x1 = G.xprev[i], x2 = G.xprev2[i];
+    // (a plain load: the history count was written by an earlier kernel)
+    const int hist = __ldg(&G.ctl->hist);
+    G.xprev2[i] = x1;
     G.xprev[i] = xn;
-    x[i] = 2.0 * xn - xp;
+    x[i] = hist >= 2 ? 3.0 * xn - 3.0 * x1 + x2 : hist == 1 ? 2.0 * xn - x1 : xn;
 }
 
 // restart the time history: the next extrapolation starts from the unknown's
@@ -826,6 +830,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_restart(PcgFine G)
     if (i >= G.n) return;
     const int pt = G.projtype_all >= 0 ? G.projtype_all : __ldg(&G.ipar[__ldg(G.cinst + i)].projtype);
     G.xprev[i] = (pt == HF_INCREMENTAL ? G.dp : G.p)[i];
+    if (i == 0) G.ctl->hist = 0;
 }
 
 // end of a step: per-instance totals, the first failure, loop counters reset
@@ -854,6 +859,7 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
     if (threadIdx.x == 0) {
         c->total_bodies += c->bodies;
         c->step += 1;
+        if (c->hist < 2) c->hist += 1;
         c->active = 0;
         c->bodies = 0;
     }
