@@ -88,7 +88,8 @@ def load_program(wl, rank=0, world=1):
     from higflow_b200 import host, workloads
     if wl.get("batch") == "c4":
         draws = workloads.batched_giesekus()[:wl.get("count", 256)]
-        return workloads.batch(shard(draws, rank, world))
+        # each rank records its own shard, with its share of the host's cores
+        return workloads.batch(shard(draws, rank, world), procs=max(1, (os.cpu_count() or 1) // world))
     if wl.get("contraction"):
         return host.record(workloads.contraction_c2(wl["contraction"]))
     return host.record(host.cavity(wl["dim"], wl["n"], Re=wl["Re"], dt=wl["dt"]))

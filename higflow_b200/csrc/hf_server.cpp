@@ -1,4 +1,6 @@
-// Serving: continuous batching of independent HigFlow cases on one device.
+// Serving: independent HigFlow cases stepping concurrently on one device, one
+// engine case per request (requests that can share a batch go to the
+// continuous-batching server, higflow_b200/serve.py, instead).
 //
 // A request is a step program, its options, an optional initial state and a
 // step count.  The server

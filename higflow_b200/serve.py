@@ -90,7 +90,8 @@ class BatchServer:
     cells per cohort; ``chunk``: steps queued per cohort between checks."""
 
     def __init__(self, device: int = 0, budget_gb: float = 150.0, max_cohorts: int = 8,
-                 max_cells: int = 8_000_000, chunk: int = 32, opts: Optional[hp.HFOptions] = None):
+                 max_cells: int = 8_000_000, chunk: int = 32, opts: Optional[hp.HFOptions] = None,
+                 window_s: float = 0.25):
         import torch
         self.torch = torch
         self.device = device
@@ -98,6 +99,7 @@ class BatchServer:
         self.max_cohorts = max_cohorts
         self.max_cells = max_cells
         self.chunk = chunk
+        self.window_s = window_s
         self.opts = opts or engine.options(rtol=1e-10, atol=1e-300, device=device)
         self.mu = threading.Lock()
         self.cv = threading.Condition(self.mu)
@@ -163,9 +165,17 @@ class BatchServer:
         return keys
 
     def _form(self) -> Optional[List[_Request]]:
-        """The next cohort from the queue head's group (lock held)."""
+        """The next cohort from the queue head's group (lock held).  While
+        other cohorts run, waiting requests gather for ``window_s`` (or until
+        they reach a quarter of ``max_cells``) so that a cohort is a batch
+        rather than a single request; an idle device takes them at once."""
         if not self.queue or len(self.cohorts) >= self.max_cohorts:
             return None
+        if self.cohorts:
+            waited = time.perf_counter() - self.queue[0].t_submit
+            cells = sum(r.prog.ncell for r in self.queue)
+            if waited < self.window_s and cells < self.max_cells // 4:
+                return None
         held = sum(c.nbytes for c in self.cohorts)
         key = batch_key(self.queue[0].prog)
         pick, cells, est = [], 0, 0

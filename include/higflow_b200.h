@@ -400,8 +400,12 @@ int  hf_case_device_bytes(const hf_program *prog, const hf_options *opt, int64_t
 const char *hf_last_error(void);
 
 /* ------------------------------------------------------------------ */
-/* serving: continuous batching of independent cases on one device    */
-/* (no counterpart in the reference, which runs one case per job)      */
+/* serving: independent cases stepping concurrently on one device,    */
+/* one engine case per request (no counterpart in the reference, which */
+/* runs one case per job).  For requests that can share a batch, the   */
+/* continuous-batching server (higflow_b200/serve.py) groups them into */
+/* batch cases with per-instance step limits instead; this server is   */
+/* for requests that cannot batch (the semi-implicit velocity forms).  */
 /* ------------------------------------------------------------------ */
 typedef struct hf_server hf_server;
 
