@@ -236,6 +236,9 @@ void *hfref_ns(hfref_case *C) { return C->ns; }
  * both print through print0f, silenced here like the rest of the harness) */
 double hfref_dt(hfref_case *C) { return C->ns->par.dt; }
 
+/* a host-side change of the time step (as a case main loop or a restart makes) */
+void hfref_set_dt(hfref_case *C, double dt) { C->ns->par.dt = dt; }
+
 double hfref_cfl(hfref_case *C)
 {
     hfh_select(C->ns);

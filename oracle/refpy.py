@@ -60,6 +60,8 @@ def lib(dim: int) -> C.CDLL:
         L.hfref_ns.restype = C.c_void_p
         L.hfref_dt.argtypes = [C.c_void_p]
         L.hfref_dt.restype = C.c_double
+        L.hfref_set_dt.argtypes = [C.c_void_p, C.c_double]
+        L.hfref_set_dt.restype = None
         L.hfref_cfl.argtypes = [C.c_void_p]
         L.hfref_cfl.restype = C.c_double
         L.hfref_adjust_timestep.argtypes = [C.c_void_p]
@@ -201,6 +203,10 @@ class RefCase:
     @property
     def dt(self) -> float:
         return self.L.hfref_dt(self.h)
+
+    @dt.setter
+    def dt(self, value: float) -> None:
+        self.L.hfref_set_dt(self.h, float(value))
 
     def cfl(self) -> float:
         """The reference's own CFL number of the current velocity."""

@@ -172,3 +172,38 @@ def test_adjust_timestep_through_the_binding_matches_the_reference():
     L.hf_detach(gpu.ns)
     ref.close()
     gpu.close()
+
+
+def test_a_host_change_of_dt_reaches_the_gpu():
+    """A case that sets ns->par.dt on the host between steps (a restart, or
+    its own time-step control) syncs out, changes dt, and pushes the state
+    back with hf_sync_to_device, which carries the new dt to the engine; the
+    GPU then steps with it exactly as the reference does."""
+    if not refpy.available(2):
+        pytest.skip("oracle build of the reference not present")
+    ref = refpy.RefCase(CASES["newtonian"]())
+    gpu = refpy.RefCase(CASES["newtonian"]())
+    _perturb(ref, False)
+    _perturb(gpu, False)
+    ref.flatten()
+    L = gpu.L
+    opts = engine.options(rtol=1e-13, atol=1e-300)
+    assert L.hf_attach(gpu.ns, C.byref(opts)) == 0, L.hf_last_error()
+    ref.step(2)
+    for _ in range(2):
+        assert L.hf_step(gpu.ns) == 0, L.hf_last_error()
+    assert L.hf_sync_to_host(gpu.ns) == 0, L.hf_last_error()
+    for c in (ref, gpu):
+        c.dt = 0.6 * c.dt
+    assert L.hf_sync_to_device(gpu.ns) == 0, L.hf_last_error()
+    ref.step(3)
+    for _ in range(3):
+        assert L.hf_step(gpu.ns) == 0, L.hf_last_error()
+    assert L.hf_sync_to_host(gpu.ns) == 0, L.hf_last_error()
+    want, got = _fields(ref, False), _fields(gpu, False)
+    for k in want:
+        err = np.linalg.norm(got[k] - want[k]) / max(np.linalg.norm(want[k]), 1e-300)
+        assert err < TOL, (k, err)
+    L.hf_detach(gpu.ns)
+    ref.close()
+    gpu.close()
