@@ -168,7 +168,10 @@ def phase_bytes(prog, mixed, iters_per_step, sweeps_per_step):
     sb = roofline.step_bytes(prog, mixed)
     nc = prog.ncell
     spmv64 = 4 * (nc + 1) + prog.p_col.size * 12 + 2 * 8 * nc
+    w = 4 if mixed else 8
     out = {"velocity": sb["velocity"]["F"] + sb["velocity"]["S"],
+           # the velocity stage's rows alone (k_vrows): their stencil bytes
+           "velocity_rows": 4 * sb["velocity"]["rows"] + sb["velocity"]["row_entries"] * (4 + w),
            "poisson_init": sb["divergence"]["F"] + sb["divergence"]["S"] + spmv64,
            "poisson_iter": iters_per_step * roofline.poisson_iter_bytes(prog, 4 if mixed else 8)
            + sweeps_per_step * spmv64,
@@ -442,7 +445,9 @@ def run_b200(args, rank, world, device):
             phase_rl[p] = {"bytes_per_step": pb[p], "ms_per_step": ms / args.steps, "launches_per_step": nl / args.steps,
                            "GB/s": pb[p] / (ms / args.steps / 1e3) / 1e9,
                            "frac": pb[p] / (ms / args.steps / 1e3) / 1e9 / peak}
-    dom = max(phase_rl, key=lambda p: phase_rl[p]["ms_per_step"])
+    # the roofline kernel: the stage's HBM-bound stencil kernel (k_vrows), the
+    # longest single kernel of the step; the phases' figures are beside it
+    dom = "velocity_rows" if "velocity_rows" in phase_rl else max(phase_rl, key=lambda p: phase_rl[p]["ms_per_step"])
     d = phase_rl[dom]
     traffic = None
     tfile = os.path.join(REPO, "profiles", f"traffic_{args.workload}.json")
@@ -509,7 +514,8 @@ def run_b200(args, rank, world, device):
                    "parallelism": f"instances partitioned by cost over {world} GPU(s)" if wl.get("batch") else
                                   f"replicas x{world}",
                    "program": "recorded by the HigFlow host (HigTree's own stencils, ids and weights)"},
-        "roofline": {"bound": "hbm", "kernel": f"{dom} phase", "achieved": d["GB/s"], "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_vrows (the velocity stage's stencil rows)" if dom == "velocity_rows"
+                     else f"{dom} phase", "achieved": d["GB/s"], "peak": peak, "unit": "GB/s",
                      "frac": d["frac"], "traffic": traffic,
                      "bytes_per_launch": d["bytes_per_step"] / max(d["launches_per_step"], 1e-9),
                      "launch_us": d["ms_per_step"] * 1e3 / max(d["launches_per_step"], 1e-9),

@@ -2372,6 +2372,7 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     int n = 0;
     if (C->P.nvrows) {
+        record(C, HF_PHASE_VELOCITY_ROWS, 0);
         const int bs = C->blk_vrows, nb = (C->P.nvrows + bs - 1) / bs;
         const bool c16 = C->P.scol16 != nullptr;
         if (C->P.sw32) {
@@ -2381,6 +2382,7 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
             if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(C->P, F);
             else k_vrows<double, false><<<nb, bs, 0, st>>>(C->P, F);
         }
+        record(C, HF_PHASE_VELOCITY_ROWS, 1);
         n++;
     }
     const int vb = C->blk_vel, nb = (C->nfacet_total + vb - 1) / vb;
@@ -2619,12 +2621,15 @@ int collect_phases(hf_case *C)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     for (int p = 0; p < HF_NPHASE; p++) {
         if (p == HF_PHASE_VE_CELL && !ve) continue;
+        if (p == HF_PHASE_VELOCITY_ROWS && !C->P.nvrows) continue;
         float ms = 0.f;
         HF_CK(cudaEventElapsedTime(&ms, C->ev[2 * p], C->ev[2 * p + 1]));
         C->phase_ms[p] += ms;
     }
-    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2;
-    C->phase_launches[HF_PHASE_VELOCITY] += 1;
+    const bool rk = C->par.tempdiscrtype == HF_EXPLICIT_RK2 || C->par.tempdiscrtype == HF_EXPLICIT_RK3;
+    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2 + (C->gptt ? 1 : 0);
+    C->phase_launches[HF_PHASE_VELOCITY] += 1 + (C->P.nvrows ? 1 : 0) + (rk ? 1 : 0);
+    if (C->P.nvrows) C->phase_launches[HF_PHASE_VELOCITY_ROWS] += 1;
     C->phase_launches[HF_PHASE_POISSON_INIT] += 2;
     C->phase_launches[HF_PHASE_POISSON_ITER] += (C->h_ctl->total_bodies - C->bodies0) * C->body_kernels;
     C->phase_launches[HF_PHASE_FINAL] += 2;

@@ -388,7 +388,9 @@ enum {
     HF_PHASE_POISSON_INIT = 2,  /* divergence rhs + first residual         */
     HF_PHASE_POISSON_ITER = 3,  /* Krylov iterations                       */
     HF_PHASE_FINAL = 4,         /* final velocity and pressure             */
-    HF_NPHASE = 5
+    HF_PHASE_VELOCITY_ROWS = 5, /* within HF_PHASE_VELOCITY: its stencil   */
+                                /* rows (k_vrows) alone; CG path only      */
+    HF_NPHASE = 6
 };
 int  hf_case_profile(hf_case *c, int32_t enable);
 int  hf_case_phase_times(hf_case *c, double *ms, int64_t *launches, int32_t n);
