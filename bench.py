@@ -570,22 +570,27 @@ def served(args, device, rtol):
         if lag > 0:
             time.sleep(lag)
         ids.append(srv.submit(prog, c.steps))
-    tts, queue, failed = [], [], 0
-    for rid in ids:
+    tts, queue, failed, why, ok = [], [], 0, {}, []
+    for rid, (_, c) in zip(ids, reqs):
         status, q, t = srv.wait(rid)
-        failed += status != 0
+        ok.append(status == 0)
+        if status != 0:
+            failed += 1
+            kind = "newtonian cavity" if c.model < 0 else f"{'oldroyd-b' if c.model == hp.OLDROYD_B else 'giesekus'} " \
+                f"{c.geometry}"
+            why.setdefault(kind, []).append({"n": c.n, "steps": c.steps, "Wi": round(c.De, 3), "status": int(status)})
         tts.append(t)
         queue.append(q)
         srv.release(rid)
     makespan = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    cells = sum(p.ncell * c.steps for p, (_, c) in zip(progs, reqs))
+    cells = sum(p.ncell * c.steps for p, (_, c), good in zip(progs, reqs, ok) if good)
     kinds = {"newtonian cavity": sum(c.model < 0 for _, c in reqs),
              "oldroyd-b cavity": sum(c.model == hp.OLDROYD_B for _, c in reqs),
              "giesekus channel": sum(c.geometry == "channel" for _, c in reqs)}
     return {
-        "requests": len(ids), "failed": int(failed), "solves_per_s": len(ids) / makespan,
+        "requests": len(ids), "failed": int(failed), "failures": why, "solves_per_s": sum(ok) / makespan,
         "p50_s": float(np.percentile(tts, 50)), "p99_s": float(np.percentile(tts, 99)),
         "queue_p50_s": float(np.percentile(queue, 50)), "queue_p99_s": float(np.percentile(queue, 99)),
         "cell_steps_per_s": cells / makespan, "makespan_s": makespan, "arrival_window_s": reqs[-1][0],

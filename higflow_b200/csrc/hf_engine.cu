@@ -294,7 +294,12 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 // the 32 pairs of a warp is one 128-byte column load and one 256-byte (FP64)
 // or 128-byte (FP32) weight load; the sum is dp_interpolate_from_stencil's
 // (pdomain.c:1026-1053): -rhs, then the entries in stencil order.  W = float
-// is the mixed form: FP32 weights and field values, FP32 accumulation.
+// is the mixed form: FP32 weights (half the weight stream), FP64 field values
+// and FP64 accumulation.  Rounding the field values or the sum to FP32 puts
+// noise of about 1e-7 of the velocity into every step's Poisson right-hand
+// side that the extrapolated initial guess cannot follow: measured on the
+// batched Giesekus cavities at Poisson rtol 1e-6, 7.2 CG iterations per
+// instance-step against 4.4 with FP64 sums (4.0 for the plain form).
 // (launch bounds of the largest block size the tuner tries)
 template <typename W, bool C16>
 __global__ void __launch_bounds__(512) k_vrows(DevProg P, DevFields F)
@@ -306,15 +311,17 @@ __global__ void __launch_bounds__(512) k_vrows(DevProg P, DevFields F)
     const int n = __ldg(P.plen + u);
     const int64_t e0 = __ldg(P.sptr + (u >> 5)) + (u & 31);
     const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)P.sw32 : (const W *)P.sw;
-    W res = (W)0;
-    res += -(W)__ldg(P.vrow.rhs + u);
-#pragma unroll 4
+    double res = 0.0;
+    res += -__ldg(P.vrow.rhs + u);
+    // the entries stream through once (evict-first loads keep L1 for the
+    // field gathers); eight entries' loads in flight per thread
+#pragma unroll 8
     for (int k = 0; k < n; k++) {
         const int64_t at = e0 + 32 * (int64_t)k;
-        const int c = C16 ? (int)__ldg(P.scol16 + at) : __ldg(P.scol + at);
-        res += (W)__ldg(fb + c) * __ldg(w + at);
+        const int c = C16 ? (int)__ldcs(P.scol16 + at) : __ldcs(P.scol + at);
+        res += __ldg(fb + c) * (double)__ldcs(w + at);
     }
-    P.rowval[u] = (double)res;
+    P.rowval[u] = res;
 }
 
 // CUBISTA convective flux of the facet velocity along one direction
@@ -3465,6 +3472,20 @@ extern "C" int hf_case_set_step_limits(hf_case *C, const int64_t *steps, int32_t
         HF_CK(cudaMemcpyAsync(C->ilim, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, C->stream));
     }
     HF_CK(cudaStreamSynchronize(C->stream));
+    return HF_OK;
+}
+
+extern "C" int hf_case_instance_failures(hf_case *C, int32_t *status, int32_t n)
+{
+    if (!C || !status) return fail(HF_ERR_INVALID, "null argument");
+    if (n != C->ninst) return fail(HF_ERR_INVALID, "array size is not the instance count");
+    if (!C->use_cg) {
+        for (int i = 0; i < n; i++) status[i] = 0;
+        return HF_OK;
+    }
+    int rc = pull_state(C);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) status[i] = C->h_S[i].failed;
     return HF_OK;
 }
 

@@ -73,7 +73,10 @@ struct IScal {
     // target, sweeps done, inner iterations of the step's earlier sweeps, and
     // fin = the FP64 residual met the target (or the solve failed)
     double tol2in;
-    int32_t outer, iters_prev, fin, pad2;
+    int32_t outer, iters_prev, fin;
+    // under step limits: the instance's first failed step's status (sticky;
+    // the instance is frozen from that step on)
+    int32_t failed;
 };
 
 // loop control and error record of the whole case
@@ -850,6 +853,11 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
             s.fin = 1;
         }
         s.total_iters += s.iters + s.iters_prev;
+        if (s.status && G.ilim) {
+            // a batch under step limits goes on without the failed instance
+            G.ilim[i] = 0;
+            if (!s.failed) s.failed = s.status;
+        }
         if (s.status && atomicCAS(&c->err_status, 0, s.status) == 0) {
             c->err_inst = i;
             c->err_step = c->step;

@@ -46,6 +46,7 @@ def lib() -> C.CDLL:
         L.hf_case_adjust_timestep.argtypes = [V, P(C.c_double), P(C.c_double), C.c_int32]
         L.hf_case_set_timestep.argtypes = [V, P(C.c_double), C.c_int32]
         L.hf_case_set_step_limits.argtypes = [V, P(C.c_int64), C.c_int32]
+        L.hf_case_instance_failures.argtypes = [V, P(C.c_int32), C.c_int32]
         L.hf_case_launch_shapes.argtypes = [V, P(C.c_int32), C.c_int32]
         L.hf_case_stats.argtypes = [V, P(hp.HFStats)]
         L.hf_case_synchronize.argtypes = [V]
@@ -139,6 +140,12 @@ class Case:
         """Instance i takes steps[i] more steps, then stays as it is (< 0: no limit)."""
         a = np.ascontiguousarray(steps, dtype=np.int64)
         _check(lib().hf_case_set_step_limits(self.h, a.ctypes.data_as(C.POINTER(C.c_int64)), a.size))
+
+    def instance_failures(self) -> np.ndarray:
+        """Under step limits: each instance's first failed step's status (0: none)."""
+        a = np.zeros(self.instances(), dtype=np.int32)
+        _check(lib().hf_case_instance_failures(self.h, a.ctypes.data_as(C.POINTER(C.c_int32)), a.size))
+        return a
 
     def set_timestep(self, dt) -> None:
         a = np.ascontiguousarray(np.atleast_1d(dt), dtype=np.float64)

@@ -12,7 +12,9 @@ stream, so a cohort formed from new arrivals overlaps the ones already running;
 a cohort is admitted while the device memory the running ones hold plus its
 estimate fits the HBM budget.  Fields stay on the device from admission until
 the request's steps are done; a finished request's fields are read back
-between chunks of steps, when its cohort's stream is idle.
+between chunks of steps, when its cohort's stream is idle.  A request whose
+step fails (a NaN, a Poisson solve that does not converge) is frozen by the
+engine at that step and fails alone; the rest of its cohort goes on.
 
 Each instance's reductions are deterministic and per instance (see
 hf_pcg.cuh), so a request's result does not depend on the other requests of
@@ -203,7 +205,8 @@ class BatchServer:
             r.t_done = time.perf_counter()
             r.done = True
             r.prog = None
-            self.cell_steps += int(r.steps) * int(c.prog.cell_off[i + 1] - c.prog.cell_off[i])
+            if status == 0:
+                self.cell_steps += int(r.steps) * int(c.prog.cell_off[i + 1] - c.prog.cell_off[i])
             self.cv.notify_all()
 
     def _run(self) -> None:
@@ -236,18 +239,32 @@ class BatchServer:
                 if c.inflight:
                     if not c.event.query():
                         continue
-                    status = 0
+                    status, error, failures = 0, "", None
                     try:
                         c.case.synchronize()
                     except engine.EngineError as e:
-                        status = e.code
+                        status, error = e.code, str(e)
+                        try:
+                            failures = c.case.instance_failures()
+                        except engine.EngineError:
+                            failures = None
                     c.done_steps += c.inflight
                     c.inflight = 0
                     progressed = True
+                    # a failed instance is frozen by the engine and fails its
+                    # request alone; any other error ends the cohort
+                    whole = status != 0 and (failures is None or not failures.any())
                     for i, r in enumerate(c.reqs):
-                        if not r.done and (r.steps <= c.done_steps or status):
-                            self._finish(c, i, r, status)
-                    if c.done_steps >= c.total or status:
+                        if r.done:
+                            continue
+                        if whole:
+                            self._finish(c, i, r, status, error)
+                        elif failures is not None and failures[i]:
+                            self._finish(c, i, r, int(failures[i]), error)
+                        elif r.steps <= c.done_steps:
+                            self._finish(c, i, r)
+                    c.total = max([r.steps for r in c.reqs if not r.done], default=c.done_steps)
+                    if c.done_steps >= c.total:
                         c.case.close()
                         self.cohorts.remove(c)
                         continue

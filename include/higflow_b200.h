@@ -75,8 +75,9 @@ enum { HF_EXPLICIT_EULER = 0, HF_EXPLICIT_RK2 = 1, HF_EXPLICIT_RK3 = 2, HF_SEMI_
 /* precision forms */
 enum {
     HF_PREC_FP64 = 0,   /* plain: every gather, update and Poisson iterate in FP64 */
-    HF_PREC_MIXED = 1   /* velocity-stage stencil rows with FP32 weights and
-                           FP32 accumulation; the Poisson solve as FP32 AMG-CG
+    HF_PREC_MIXED = 1   /* velocity-stage stencil rows with FP32 weights
+                           (FP64 field values and sums), FP32 CUBISTA
+                           convection; the Poisson solve as FP32 AMG-CG
                            sweeps (operator, vectors, V-cycle in FP32) inside
                            FP64 iterative refinement: after each sweep the
                            FP64 unknown takes the correction and the FP64
@@ -373,8 +374,15 @@ int  hf_case_set_timestep(hf_case *c, const double *dt, int32_t n);
  * n = ninst.  Each frozen instance's fields stay those of its last step, so
  * its result is the same as when it runs alone for steps[i] steps.  Needs the
  * CG Poisson path and an explicit velocity scheme (HF_ERR_UNSUPPORTED
- * otherwise). */
+ * otherwise).  Once limits are set, an instance whose step fails (a NaN, a
+ * Poisson solve that does not converge) is frozen after that step and the
+ * others go on; the step call still returns the first failure. */
 int  hf_case_set_step_limits(hf_case *c, const int64_t *steps, int32_t n);
+
+/* Under step limits: each instance's first failed step's status (0: none so
+ * far; HF_ERR_NAN, HF_ERR_NOT_CONVERGED), n = ninst.  Waits for the case's
+ * stream. */
+int  hf_case_instance_failures(hf_case *c, int32_t *status, int32_t n);
 
 /* The CUDA stream every kernel of this case runs on (a cudaStream_t). */
 int  hf_case_stream(hf_case *c, void **stream);

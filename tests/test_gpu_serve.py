@@ -115,3 +115,32 @@ def test_batch_server_results_are_the_same_alone_and_in_the_mix():
         for k in alone:
             err = np.linalg.norm(alone[k] - mix[k]) / max(np.linalg.norm(alone[k]), 1e-300)
             assert err < 1e-10, (k, err)
+
+
+def test_batch_server_failing_request_fails_alone():
+    """A request whose fields hold a NaN fails with HF_ERR_NAN; the engine
+    freezes its instance and the rest of its cohort finishes unchanged."""
+    from higflow_b200 import serve
+    reqs = _requests()[:4]
+    opts = engine.options(rtol=1e-13, atol=1e-300)
+    bad = {k: v.copy() for k, v in reqs[1][3].items()}
+    bad[(hp.FIELD_U, 0)][7] = np.nan
+    srv = serve.BatchServer(opts=opts, max_cohorts=1, chunk=2)
+    ids = [srv.submit(prog, steps, bad if k == 1 else fields) for k, (prog, _, steps, fields) in enumerate(reqs)]
+    statuses = [srv.wait(rid, timeout=300)[0] for rid in ids]
+    assert statuses == [0, -4, 0, 0]
+    got = {k: {key: srv.get(ids[k], *key) for key in _fields(lambda f, c: None, reqs[k][0])} for k in (0, 2, 3)}
+    st = srv.stats()
+    srv.close()
+    assert st["cell_steps"] == sum(reqs[k][0].ncell * reqs[k][2] for k in (0, 2, 3))
+    for k in (0, 2, 3):
+        prog, _, steps, fields = reqs[k]
+        case = engine.Case(prog, opts)
+        for key, v in fields.items():
+            case.set(*key, v)
+        case.step(steps)
+        alone = _fields(case.get, prog)
+        case.close()
+        for key in alone:
+            err = np.linalg.norm(alone[key] - got[k][key]) / max(np.linalg.norm(alone[key]), 1e-300)
+            assert err < 1e-10, (k, key, err)
