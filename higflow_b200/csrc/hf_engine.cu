@@ -70,6 +70,59 @@ constexpr int kBlock = 256;
 // ---------------------------------------------------------------------------
 // device data
 // ---------------------------------------------------------------------------
+// A set of (general row, field read) pairs that k_vrows evaluates once per
+// use into val: pair u's value is -rhs[u] + sum_k w_k * field(tag[u])[col_k]
+// in stencil order (dp_interpolate_from_stencil, pdomain.c:1026-1053).  Slot
+// codes of the kernels that read them index the pairs.  Sliced layout
+// (SELL-32): pair u is lane u % 32 of slice u / 32, and its entry k sits at
+// sptr[u / 32] + 32 k + u % 32, so a warp's k-th entries are one coalesced
+// load; plen[u] is the pair's entry count.  Columns are absolute (row base
+// added) in scol, or, when every pair's entries lie within +-32767 of its
+// first column pcol0[u] (interpolation stencils are local: 2D meshes up to
+// several thousand cells a side), 16-bit offsets in scol16 (scol null).
+// Weights are FP64 (sw) or FP32 (sw32, the mixed form's velocity rows).
+struct PairRows {
+    int n;
+    const uint8_t *tag;
+    const double *rhs;
+    const int64_t *sptr;
+    const uint8_t *plen;
+    const int32_t *scol;
+    const int16_t *scol16;
+    const int32_t *pcol0;
+    const double *sw;
+    const float *sw32;
+    double *val;
+};
+
+// The mixed form's velocity-stage pairs by FP32 pattern.  The interpolation
+// weights HigTree computes for each row differ from row to row in their last
+// bits (each row is fitted at its own coordinates) and list the stencil's
+// points in a row-dependent order; with the entries in column order and the
+// weights in FP32, most rows share a few (column offsets, weights) patterns:
+// on 16 of the batched Giesekus cavities 7,368 patterns cover 1.16 M rows
+// (50.5 M entries).  The pairs keep their order (consecutive pairs are
+// consecutive facets of one slot: a warp's field gathers touch about 9
+// sectors per entry, and its 32 pairs use about 3.6 patterns), each reads its
+// pattern's (offset, weight) entries from the small table that stays in L1/L2
+// instead of streaming its own columns and weights from HBM.  The sum runs
+// in column order: FP64 values times FP32 weights, summed in FP64.
+struct PatEntry {
+    int32_t off;            // column offset from the pair's first column
+    float w;                // FP32 weight
+};
+struct PatRows {
+    int n;                  // pairs (the velocity pair set's order)
+    const int32_t *pid;     // per pair: its pattern
+    const int32_t *col0;    // ... the absolute column of offset 0 (its row's smallest)
+    const uint8_t *tag;     // ... the field it reads
+    const double *rhs;      // ... its row's boundary term
+    const int32_t *pstart;  // per pattern: first entry
+    const uint8_t *plen;    // per pattern: entry count
+    const PatEntry *ent;
+    double *val;
+};
+
 struct DevProg {
     int D, ncell, nf[3], off[4];
     hf_params par;
@@ -81,27 +134,16 @@ struct DevProg {
     const uint16_t *vdelta[3];
     int vns;
     // general rows of the velocity stage, one per (row, field read) pair: the
-    // velocity slot codes index these pairs; k_vrows evaluates them into rowval
+    // velocity slot codes index these pairs (vrow: the same rows for
+    // hf::query), evaluated by k_vrows at the start of the stage
     hf::Rows<double> vrow;
-    const uint8_t *vtag;
-    int nvrows;
-    double *rowval;
-    // the same pairs for k_vrows in a sliced layout (SELL-32): pair u is lane
-    // u % 32 of slice u / 32, and its entry k sits at sptr[u / 32] + 32 k +
-    // u % 32, so a warp's k-th entries are one coalesced load; the column is
-    // absolute (row base added), plen[u] is the pair's entry count.  The
-    // weights are FP64 (plain) or FP32 (mixed: sw32, FP32 accumulation).
-    const int64_t *sptr;
-    const uint8_t *plen;
-    const int32_t *scol;
-    const double *sw;
-    const float *sw32;
-    // the columns as 16-bit offsets from the pair's first column (pcol0), when
-    // every pair's entries lie within +-32767 of it (interpolation stencils
-    // are local: 2D meshes up to several thousand cells a side); scol16 null
-    // otherwise
-    const int16_t *scol16;
-    const int32_t *pcol0;
+    PairRows vr;
+    // general rows of the viscoelastic cell stage (velocity at the cell's
+    // faces and corners, the kernel's neighbours; FP64 weights in both
+    // forms), evaluated by k_vrows ahead of k_ve_cell: negative cell slot
+    // codes index cr.val (a kernel query's pair is the first of the upper
+    // triangle's components, which follow it in row-major order)
+    PairRows cr;
     // semi-implicit Euler: the velocity kernel writes each direction's
     // right-hand side, u + dt (sources - grad p [+ div S] - conv) plus the
     // system's boundary part sie_bc, into sie_b instead of u*
@@ -262,8 +304,9 @@ __device__ __forceinline__ const double *vslot_field(const DevFields &F, int d, 
     return d == 0 ? F.S[d2] : d == 1 ? F.S[D + d2] : F.S[(D - 1) * D + d2];
 }
 
-// field of a velocity-stage general row by tag: 0-2 FU[d], 3 p, 4 F, 5-7 u[d],
-// 8-16 S[d * D + d2] (switches: a dynamic index would copy the parameters)
+// field of a general-row pair by tag: 0-2 FU[d], 3 p, 4 F, 5-7 u[d], 8-16
+// S[d * D + d2], 17-25 K[d * D + d2] (switches: a dynamic index would copy
+// the parameters)
 
 __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 {
@@ -284,44 +327,74 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
     case 13: return F.S[5];
     case 14: return F.S[6];
     case 15: return F.S[7];
-    default: return F.S[8];
+    case 16: return F.S[8];
+    case 17: return F.K[0];
+    case 18: return F.K[1];
+    case 19: return F.K[2];
+    case 20: return F.K[3];
+    case 21: return F.K[4];
+    case 22: return F.K[5];
+    case 23: return F.K[6];
+    case 24: return F.K[7];
+    default: return F.K[8];
     }
 }
 
-// The general rows the velocity stage reads, one thread per (row, field)
-// pair: the long interpolation stencils (tens of entries) run here, coalesced
-// and without divergence, instead of inside the per-facet kernel.  Entry k of
-// the 32 pairs of a warp is one 128-byte column load and one 256-byte (FP64)
-// or 128-byte (FP32) weight load; the sum is dp_interpolate_from_stencil's
-// (pdomain.c:1026-1053): -rhs, then the entries in stencil order.  W = float
-// is the mixed form: FP32 weights (half the weight stream), FP64 field values
-// and FP64 accumulation.  Rounding the field values or the sum to FP32 puts
-// noise of about 1e-7 of the velocity into every step's Poisson right-hand
-// side that the extrapolated initial guess cannot follow: measured on the
-// batched Giesekus cavities at Poisson rtol 1e-6, 7.2 CG iterations per
-// instance-step against 4.4 with FP64 sums (4.0 for the plain form).
+// General-row pairs (PairRows), one thread per pair: the long interpolation
+// stencils (tens of entries) run here, coalesced and without divergence,
+// instead of inside the per-facet and per-cell kernels.  Entry k of the 32
+// pairs of a warp is one 128-byte (or 64-byte, 16-bit) column load and one
+// 256-byte (FP64) or 128-byte (FP32) weight load; the sum is
+// dp_interpolate_from_stencil's (pdomain.c:1026-1053): -rhs, then the entries
+// in stencil order, in FP64.  W = float reads FP32 weights (the mixed form's
+// velocity rows: half the weight stream) and still sums FP64 field values in
+// FP64: rounding the values or the sum to FP32 puts noise of about 1e-7 of the
+// velocity into every step's Poisson right-hand side that the extrapolated
+// initial guess cannot follow (measured on the batched Giesekus cavities at
+// Poisson rtol 1e-6: 7.2 CG iterations per instance-step against 4.4 with
+// FP64 sums, 4.0 for the plain form).
 // (launch bounds of the largest block size the tuner tries)
 template <typename W, bool C16>
-__global__ void __launch_bounds__(512) k_vrows(DevProg P, DevFields F)
+__global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= P.nvrows) return;
-    const double *__restrict__ fb = vtag_field(F, __ldg(P.vtag + u));
-    if (C16) fb += __ldg(P.pcol0 + u);
-    const int n = __ldg(P.plen + u);
-    const int64_t e0 = __ldg(P.sptr + (u >> 5)) + (u & 31);
-    const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)P.sw32 : (const W *)P.sw;
+    if (u >= R.n) return;
+    const double *__restrict__ fb = vtag_field(F, __ldg(R.tag + u));
+    if (C16) fb += __ldg(R.pcol0 + u);
+    const int n = __ldg(R.plen + u);
+    const int64_t e0 = __ldg(R.sptr + (u >> 5)) + (u & 31);
+    const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)R.sw32 : (const W *)R.sw;
     double res = 0.0;
-    res += -__ldg(P.vrow.rhs + u);
+    res += -__ldg(R.rhs + u);
     // the entries stream through once (evict-first loads keep L1 for the
     // field gathers); eight entries' loads in flight per thread
 #pragma unroll 8
     for (int k = 0; k < n; k++) {
         const int64_t at = e0 + 32 * (int64_t)k;
-        const int c = C16 ? (int)__ldcs(P.scol16 + at) : __ldcs(P.scol + at);
+        const int c = C16 ? (int)__ldcs(R.scol16 + at) : __ldcs(R.scol + at);
         res += __ldg(fb + c) * (double)__ldcs(w + at);
     }
-    P.rowval[u] = res;
+    R.val[u] = res;
+}
+
+// PatRows: one thread per pair; -rhs, then the pattern's entries in column
+// order, FP64 values times FP32 weights summed in FP64.
+__global__ void __launch_bounds__(512) k_vrows_pat(PatRows R, DevFields F)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= R.n) return;
+    const int p = __ldg(R.pid + u);
+    const double *__restrict__ fb = vtag_field(F, __ldg(R.tag + u)) + __ldg(R.col0 + u);
+    const int e0 = __ldg(R.pstart + p), n = __ldg(R.plen + p);
+    const int2 *__restrict__ ent = reinterpret_cast<const int2 *>(R.ent) + e0;
+    double res = 0.0;
+    res += -__ldg(R.rhs + u);
+#pragma unroll 4
+    for (int k = 0; k < n; k++) {
+        const int2 e = __ldg(ent + k);
+        res += __ldg(fb + e.x) * (double)__int_as_float(e.y);
+    }
+    R.val[u] = res;
 }
 
 // CUBISTA convective flux of the facet velocity along one direction
@@ -429,7 +502,7 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     for (int s = 0; s < NS; s++) {
         const bool unused = s >= HF_V_BLK0 && s < HF_V_NSLOT_NEWT(D) && (s - HF_V_BLK0) % HF_V_NB < 4 &&
                             (s - HF_V_BLK0) / HF_V_NB == d;   // u[d] corners of the facet's own direction
-        const double *src = code[s] >= 0 ? vslot_field<D>(F, d, s) + code[s] : P.rowval + (-code[s] - 1);
+        const double *src = code[s] >= 0 ? vslot_field<D>(F, d, s) + code[s] : P.vr.val + (-code[s] - 1);
         val[s] = unused ? 0.0 : __ldg(src);
     }
 #define SLQ(s, fld) (val[s])
@@ -648,7 +721,6 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
     const int cc = blockIdx.x * blockDim.x + threadIdx.x;
     if (cc >= P.ncell) return;
     const int n = P.ncell;
-    const hf::Rows<double> &R = P.rows;
 #define CS(s) __ldg(P.cslots + (size_t)(s) * n + cc)
     const double *cd = P.delta + (size_t)__ldg(P.cdelta + cc) * D;
     const uint32_t fl = __ldg(P.cflags + cc);
@@ -663,8 +735,8 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
     // The velocity values this cell reads: its face velocities (u[dim] at
     // -/+ half a cell, UVL/UVR) and the Du corner queries (HF_C_NQ per ordered
     // pair dim != dim2, on u[dim]).  All slot codes, then all values as
-    // independent loads; general rows (cells at boundaries) are fixed up
-    // afterwards, out of line.
+    // independent loads: a centre hit from the field, a general row (cells at
+    // boundaries) from its cell-stage pair, which k_vrows evaluated.
     constexpr int NU = 2 * D, NQ = HF_C_NQ * D * (D - 1);
     int32_t cu[NU + NQ];
     double vu[NU + NQ];
@@ -673,10 +745,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
     for (int k = 0; k < NU + NQ; k++) cu[k] = CS(uslot(k));
 #pragma unroll
-    for (int k = 0; k < NU + NQ; k++) vu[k] = cu[k] >= 0 ? __ldg(ufield(k) + cu[k]) : 0.0;
-#pragma unroll
-    for (int k = 0; k < NU + NQ; k++)
-        if (cu[k] < 0) vu[k] = hf::query_row(R, cu[k], ufield(k));
+    for (int k = 0; k < NU + NQ; k++) vu[k] = cu[k] >= 0 ? __ldg(ufield(k) + cu[k]) : __ldg(P.cr.val + (-cu[k] - 1));
     // velocity at the faces of this cell, shared by Du, u_c and the CUBISTA flux
     double vl[D], vr[D];
 #pragma unroll
@@ -814,8 +883,9 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
             RHS[i][j] = ok - ko + 2.0 * BB[i][j] + MM[i][j] / De;
         }
     // the kernel's neighbour values: per direction KL, KR, KLL, KRR (the same
-    // codes for every component), loaded component by component, all
-    // directions at once
+    // codes for every component; a general row's pairs are the upper
+    // triangle's components in row-major order), loaded component by
+    // component, all directions at once
     // (KLL/KRR are loaded for every cell, so that no load waits for the
     // instance's parameters; without CUBISTA their values go unused)
     const bool cub = pr.ve_convecdiscrtype == HF_CELL_CUBISTA;
@@ -829,12 +899,10 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
         for (int j = i; j < D; j++) {
             const double *Kf = F.K[i * D + j];
+            const int m = i * D - i * (i - 1) / 2 + (j - i);   // upper-triangle index of (i, j)
             double kv[4 * D];
 #pragma unroll
-            for (int k = 0; k < 4 * D; k++) kv[k] = ck[k] >= 0 ? __ldg(Kf + ck[k]) : 0.0;
-#pragma unroll
-            for (int k = 0; k < 4 * D; k++)
-                if (ck[k] < 0 && ((k & 3) < 2 || cub)) kv[k] = hf::query_row(R, ck[k], Kf);
+            for (int k = 0; k < 4 * D; k++) kv[k] = ck[k] >= 0 ? __ldg(Kf + ck[k]) : __ldg(P.cr.val + (-ck[k] - 1) + m);
             double rhs = 0.0;
 #pragma unroll
             for (int dim = 0; dim < D; dim++) {
@@ -1338,7 +1406,10 @@ struct hf_case {
     cudaGraph_t graph[2] = {};
     cudaGraphExec_t exec[2] = {};
     int64_t ntemplates = 0;         // row templates of the finest Poisson operator
-    int64_t vel_entries = 0;        // stored entries of the velocity-stage rows (padded slices)
+    int64_t vel_entries = 0;        // stored entries of the velocity-stage rows (padded slices; patterns)
+    bool vmix = false;              // mixed form's velocity and cell stages (FP32 weights, FP32 CUBISTA)
+    PatRows vp = {};                // mixed form: the velocity-stage pairs by FP32 pattern
+    int64_t cell_entries = 0;       // ... and of the cell-stage rows
     int64_t *ilim = nullptr;        // per-instance step limits on the device (null: none)
     // launch shapes of the tuned kernels (hf_options.tuning): k_vrows,
     // k_velocity, k_ve_cell block sizes; tuned before the first step
@@ -1422,7 +1493,10 @@ int build_matrix(const hf_program *pg, const std::vector<int> &pins, std::vector
         if (col.size() > (size_t)INT32_MAX) return fail(HF_ERR_UNSUPPORTED, "Poisson matrix too large for int32 indexing");
         ptr[r + 1] = (int32_t)col.size();
     }
-    // symmetry check: every (r, c, v) must have a matching (c, r, v)
+    // symmetry check: every (r, c, v) must have a matching (c, r, v) up to
+    // the rounding of HigTree's weights, which grows with the mesh (up to
+    // 1.4e-13 relative measured on 512^2 cavities and 640 x 160 channels);
+    // rows that are structurally non-symmetric differ at O(1)
     symmetric = true;
     for (int r = 0; r < n && symmetric; r++) {
         for (int k = ptr[r]; k < ptr[r + 1]; k++) {
@@ -1431,7 +1505,7 @@ int build_matrix(const hf_program *pg, const std::vector<int> &pins, std::vector
             bool found = false;
             for (int m = ptr[c]; m < ptr[c + 1]; m++)
                 if (col[m] == r) {
-                    found = fabs(val[m] - val[k]) <= 1e-13 * fabs(val[k]);
+                    found = fabs(val[m] - val[k]) <= 1e-10 * fabs(val[k]);
                     break;
                 }
             if (!found) { symmetric = false; break; }
@@ -2282,12 +2356,37 @@ void record(hf_case *C, int phase, int end)
     else cudaEventRecord(C->ev[2 * phase + end], C->stream);
 }
 
+// k_vrows over one pair set at the case's block size for it
+void enqueue_pairs(hf_case *C, const PairRows &R, const DevFields &F, cudaStream_t st)
+{
+    const int bs = C->blk_vrows, nb = (R.n + bs - 1) / bs;
+    const bool c16 = R.scol16 != nullptr;
+    if (R.sw32) {
+        if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(R, F);
+        else k_vrows<float, false><<<nb, bs, 0, st>>>(R, F);
+    } else {
+        if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(R, F);
+        else k_vrows<double, false><<<nb, bs, 0, st>>>(R, F);
+    }
+}
+
+// the velocity stage's general rows: by pattern (mixed form) or sliced
+void enqueue_vrows(hf_case *C, const DevFields &F, cudaStream_t st)
+{
+    if (C->vp.n) {
+        const int bs = C->blk_vrows, nb = (C->vp.n + bs - 1) / bs;
+        k_vrows_pat<<<nb, bs, 0, st>>>(C->vp, F);
+    } else {
+        enqueue_pairs(C, C->P.vr, F, st);
+    }
+}
+
 // The viscoelastic cell stage's main kernel at the case's block size
 template <int D>
 void enqueue_ve_cell(hf_case *C, const DevFields &F, cudaStream_t st)
 {
     const int vb = C->blk_ve, nb = (C->P.ncell + vb - 1) / vb;
-    const bool mix = C->P.sw32 != nullptr;
+    const bool mix = C->vmix;
     if (C->par.ve_discrtype == HF_VE_IMPLICIT) {
         if (mix) k_ve_cell<D, true, true><<<nb, vb, 0, st>>>(C->P, F);
         else k_ve_cell<D, true, false><<<nb, vb, 0, st>>>(C->P, F);
@@ -2341,22 +2440,14 @@ int autotune(hf_case *C)
         slot = keep;
     };
     const DevFields F = C->F;
-    // k_vrows alone (the facet kernel reads its output)
-    if (C->P.nvrows) {
-        pick(C->blk_vrows, {128, 256, 512}, [&]() {
-            const int bs = C->blk_vrows, nb = (C->P.nvrows + bs - 1) / bs;
-            const bool c16 = C->P.scol16 != nullptr;
-            if (C->P.sw32) {
-                if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(C->P, F);
-                else k_vrows<float, false><<<nb, bs, 0, st>>>(C->P, F);
-            } else {
-                if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(C->P, F);
-                else k_vrows<double, false><<<nb, bs, 0, st>>>(C->P, F);
-            }
-        });
-    }
+    // k_vrows alone on the velocity-stage pairs (the facet kernel reads its
+    // output); the cell-stage pairs are evaluated once for k_ve_cell's trials
+    if (C->P.vr.n) pick(C->blk_vrows, {128, 256, 512}, [&]() { enqueue_vrows(C, F, st); });
     if (!C->sie) pick(C->blk_vel, {64, 128, 256}, [&]() { enqueue_velocity<D>(C, F, st); });
-    if (C->par.flowtype == HF_VISCOELASTIC) pick(C->blk_ve, {64, 128}, [&]() { enqueue_ve_cell<D>(C, F, st); });
+    if (C->par.flowtype == HF_VISCOELASTIC) {
+        if (C->P.cr.n) enqueue_pairs(C, C->P.cr, F, st);
+        pick(C->blk_ve, {64, 128}, [&]() { enqueue_ve_cell<D>(C, F, st); });
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     HF_CK(cudaStreamSynchronize(st));
@@ -2378,22 +2469,14 @@ int enqueue_velocity(hf_case *C, const DevFields &F, cudaStream_t st)
 {
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     int n = 0;
-    if (C->P.nvrows) {
+    if (C->P.vr.n) {
         record(C, HF_PHASE_VELOCITY_ROWS, 0);
-        const int bs = C->blk_vrows, nb = (C->P.nvrows + bs - 1) / bs;
-        const bool c16 = C->P.scol16 != nullptr;
-        if (C->P.sw32) {
-            if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(C->P, F);
-            else k_vrows<float, false><<<nb, bs, 0, st>>>(C->P, F);
-        } else {
-            if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(C->P, F);
-            else k_vrows<double, false><<<nb, bs, 0, st>>>(C->P, F);
-        }
+        enqueue_vrows(C, F, st);
         record(C, HF_PHASE_VELOCITY_ROWS, 1);
         n++;
     }
     const int vb = C->blk_vel, nb = (C->nfacet_total + vb - 1) / vb;
-    const bool mix = C->P.sw32 != nullptr;
+    const bool mix = C->vmix;
     if (ve) {
         if (mix) k_velocity<D, true, true><<<nb, vb, 0, st>>>(C->P, F);
         else k_velocity<D, true, false><<<nb, vb, 0, st>>>(C->P, F);
@@ -2421,6 +2504,10 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
         record(C, HF_PHASE_VE_CELL, 0);
         if (C->gptt) {
             k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
+            fixed++;
+        }
+        if (C->P.cr.n) {
+            enqueue_pairs(C, C->P.cr, F, st);
             fixed++;
         }
         enqueue_ve_cell<D>(C, F, st);
@@ -2628,15 +2715,15 @@ int collect_phases(hf_case *C)
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     for (int p = 0; p < HF_NPHASE; p++) {
         if (p == HF_PHASE_VE_CELL && !ve) continue;
-        if (p == HF_PHASE_VELOCITY_ROWS && !C->P.nvrows) continue;
+        if (p == HF_PHASE_VELOCITY_ROWS && !C->P.vr.n) continue;
         float ms = 0.f;
         HF_CK(cudaEventElapsedTime(&ms, C->ev[2 * p], C->ev[2 * p + 1]));
         C->phase_ms[p] += ms;
     }
     const bool rk = C->par.tempdiscrtype == HF_EXPLICIT_RK2 || C->par.tempdiscrtype == HF_EXPLICIT_RK3;
-    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2 + (C->gptt ? 1 : 0);
-    C->phase_launches[HF_PHASE_VELOCITY] += 1 + (C->P.nvrows ? 1 : 0) + (rk ? 1 : 0);
-    if (C->P.nvrows) C->phase_launches[HF_PHASE_VELOCITY_ROWS] += 1;
+    if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2 + (C->gptt ? 1 : 0) + (C->P.cr.n ? 1 : 0);
+    C->phase_launches[HF_PHASE_VELOCITY] += 1 + (C->P.vr.n ? 1 : 0) + (rk ? 1 : 0);
+    if (C->P.vr.n) C->phase_launches[HF_PHASE_VELOCITY_ROWS] += 1;
     C->phase_launches[HF_PHASE_POISSON_INIT] += 2;
     C->phase_launches[HF_PHASE_POISSON_ITER] += (C->h_ctl->total_bodies - C->bodies0) * C->body_kernels;
     C->phase_launches[HF_PHASE_FINAL] += 2;
@@ -2691,6 +2778,10 @@ int bicg_step(hf_case *C)
         PhaseTimer t(C, HF_PHASE_VE_CELL, launches);
         if (C->gptt) {
             k_gptt_ml<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, C->F);
+            launches++;
+        }
+        if (C->P.cr.n) {
+            enqueue_pairs(C, C->P.cr, C->F, st);
             launches++;
         }
         // (the BiCGStab path is plain FP64: the mixed form needs the CG solver)
@@ -2798,6 +2889,159 @@ extern "C" int hf_case_device_bytes(const hf_program *pg, const hf_options *opt,
     if (pg->par.flowtype == HF_VISCOELASTIC) b += (int64_t)pg->ncell * 8 * 4 * D * D;
     b += (int64_t)pg->ncell * 8 * 10;                                // solver vectors
     *bytes = b;
+    return HF_OK;
+}
+
+// A pair set's sliced layout (PairRows) from its rows, uploaded on the case
+// stream into device memory the case owns: fills R except rhs; entries = the
+// stored (padded) entry count.  A slice holds 32 consecutive pairs padded to
+// its longest; consecutive pairs are consecutive elements of one slot, so
+// lengths within a slice rarely differ.  fp32: FP32 weights.
+int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_program *pg,
+                const std::vector<int32_t> &ptmpl, const std::vector<int32_t> &pbase,
+                const std::vector<double> &prhs, const std::vector<uint8_t> &ptag, bool fp32, PairRows &R,
+                int64_t &entries, const char *what)
+{
+    (void)prhs;
+    int rc;
+    const size_t np = ptmpl.size(), nsl = (np + 31) / 32;
+    R.n = (int)np;
+    std::vector<int64_t> sptr(nsl + 1, 0);
+    std::vector<uint8_t> plen(np);
+    for (size_t sl = 0; sl < nsl; sl++) {
+        int64_t mx = 0;
+        for (size_t u = sl * 32; u < std::min(np, sl * 32 + 32); u++) {
+            const int64_t len = pg->tmpl_ptr[ptmpl[u] + 1] - pg->tmpl_ptr[ptmpl[u]];
+            if (len > 255) return fail(HF_ERR_UNSUPPORTED, std::string(what) + " stencil longer than 255 entries");
+            plen[u] = (uint8_t)len;
+            mx = std::max(mx, len);
+        }
+        sptr[sl + 1] = sptr[sl] + 32 * mx;
+    }
+    const size_t ne = (size_t)sptr[nsl];
+    // the columns: 16-bit offsets from the pair's first column when every
+    // pair's entries stay within +-32767 of it, else 32-bit
+    bool c16 = true;
+    std::vector<int32_t> pcol0(np, 0);
+    for (size_t u = 0; u < np && c16; u++) {
+        const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
+        pcol0[u] = plen[u] ? pbase[u] + pg->tmpl_col[a0] : 0;
+        for (int k = 0; k < plen[u]; k++) {
+            const int64_t d = (int64_t)pbase[u] + pg->tmpl_col[a0 + k] - pcol0[u];
+            if (d < -32767 || d > 32767) { c16 = false; break; }
+        }
+    }
+    std::vector<int32_t> scol(c16 ? 0 : ne, 0);
+    std::vector<int16_t> scol16(c16 ? ne : 0, 0);
+    std::vector<double> sw;
+    std::vector<float> sw32;
+    if (fp32) sw32.assign(ne, 0.f);
+    else sw.assign(ne, 0.0);
+    for (size_t u = 0; u < np; u++) {
+        const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
+        int64_t at = sptr[u / 32] + (int64_t)(u % 32);
+        for (int k = 0; k < plen[u]; k++, at += 32) {
+            const int64_t c = (int64_t)pbase[u] + pg->tmpl_col[a0 + k];
+            if (c < 0 || c > INT32_MAX) return fail(HF_ERR_INVALID, std::string(what) + " column out of range");
+            if (c16) scol16[at] = (int16_t)(c - pcol0[u]);
+            else scol[at] = (int32_t)c;
+            if (fp32) sw32[at] = (float)pg->tmpl_w[a0 + k];
+            else sw[at] = pg->tmpl_w[a0 + k];
+        }
+    }
+    R.scol = nullptr;
+    R.scol16 = nullptr;
+    R.pcol0 = nullptr;
+    R.sw = nullptr;
+    R.sw32 = nullptr;
+    if ((rc = upload(own, (int64_t **)&R.sptr, sptr.data(), sptr.size(), B, C->stream))) return rc;
+    if ((rc = upload(own, (uint8_t **)&R.plen, plen.data(), plen.size(), B, C->stream))) return rc;
+    if (c16) {
+        if ((rc = upload(own, (int16_t **)&R.scol16, scol16.data(), scol16.size(), B, C->stream))) return rc;
+        if ((rc = upload(own, (int32_t **)&R.pcol0, pcol0.data(), pcol0.size(), B, C->stream))) return rc;
+    } else {
+        if ((rc = upload(own, (int32_t **)&R.scol, scol.data(), scol.size(), B, C->stream))) return rc;
+    }
+    if (fp32) {
+        if ((rc = upload(own, (float **)&R.sw32, sw32.data(), sw32.size(), B, C->stream))) return rc;
+    } else {
+        if ((rc = upload(own, (double **)&R.sw, sw.data(), sw.size(), B, C->stream))) return rc;
+    }
+    if ((rc = upload(own, (uint8_t **)&R.tag, ptag.data(), ptag.size(), B, C->stream))) return rc;
+    if ((rc = upload(own, &R.val, (const double *)nullptr, np, B, C->stream))) return rc;
+    entries = (int64_t)ne;
+    // wait for the uploads before the host staging vectors go away
+    if (cudaStreamSynchronize(C->stream) != cudaSuccess) return fail(HF_ERR_CUDA, std::string(what) + " rows");
+    return HF_OK;
+}
+
+// The mixed form's velocity pairs by FP32 pattern (PatRows), uploaded on the
+// case stream: R (the velocity pair set) gets its count and result array
+// only; entries = the patterns' entry count.
+int build_patterns(hf_case *C, std::vector<void *> &own, double &B, const hf_program *pg,
+                   const std::vector<int32_t> &ptmpl, const std::vector<int32_t> &pbase,
+                   const std::vector<double> &prhs, const std::vector<uint8_t> &ptag, PairRows &R, PatRows &V,
+                   int64_t &entries)
+{
+    int rc;
+    const size_t np = ptmpl.size();
+    R.n = V.n = (int)np;
+    // the pattern of every template the pairs use: its entries in column
+    // order (weight bits breaking ties), offsets from its smallest column,
+    // FP32 weights, byte for byte
+    std::vector<int32_t> tpat(pg->ntmpl, -1), tmin(pg->ntmpl, 0), pstart;
+    std::vector<uint8_t> plen;
+    std::vector<PatEntry> ent;
+    std::unordered_map<std::string, int32_t> known;
+    std::string key;
+    std::vector<PatEntry> row;
+    for (size_t u = 0; u < np; u++) {
+        const int32_t t = ptmpl[u];
+        if (tpat[t] >= 0) continue;
+        const int64_t a = pg->tmpl_ptr[t], e = pg->tmpl_ptr[t + 1];
+        if (e - a > 255) return fail(HF_ERR_UNSUPPORTED, "velocity-stage stencil longer than 255 entries");
+        int32_t m = 0;
+        for (int64_t k = a; k < e; k++) m = k == a ? pg->tmpl_col[k] : std::min(m, pg->tmpl_col[k]);
+        row.clear();
+        for (int64_t k = a; k < e; k++) row.push_back({pg->tmpl_col[k] - m, (float)pg->tmpl_w[k]});
+        std::sort(row.begin(), row.end(), [](const PatEntry &x, const PatEntry &y) {
+            if (x.off != y.off) return x.off < y.off;
+            uint32_t bx, by;
+            memcpy(&bx, &x.w, 4);
+            memcpy(&by, &y.w, 4);
+            return bx < by;
+        });
+        key.assign((const char *)row.data(), row.size() * sizeof(PatEntry));
+        auto it = known.find(key);
+        if (it == known.end()) {
+            if (ent.size() + row.size() > (size_t)INT32_MAX) return fail(HF_ERR_UNSUPPORTED, "too many velocity-stage patterns");
+            it = known.emplace(key, (int32_t)pstart.size()).first;
+            pstart.push_back((int32_t)ent.size());
+            plen.push_back((uint8_t)row.size());
+            ent.insert(ent.end(), row.begin(), row.end());
+        }
+        tpat[t] = it->second;
+        tmin[t] = m;
+    }
+    std::vector<int32_t> pid(np), col0(np);
+    for (size_t u = 0; u < np; u++) {
+        const int64_t c = (int64_t)pbase[u] + tmin[ptmpl[u]];
+        if (c < 0 || c > INT32_MAX) return fail(HF_ERR_INVALID, "velocity-stage column out of range");
+        pid[u] = tpat[ptmpl[u]];
+        col0[u] = (int32_t)c;
+    }
+    if ((rc = upload(own, (int32_t **)&V.pid, pid.data(), np, B, C->stream))) return rc;
+    if ((rc = upload(own, (int32_t **)&V.col0, col0.data(), np, B, C->stream))) return rc;
+    if ((rc = upload(own, (uint8_t **)&V.tag, ptag.data(), np, B, C->stream))) return rc;
+    if ((rc = upload(own, (double **)&V.rhs, prhs.data(), np, B, C->stream))) return rc;
+    if ((rc = upload(own, (int32_t **)&V.pstart, pstart.data(), pstart.size(), B, C->stream))) return rc;
+    if ((rc = upload(own, (uint8_t **)&V.plen, plen.data(), plen.size(), B, C->stream))) return rc;
+    if ((rc = upload(own, (PatEntry **)&V.ent, ent.data(), ent.size(), B, C->stream))) return rc;
+    if ((rc = upload(own, &R.val, (const double *)nullptr, np, B, C->stream))) return rc;
+    V.val = R.val;
+    entries = (int64_t)ent.size();
+    // wait for the uploads before the host staging vectors go away
+    if (cudaStreamSynchronize(C->stream) != cudaSuccess) return fail(HF_ERR_CUDA, "velocity-stage patterns");
     return HF_OK;
 }
 
@@ -2989,83 +3233,70 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
             UP((uint32_t **)&P.vflags[d], pg->vel_flags[d], pg->nfacet[d]);
             UP((uint16_t **)&P.vdelta[d], pg->vel_delta[d], pg->nfacet[d]);
         }
-        P.nvrows = (int)ptmpl.size();
-        {
-            // sliced layout (see DevProg): a slice holds 32 consecutive pairs,
-            // padded to its longest; consecutive pairs are consecutive elements
-            // of one slot, so lengths within a slice rarely differ
-            const size_t np = ptmpl.size(), nsl = (np + 31) / 32;
-            std::vector<int64_t> sptr(nsl + 1, 0);
-            std::vector<uint8_t> plen(np);
-            for (size_t sl = 0; sl < nsl; sl++) {
-                int64_t mx = 0;
-                for (size_t u = sl * 32; u < std::min(np, sl * 32 + 32); u++) {
-                    const int64_t len = pg->tmpl_ptr[ptmpl[u] + 1] - pg->tmpl_ptr[ptmpl[u]];
-                    if (len > 255) return cleanup(fail(HF_ERR_UNSUPPORTED, "velocity-stage stencil longer than 255 entries"));
-                    plen[u] = (uint8_t)len;
-                    mx = std::max(mx, len);
-                }
-                sptr[sl + 1] = sptr[sl] + 32 * mx;
-            }
-            const size_t ne = (size_t)sptr[nsl];
-            // the columns: 16-bit offsets from the pair's first column when
-            // every pair's entries stay within +-32767 of it, else 32-bit
-            bool c16 = true;
-            std::vector<int32_t> pcol0(np, 0);
-            for (size_t u = 0; u < np && c16; u++) {
-                const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
-                pcol0[u] = plen[u] ? pbase[u] + pg->tmpl_col[a0] : 0;
-                for (int k = 0; k < plen[u]; k++) {
-                    const int64_t d = (int64_t)pbase[u] + pg->tmpl_col[a0 + k] - pcol0[u];
-                    if (d < -32767 || d > 32767) { c16 = false; break; }
-                }
-            }
-            std::vector<int32_t> scol(c16 ? 0 : ne, 0);
-            std::vector<int16_t> scol16(c16 ? ne : 0, 0);
-            std::vector<double> sw;
-            std::vector<float> sw32;
-            if (opt.precision == HF_PREC_MIXED) sw32.assign(ne, 0.f);
-            else sw.assign(ne, 0.0);
-            for (size_t u = 0; u < np; u++) {
-                const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
-                int64_t at = sptr[u / 32] + (int64_t)(u % 32);
-                for (int k = 0; k < plen[u]; k++, at += 32) {
-                    const int64_t c = (int64_t)pbase[u] + pg->tmpl_col[a0 + k];
-                    if (c < 0 || c > INT32_MAX) return cleanup(fail(HF_ERR_INVALID, "velocity-stage column out of range"));
-                    if (c16) scol16[at] = (int16_t)(c - pcol0[u]);
-                    else scol[at] = (int32_t)c;
-                    if (opt.precision == HF_PREC_MIXED) sw32[at] = (float)pg->tmpl_w[a0 + k];
-                    else sw[at] = pg->tmpl_w[a0 + k];
-                }
-            }
-            UP((int64_t **)&P.sptr, sptr.data(), sptr.size());
-            UP((uint8_t **)&P.plen, plen.data(), plen.size());
-            if (c16) {
-                UP((int16_t **)&P.scol16, scol16.data(), scol16.size());
-                UP((int32_t **)&P.pcol0, pcol0.data(), pcol0.size());
-            } else {
-                UP((int32_t **)&P.scol, scol.data(), scol.size());
-            }
-            if (opt.precision == HF_PREC_MIXED) UP((float **)&P.sw32, sw32.data(), sw32.size());
-            else UP((double **)&P.sw, sw.data(), sw.size());
-            C->vel_entries = (int64_t)ne;
-            // wait for the uploads before the host staging vectors go away
-            if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "velocity rows"));
-        }
+        C->vmix = opt.precision == HF_PREC_MIXED;
+        if (C->vmix) rc = build_patterns(C, own, B, pg, ptmpl, pbase, prhs, ptag, P.vr, C->vp, C->vel_entries);
+        else rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, false, P.vr, C->vel_entries, "velocity-stage");
+        if (rc) return cleanup(rc);
         P.vrow.tptr = P.rows.tptr;
         P.vrow.col = P.rows.col;
         P.vrow.w = P.rows.w;
         UP((int32_t **)&P.vrow.tmpl, ptmpl.data(), ptmpl.size());
         UP((int32_t **)&P.vrow.base, pbase.data(), pbase.size());
         UP((double **)&P.vrow.rhs, prhs.data(), prhs.size());
-        UP((uint8_t **)&P.vtag, ptag.data(), ptag.size());
-        UP(&P.rowval, (const double *)nullptr, ptmpl.size());
+        P.vr.rhs = P.vrow.rhs;
     }
     UP((int32_t **)&P.dslots, pg->div_slots, (size_t)2 * D * pg->ncell);
     UP((uint16_t **)&P.cdelta, pg->cell_delta, pg->ncell);
     if (pg->par.flowtype == HF_VISCOELASTIC) {
-        UP((int32_t **)&P.cslots, pg->cell_slots, (size_t)pg->cell_nslot * pg->ncell);
+        // cell slots: the general codes k_ve_cell reads renumbered to cell-stage
+        // pairs (velocity at the faces and corners on u[d]; the kernel's
+        // neighbours on each upper-triangle component, consecutive pairs)
+        const int64_t nc = pg->ncell;
+        std::vector<int32_t> cs(pg->cell_slots, pg->cell_slots + (size_t)pg->cell_nslot * nc);
+        std::vector<int32_t> ptmpl, pbase;
+        std::vector<double> prhs;
+        std::vector<uint8_t> ptag;
+        std::unordered_map<uint64_t, int32_t> seen;   // (row, first tag) -> first pair
+        bool overflow = false;
+        auto pairs_of = [&](int64_t r, const int *tags, int ntag) -> int32_t {
+            const uint64_t key = (uint64_t)r * 32 + (uint64_t)tags[0];
+            auto it = seen.find(key);
+            if (it != seen.end()) return it->second;
+            if (ptmpl.size() + ntag >= (size_t)INT32_MAX) overflow = true;
+            const int32_t first = (int32_t)ptmpl.size();
+            for (int m = 0; m < ntag; m++) {
+                ptmpl.push_back(pg->row_tmpl[r]);
+                pbase.push_back(pg->row_base[r]);
+                prhs.push_back(pg->row_rhs[r]);
+                ptag.push_back((uint8_t)tags[m]);
+            }
+            seen.emplace(key, first);
+            return first;
+        };
+        int ktags[6], nk = 0;
+        for (int i = 0; i < D; i++)
+            for (int j = i; j < D; j++) ktags[nk++] = 17 + i * D + j;
+        const int NU = 2 * D, NQ = HF_C_NQ * D * (D - 1);
+        for (int k = 0; k < NU + NQ; k++) {
+            const int slot = k < NU ? HF_C_BLK0 + HF_C_NB * (k >> 1) + (k & 1) : HF_C_BLK0 + HF_C_NB * D + (k - NU);
+            const int tag = 5 + (k < NU ? (k >> 1) : (k - NU) / (HF_C_NQ * (D - 1)));
+            int32_t *sl = cs.data() + (size_t)slot * nc;
+            for (int64_t c = 0; c < nc; c++)
+                if (sl[c] < 0) sl[c] = -pairs_of(-(int64_t)sl[c] - 1, &tag, 1) - 1;
+        }
+        for (int k = 0; k < 4 * D; k++) {
+            int32_t *sl = cs.data() + (size_t)(HF_C_BLK0 + HF_C_NB * (k >> 2) + HF_C_KL + (k & 3)) * nc;
+            for (int64_t c = 0; c < nc; c++)
+                if (sl[c] < 0) sl[c] = -pairs_of(-(int64_t)sl[c] - 1, ktags, nk) - 1;
+        }
+        if (overflow) return cleanup(fail(HF_ERR_UNSUPPORTED, "too many cell-stage rows"));
+        UP((int32_t **)&P.cslots, cs.data(), cs.size());
         UP((uint32_t **)&P.cflags, pg->cell_flags, pg->ncell);
+        if ((rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, false, P.cr, C->cell_entries, "cell-stage")))
+            return cleanup(rc);
+        UP((double **)&P.cr.rhs, prhs.data(), prhs.size());
+        // wait for the uploads before the host staging vectors go away
+        if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "cell slots"));
     }
     // fields
     DevFields &F = C->F;

@@ -137,6 +137,11 @@ class BatchServer:
                 raise TimeoutError(rid)
             return r.status, r.t_admit - r.t_submit, r.t_done - r.t_submit
 
+    def error(self, rid: int) -> str:
+        """The engine's message for a failed request ('' when it succeeded)."""
+        with self.cv:
+            return self.reqs[rid].error
+
     def get(self, rid: int, fid: int, comp: int = 0) -> np.ndarray:
         with self.cv:
             r = self.reqs[rid]

@@ -24,7 +24,7 @@ first step (HigTree's first, uncached answer to an interpolation query differs
 in the last bits from the cached one that every later step reads), so its
 first step already uses the stencils the recorded program holds.
 
-    python tests/golden/make_configs.py            # c1_64_200, c4_sub_20, c2_8
+    python tests/golden/make_configs.py            # c1_64_200, c4_sub_20, c2_8, c4_61_2000
 """
 from __future__ import annotations
 
@@ -181,11 +181,60 @@ def make_c2():
     np.savez_compressed(os.path.join(HERE, f"c2_{C2_PER_UNIT}.npz"), **save)
 
 
+# one instance of the batched population over the configuration's full 2000
+# steps: instance 61 (N = 129, Wi 1.46, alpha 0.084), the subset's instance
+# whose K is the most ill-conditioned after 20 steps
+C4_LONG_INDEX = 61
+C4_LONG_MARKS = (200, 2000)
+
+
+def _snapshots_cmd(spec_expr, marks, rtol):
+    code = ("import json, os, sys\n"
+            f"os.environ['HF_ORACLE_RTOL'] = '{rtol!r}'\n"
+            f"sys.path.insert(0, {REPO!r})\n"
+            "sys.path.insert(0, os.path.join(" + repr(REPO) + ", 'tests', 'golden'))\n"
+            "import make_configs as m\n"
+            "from higflow_b200 import workloads\n"
+            f"snap = m.run_snapshots({spec_expr}, {marks!r})\n"
+            "json.dump({str(k): {f: v.tolist() for f, v in o.items()} for k, o in snap.items()}, sys.stdout)\n")
+    return [sys.executable, "-c", code]
+
+
+def make_c4_long():
+    """Reference fields of instance C4_LONG_INDEX after each of C4_LONG_MARKS
+    steps, with the reference's own sensitivity to its Poisson tolerance
+    (1e-13 and 1e-6 against 1e-15): three reference runs side by side."""
+    import json
+    import subprocess
+    spec_expr = f"workloads.spec(workloads.batched_giesekus()[{C4_LONG_INDEX}])"
+    procs = {rt: subprocess.Popen(_snapshots_cmd(spec_expr, C4_LONG_MARKS, rt), stdout=subprocess.PIPE, text=True)
+             for rt in (1e-15, 1e-13, 1e-6)}
+    snaps = {}
+    for rt, pr in procs.items():
+        out, _ = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"reference run at rtol {rt} failed")
+        snaps[rt] = {int(k): {f: np.array(v) for f, v in o.items()} for k, o in json.loads(out).items()}
+    save = {"index": np.int64(C4_LONG_INDEX), "marks": np.array(C4_LONG_MARKS, dtype=np.int64)}
+    for m in C4_LONG_MARKS:
+        for k, v in snaps[1e-15][m].items():
+            save[f"ref{m}_{k}"] = v
+            for tag, rt in (("sens", 1e-13), ("sens6_", 1e-6)):
+                w = snaps[rt][m][k]
+                save[f"{tag}{m}_{k}"] = np.float64(np.linalg.norm(w - v) / max(np.linalg.norm(v), 1e-300))
+        print(f"c4 instance {C4_LONG_INDEX} after {m} steps: reference sensitivity "
+              + " ".join(f"{k}={float(save[f'sens{m}_{k}']):.1e}/{float(save[f'sens6_{m}_{k}']):.1e}"
+                         for k in snaps[1e-15][m]))
+    np.savez_compressed(os.path.join(HERE, f"c4_{C4_LONG_INDEX}_{C4_LONG_MARKS[-1]}.npz"), **save)
+
+
 if __name__ == "__main__":
-    todo = sys.argv[1:] or ["c1", "c4_sub", "c2"]
+    todo = sys.argv[1:] or ["c1", "c4_sub", "c2", "c4_long"]
     if "c1" in todo:
         make_c1()
     if "c4_sub" in todo:
         make_c4_sub()
     if "c2" in todo:
         make_c2()
+    if "c4_long" in todo:
+        make_c4_long()
