@@ -517,9 +517,18 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     const double *ud = pick<3>(F.u, d);
     const double ufacet = __ldg(ud + f);
     double Fs = SLQ(HF_V_FU, pick<3>(F.FU, d));
+    // the mixed form divides by each direction's spacing once and multiplies
+    // (a quotient within one rounding of the plain form's)
+    double ifd[D], ifd2[D];
+#pragma unroll
+    for (int d2 = 0; d2 < D; d2++) {
+        ifd[d2] = MIX ? 1.0 / fd[d2] : 0.0;
+        ifd2[d2] = MIX ? 1.0 / (fd[d2] * fd[d2]) : 0.0;
+    }
+#define HF_QUOT(a, b, inv) (MIX ? (a) * (inv) : (a) / (b))
     const double pl = SLQ(HF_V_PL, F.p);
     const double pr = SLQ(HF_V_PR, F.p);
-    const double dpdx = (pr - pl) / (2.0 * 0.5 * fd[d]);
+    const double dpdx = HF_QUOT(pr - pl, 2.0 * 0.5 * fd[d], ifd[d]);
     const double Fl = SLQ(HF_V_FL, F.F);
     const double Fr = SLQ(HF_V_FR, F.F);
     Fs += (Fr + Fl) / 2.0;
@@ -545,17 +554,17 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
         const double ur = SLQ(B + HF_V_UR, ud);
         const int infr = (fl >> (4 * d2 + 1)) & 1;
         if (infr == 0 && convec == HF_SECOND_ORDER) convec = HF_FIRST_ORDER;
-        dudxc[d2] = (ur - ul) / (2.0 * 1.0 * fd[d2]);
-        dudxr[d2] = (ur - ufacet) / (1.0 * fd[d2]);
-        dudxl[d2] = (ufacet - ul) / (1.0 * fd[d2]);
+        dudxc[d2] = HF_QUOT(ur - ul, 2.0 * 1.0 * fd[d2], 0.5 * ifd[d2]);
+        dudxr[d2] = HF_QUOT(ur - ufacet, 1.0 * fd[d2], ifd[d2]);
+        dudxl[d2] = HF_QUOT(ufacet - ul, 1.0 * fd[d2], ifd[d2]);
         const double urr = SLQ(B + HF_V_URR, ud);
         const int infrr = (fl >> (4 * d2 + 3)) & 1;
         const double ull = SLQ(B + HF_V_ULL, ud);
         const int infll = (fl >> (4 * d2 + 2)) & 1;
         if (convec == HF_SECOND_ORDER) {
             if (second == HF_QUICK) {
-                dudxrr[d2] = (urr - ur) / (1.0 * fd[d2]);
-                dudxll[d2] = (ul - ull) / (1.0 * fd[d2]);
+                dudxrr[d2] = HF_QUOT(urr - ur, 1.0 * fd[d2], ifd[d2]);
+                dudxll[d2] = HF_QUOT(ul - ull, 1.0 * fd[d2], ifd[d2]);
             } else if (second == HF_CUBISTA) {
                 const double vcr = SLQ(B + HF_V_VCR, F.u[d2]);
                 const double vcl = SLQ(B + HF_V_VCL, F.u[d2]);
@@ -563,10 +572,10 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
                     ufacet, ul, ur, ull, urr, infll, infrr, vcr, vcl, conv1, conv2);
                 conv1 = cv.x;
                 conv2 = cv.y;
-                vc[d2] = ((conv1 - conv2) / fd[d]);
+                vc[d2] = HF_QUOT(conv1 - conv2, fd[d], ifd[d]);
             }
         }
-        du2dx2[d2] = (ul - 2.0 * ufacet + ur) / (fd[d2] * fd[d2] * 1.0 * 1.0);
+        du2dx2[d2] = HF_QUOT(ul - 2.0 * ufacet + ur, fd[d2] * fd[d2] * 1.0 * 1.0, ifd2[d2]);
     }
     double tens = 0.0;
     if (VE) {
@@ -578,7 +587,7 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
             if (d2 == d) {
                 const double Sl = SLQ(B + 0, Sf);
                 const double Sr = SLQ(B + 2, Sf);
-                dSdx[d2] = (Sr - Sl) / (2.0 * 0.5 * fd[d2]);
+                dSdx[d2] = HF_QUOT(Sr - Sl, 2.0 * 0.5 * fd[d2], ifd[d2]);
             } else {
                 const double l1 = SLQ(B + 0, Sf);
                 const double l2 = SLQ(B + 1, Sf);
@@ -586,13 +595,14 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
                 const double r1 = SLQ(B + 2, Sf);
                 const double r2 = SLQ(B + 3, Sf);
                 const double Sr = 0.5 * (r1 + r2);
-                dSdx[d2] = (Sr - Sl) / (2.0 * 1.0 * fd[d2]);
+                dSdx[d2] = HF_QUOT(Sr - Sl, 2.0 * 1.0 * fd[d2], 0.5 * ifd[d2]);
             }
         }
 #pragma unroll
         for (int d2 = 0; d2 < D; d2++) tens += dSdx[d2];
     }
 #undef SLQ
+#undef HF_QUOT
     const double pterm = par.projtype == HF_INCREMENTAL ? dpdx : 0.0;
     double conv = 0.0;
     if (convec == HF_CENTRAL) {

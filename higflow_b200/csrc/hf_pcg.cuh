@@ -176,13 +176,12 @@ struct VLev {
 // The small levels of one instance, from the first level with at most
 // kTailRows rows (s) down to its coarsest (clev, dense inverse), run by one
 // CTA: phases separated by __syncthreads instead of kernel launches.
-// 2048 rows over 512 threads: a tail phase is at most four rows per thread,
-// and every level that small leaves the level-synchronous kernels (on the
-// batched cavities of 32^2 to 256^2 cells that takes the third level out of
-// them: four launches fewer per CG iteration); 512 threads keep two tail
-// CTAs per SM, so 296 instances run in one wave.  Larger levels run
-// level-synchronously
-constexpr int kTailRows = 2048;
+// 256 rows: a tail phase is then at most one row per thread, so the tail's
+// dependent load chains stay short; larger levels run level-synchronously
+// (measured on the batched cavities: taking levels of up to 2048 rows into
+// the tail saves four launches per CG iteration but doubles the tail's time,
+// 2.74 against 2.68 ms of Poisson iterations per step)
+constexpr int kTailRows = 256;
 constexpr int kTailThreads = 512;
 
 template <typename T>
