@@ -52,6 +52,11 @@ WORKLOADS = {
              "the kernel profiles are taken on",
         batch="c4", count=16, precision="mixed", dim=2,
     ),
+    "c4_16_plain": dict(
+        name="the first 16 cavities of the batched Giesekus population (seed 0), otherwise as c4, plain FP64; the "
+             "small case the plain form's kernel profiles are taken on",
+        batch="c4", count=16, precision="fp64", dim=2,
+    ),
     "c1": dict(
         name="2D Newtonian lid-driven cavity 64x64 (uniform quadtree, unit square), Re=100, lid u=1, "
              "explicit Euler dt=1e-4, CUBISTA, incremental projection, Poisson CG to 1e-10 relative residual, "

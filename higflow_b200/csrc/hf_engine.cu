@@ -80,7 +80,7 @@ constexpr int kBlock = 256;
 // added) in scol, or, when every pair's entries lie within +-32767 of its
 // first column pcol0[u] (interpolation stencils are local: 2D meshes up to
 // several thousand cells a side), 16-bit offsets in scol16 (scol null).
-// Weights are FP64 (sw) or FP32 (sw32, the mixed form's velocity rows).
+// Weights are FP64 (sw).
 struct PairRows {
     int n;
     const uint8_t *tag;
@@ -91,7 +91,6 @@ struct PairRows {
     const int16_t *scol16;
     const int32_t *pcol0;
     const double *sw;
-    const float *sw32;
     double *val;
 };
 
@@ -344,17 +343,10 @@ __device__ __forceinline__ const double *vtag_field(const DevFields &F, int tag)
 // stencils (tens of entries) run here, coalesced and without divergence,
 // instead of inside the per-facet and per-cell kernels.  Entry k of the 32
 // pairs of a warp is one 128-byte (or 64-byte, 16-bit) column load and one
-// 256-byte (FP64) or 128-byte (FP32) weight load; the sum is
-// dp_interpolate_from_stencil's (pdomain.c:1026-1053): -rhs, then the entries
-// in stencil order, in FP64.  W = float reads FP32 weights (the mixed form's
-// velocity rows: half the weight stream) and still sums FP64 field values in
-// FP64: rounding the values or the sum to FP32 puts noise of about 1e-7 of the
-// velocity into every step's Poisson right-hand side that the extrapolated
-// initial guess cannot follow (measured on the batched Giesekus cavities at
-// Poisson rtol 1e-6: 7.2 CG iterations per instance-step against 4.4 with
-// FP64 sums, 4.0 for the plain form).
+// 256-byte weight load; the sum is dp_interpolate_from_stencil's
+// (pdomain.c:1026-1053): -rhs, then the entries in stencil order, in FP64.
 // (launch bounds of the largest block size the tuner tries)
-template <typename W, bool C16>
+template <bool C16>
 __global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -363,7 +355,6 @@ __global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
     if (C16) fb += __ldg(R.pcol0 + u);
     const int n = __ldg(R.plen + u);
     const int64_t e0 = __ldg(R.sptr + (u >> 5)) + (u & 31);
-    const W *__restrict__ w = std::is_same<W, float>::value ? (const W *)R.sw32 : (const W *)R.sw;
     double res = 0.0;
     res += -__ldg(R.rhs + u);
     // the entries stream through once (evict-first loads keep L1 for the
@@ -372,13 +363,18 @@ __global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
     for (int k = 0; k < n; k++) {
         const int64_t at = e0 + 32 * (int64_t)k;
         const int c = C16 ? (int)__ldcs(R.scol16 + at) : __ldcs(R.scol + at);
-        res += __ldg(fb + c) * (double)__ldcs(w + at);
+        res += __ldg(fb + c) * __ldcs(R.sw + at);
     }
     R.val[u] = res;
 }
 
 // PatRows: one thread per pair; -rhs, then the pattern's entries in column
-// order, FP64 values times FP32 weights summed in FP64.
+// order, FP64 values times FP32 weights summed in FP64.  Rounding the values
+// or the sum to FP32 as well puts noise of about 1e-7 of the velocity into
+// every step's Poisson right-hand side that the extrapolated initial guess
+// cannot follow (measured on the batched Giesekus cavities at Poisson rtol
+// 1e-6: 7.2 CG iterations per instance-step against 4.4 with FP64 sums, 4.0
+// for the plain form).
 __global__ void __launch_bounds__(512) k_vrows_pat(PatRows R, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2370,14 +2366,8 @@ void record(hf_case *C, int phase, int end)
 void enqueue_pairs(hf_case *C, const PairRows &R, const DevFields &F, cudaStream_t st)
 {
     const int bs = C->blk_vrows, nb = (R.n + bs - 1) / bs;
-    const bool c16 = R.scol16 != nullptr;
-    if (R.sw32) {
-        if (c16) k_vrows<float, true><<<nb, bs, 0, st>>>(R, F);
-        else k_vrows<float, false><<<nb, bs, 0, st>>>(R, F);
-    } else {
-        if (c16) k_vrows<double, true><<<nb, bs, 0, st>>>(R, F);
-        else k_vrows<double, false><<<nb, bs, 0, st>>>(R, F);
-    }
+    if (R.scol16) k_vrows<true><<<nb, bs, 0, st>>>(R, F);
+    else k_vrows<false><<<nb, bs, 0, st>>>(R, F);
 }
 
 // the velocity stage's general rows: by pattern (mixed form) or sliced
@@ -2906,10 +2896,10 @@ extern "C" int hf_case_device_bytes(const hf_program *pg, const hf_options *opt,
 // stream into device memory the case owns: fills R except rhs; entries = the
 // stored (padded) entry count.  A slice holds 32 consecutive pairs padded to
 // its longest; consecutive pairs are consecutive elements of one slot, so
-// lengths within a slice rarely differ.  fp32: FP32 weights.
+// lengths within a slice rarely differ.
 int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_program *pg,
                 const std::vector<int32_t> &ptmpl, const std::vector<int32_t> &pbase,
-                const std::vector<double> &prhs, const std::vector<uint8_t> &ptag, bool fp32, PairRows &R,
+                const std::vector<double> &prhs, const std::vector<uint8_t> &ptag, PairRows &R,
                 int64_t &entries, const char *what)
 {
     (void)prhs;
@@ -2943,10 +2933,7 @@ int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_progra
     }
     std::vector<int32_t> scol(c16 ? 0 : ne, 0);
     std::vector<int16_t> scol16(c16 ? ne : 0, 0);
-    std::vector<double> sw;
-    std::vector<float> sw32;
-    if (fp32) sw32.assign(ne, 0.f);
-    else sw.assign(ne, 0.0);
+    std::vector<double> sw(ne, 0.0);
     for (size_t u = 0; u < np; u++) {
         const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
         int64_t at = sptr[u / 32] + (int64_t)(u % 32);
@@ -2955,15 +2942,13 @@ int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_progra
             if (c < 0 || c > INT32_MAX) return fail(HF_ERR_INVALID, std::string(what) + " column out of range");
             if (c16) scol16[at] = (int16_t)(c - pcol0[u]);
             else scol[at] = (int32_t)c;
-            if (fp32) sw32[at] = (float)pg->tmpl_w[a0 + k];
-            else sw[at] = pg->tmpl_w[a0 + k];
+            sw[at] = pg->tmpl_w[a0 + k];
         }
     }
     R.scol = nullptr;
     R.scol16 = nullptr;
     R.pcol0 = nullptr;
     R.sw = nullptr;
-    R.sw32 = nullptr;
     if ((rc = upload(own, (int64_t **)&R.sptr, sptr.data(), sptr.size(), B, C->stream))) return rc;
     if ((rc = upload(own, (uint8_t **)&R.plen, plen.data(), plen.size(), B, C->stream))) return rc;
     if (c16) {
@@ -2972,11 +2957,7 @@ int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_progra
     } else {
         if ((rc = upload(own, (int32_t **)&R.scol, scol.data(), scol.size(), B, C->stream))) return rc;
     }
-    if (fp32) {
-        if ((rc = upload(own, (float **)&R.sw32, sw32.data(), sw32.size(), B, C->stream))) return rc;
-    } else {
-        if ((rc = upload(own, (double **)&R.sw, sw.data(), sw.size(), B, C->stream))) return rc;
-    }
+    if ((rc = upload(own, (double **)&R.sw, sw.data(), sw.size(), B, C->stream))) return rc;
     if ((rc = upload(own, (uint8_t **)&R.tag, ptag.data(), ptag.size(), B, C->stream))) return rc;
     if ((rc = upload(own, &R.val, (const double *)nullptr, np, B, C->stream))) return rc;
     entries = (int64_t)ne;
@@ -3245,7 +3226,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         }
         C->vmix = opt.precision == HF_PREC_MIXED;
         if (C->vmix) rc = build_patterns(C, own, B, pg, ptmpl, pbase, prhs, ptag, P.vr, C->vp, C->vel_entries);
-        else rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, false, P.vr, C->vel_entries, "velocity-stage");
+        else rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, P.vr, C->vel_entries, "velocity-stage");
         if (rc) return cleanup(rc);
         P.vrow.tptr = P.rows.tptr;
         P.vrow.col = P.rows.col;
@@ -3302,7 +3283,7 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         if (overflow) return cleanup(fail(HF_ERR_UNSUPPORTED, "too many cell-stage rows"));
         UP((int32_t **)&P.cslots, cs.data(), cs.size());
         UP((uint32_t **)&P.cflags, pg->cell_flags, pg->ncell);
-        if ((rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, false, P.cr, C->cell_entries, "cell-stage")))
+        if ((rc = build_pairs(C, own, B, pg, ptmpl, pbase, prhs, ptag, P.cr, C->cell_entries, "cell-stage")))
             return cleanup(rc);
         UP((double **)&P.cr.rhs, prhs.data(), prhs.size());
         // wait for the uploads before the host staging vectors go away
