@@ -2510,7 +2510,9 @@ void enqueue_pre(hf_case *C, DevFields &F, int &fixed)
             enqueue_pairs(C, C->P.cr, F, st);
             fixed++;
         }
+        record(C, HF_PHASE_VE_CELL_MAIN, 0);
         enqueue_ve_cell<D>(C, F, st);
+        record(C, HF_PHASE_VE_CELL_MAIN, 1);
         k_ve_stress<D><<<blocks(C->P.ncell), kBlock, 0, st>>>(C->P, F);
         record(C, HF_PHASE_VE_CELL, 1);
         for (int k = 0; k < D * D; k++) std::swap(F.K[k], F.Knew[k]);
@@ -2714,7 +2716,7 @@ int collect_phases(hf_case *C)
     if (rc) return rc;
     const bool ve = C->par.flowtype == HF_VISCOELASTIC;
     for (int p = 0; p < HF_NPHASE; p++) {
-        if (p == HF_PHASE_VE_CELL && !ve) continue;
+        if ((p == HF_PHASE_VE_CELL || p == HF_PHASE_VE_CELL_MAIN) && !ve) continue;
         if (p == HF_PHASE_VELOCITY_ROWS && !C->P.vr.n) continue;
         float ms = 0.f;
         HF_CK(cudaEventElapsedTime(&ms, C->ev[2 * p], C->ev[2 * p + 1]));
@@ -2722,6 +2724,7 @@ int collect_phases(hf_case *C)
     }
     const bool rk = C->par.tempdiscrtype == HF_EXPLICIT_RK2 || C->par.tempdiscrtype == HF_EXPLICIT_RK3;
     if (ve) C->phase_launches[HF_PHASE_VE_CELL] += 2 + (C->gptt ? 1 : 0) + (C->P.cr.n ? 1 : 0);
+    if (ve) C->phase_launches[HF_PHASE_VE_CELL_MAIN] += 1;
     C->phase_launches[HF_PHASE_VELOCITY] += 1 + (C->P.vr.n ? 1 : 0) + (rk ? 1 : 0);
     if (C->P.vr.n) C->phase_launches[HF_PHASE_VELOCITY_ROWS] += 1;
     C->phase_launches[HF_PHASE_POISSON_INIT] += 2;

@@ -209,7 +209,7 @@ class Case:
         method = {hp.PRECOND_AMG: "amg-cg", hp.PRECOND_JACOBI: "jacobi-cg", -1: "bicgstab"}[m.value]
         return {"method": method, "levels": [(rows[i], na[i], npp[i], nr[i]) for i in range(nl.value)]}
 
-    PHASES = ("ve_cell", "velocity", "poisson_init", "poisson_iter", "final", "velocity_rows")
+    PHASES = ("ve_cell", "velocity", "poisson_init", "poisson_iter", "final", "velocity_rows", "ve_cell_main")
 
     def phase_times(self):
         """{phase: (device ms, kernel launches)} accumulated since profile()."""

@@ -398,7 +398,9 @@ enum {
     HF_PHASE_FINAL = 4,         /* final velocity and pressure             */
     HF_PHASE_VELOCITY_ROWS = 5, /* within HF_PHASE_VELOCITY: its stencil   */
                                 /* rows (k_vrows) alone; CG path only      */
-    HF_NPHASE = 6
+    HF_PHASE_VE_CELL_MAIN = 6,  /* within HF_PHASE_VE_CELL: its main       */
+                                /* kernel (k_ve_cell) alone; CG path only  */
+    HF_NPHASE = 7
 };
 int  hf_case_profile(hf_case *c, int32_t enable);
 int  hf_case_phase_times(hf_case *c, double *ms, int64_t *launches, int32_t n);
