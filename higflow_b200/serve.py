@@ -172,17 +172,18 @@ class BatchServer:
         return keys
 
     def _form(self) -> Optional[List[_Request]]:
-        """The next cohort from the queue head's group (lock held).  While
-        other cohorts run, waiting requests gather for ``window_s`` (or until
+        """The next cohort from the queue head's group (lock held).  Waiting
+        requests gather for ``window_s`` after the head's arrival (or until
         they reach a quarter of ``max_cells``) so that a cohort is a batch
-        rather than a single request; an idle device takes them at once."""
+        rather than a single request: a cohort runs until its longest request
+        is done, and a cohort of one long request would hold a stream at the
+        step's latency floor for all of its steps."""
         if not self.queue or len(self.cohorts) >= self.max_cohorts:
             return None
-        if self.cohorts:
-            waited = time.perf_counter() - self.queue[0].t_submit
-            cells = sum(r.prog.ncell for r in self.queue)
-            if waited < self.window_s and cells < self.max_cells // 4:
-                return None
+        waited = time.perf_counter() - self.queue[0].t_submit
+        cells = sum(r.prog.ncell for r in self.queue)
+        if waited < self.window_s and cells < self.max_cells // 4 and not self.stop:
+            return None
         held = sum(c.nbytes for c in self.cohorts)
         key = batch_key(self.queue[0].prog)
         pick, cells, est = [], 0, 0
