@@ -492,14 +492,16 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     constexpr int NS = VE ? HF_V_NSLOT_VE(D) : HF_V_NSLOT_NEWT(D);
     int32_t code[NS];
     double val[NS];
+    // (the u[d] corner slots of the facet's own direction are not read)
+    auto unused = [&](int s) {
+        return s >= HF_V_BLK0 && s < HF_V_NSLOT_NEWT(D) && (s - HF_V_BLK0) % HF_V_NB < 4 && (s - HF_V_BLK0) / HF_V_NB == d;
+    };
 #pragma unroll
-    for (int s = 0; s < NS; s++) code[s] = __ldg(sl + (size_t)s * nf + f);
+    for (int s = 0; s < NS; s++) code[s] = unused(s) ? 0 : __ldg(sl + (size_t)s * nf + f);
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        const bool unused = s >= HF_V_BLK0 && s < HF_V_NSLOT_NEWT(D) && (s - HF_V_BLK0) % HF_V_NB < 4 &&
-                            (s - HF_V_BLK0) / HF_V_NB == d;   // u[d] corners of the facet's own direction
         const double *src = code[s] >= 0 ? vslot_field<D>(F, d, s) + code[s] : P.vr.val + (-code[s] - 1);
-        val[s] = unused ? 0.0 : __ldg(src);
+        val[s] = unused(s) ? 0.0 : __ldg(src);
     }
 #define SLQ(s, fld) (val[s])
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
