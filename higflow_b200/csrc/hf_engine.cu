@@ -2220,6 +2220,24 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
 // ---------------------------------------------------------------------------
 // one time step as a CUDA graph
 // ---------------------------------------------------------------------------
+// A kernel of the CG loop body, launched with programmatic stream
+// serialization (the kernel starts with pdl_wait, hf_pcg.cuh)
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <typename T, typename R>
 void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T> *H, const TailInst<T> *ti,
                     const R *r0, int &kernels)
@@ -2228,24 +2246,24 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T>
     // the large levels, every instance at once, down to each instance's tail
     for (int l = 0; l < C->nreg; l++) {
         if (L[l].nsblk) {
-            if (l == 0) k_vc_down<T, true, R><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
-            else k_vc_down<T, false, R><<<L[l].nsblk, kBlock, 0, st>>>(L[l], r0, S);
+            if (l == 0) launch_pdl(k_vc_down<T, true, R>, L[l].nsblk, kBlock, st, L[l], r0, S);
+            else launch_pdl(k_vc_down<T, false, R>, L[l].nsblk, kBlock, st, L[l], r0, S);
             kernels++;
         }
         if (L[l + 1].nablk) {
-            k_vc_restrict<T><<<L[l + 1].nablk, kBlock, 0, st>>>(L[l], L[l + 1], S);
+            launch_pdl(k_vc_restrict<T>, L[l + 1].nablk, kBlock, st, L[l], L[l + 1], S);
             kernels++;
         }
     }
     // the small levels: one CTA per instance
-    k_vc_tail<T, R><<<C->ninst, kTailThreads, 0, st>>>(H, ti, r0, S);
+    launch_pdl(k_vc_tail<T, R>, C->ninst, kTailThreads, st, H, ti, r0, S);
     kernels++;
     for (int l = C->nreg - 1; l >= 0; l--) {
         if (!L[l].nsblk) continue;
-        k_vc_prolong<T><<<L[l].nsblk, kBlock, 0, st>>>(L[l], L[l + 1].out, S);
+        launch_pdl(k_vc_prolong<T>, L[l].nsblk, kBlock, st, L[l], (const T *)L[l + 1].out, S);
         kernels++;
         if (l > 0) {
-            k_vc_post<T><<<L[l].nsblk, kBlock, 0, st>>>(L[l], S);
+            launch_pdl(k_vc_post<T>, L[l].nsblk, kBlock, st, L[l], S);
             kernels++;
         }
     }
@@ -2261,23 +2279,23 @@ void enqueue_body(hf_case *C, cudaStream_t st, cudaGraphConditionalHandle cond, 
         if (C->mixed) {
             // the inner FP32 iteration of the mixed form
             enqueue_vcycle<float, float>(C, st, C->L32, C->h32, C->t32, C->G.r32, kernels);
-            k_pcg_z32<<<C->G.nblk, kBlock, 0, st>>>(C->G, C->L32[0]);
+            launch_pdl(k_pcg_z32, C->G.nblk, kBlock, st, C->G, C->L32[0]);
             float *po = it == 0 ? C->pa32 : C->pb32, *pn = it == 0 ? C->pb32 : C->pa32;
-            k_pcg_dir32<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
-            k_pcg_update32<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, set);
+            launch_pdl(k_pcg_dir32, C->G.nblk, kBlock, st, C->G, (const float *)po, pn);
+            launch_pdl(k_pcg_update32, C->G.nblk, kBlock, st, C->G, (const float *)pn, cond, set);
             kernels += 3;
             continue;
         }
         if (!C->amg) {
-            k_pcg_z<double, true><<<C->G.nblk, kBlock, 0, st>>>(C->G, VLev<double>{});
+            launch_pdl(k_pcg_z<double, true>, C->G.nblk, kBlock, st, C->G, VLev<double>{});
         } else {
             enqueue_vcycle<double, double>(C, st, C->L64, C->h64, C->t64, C->G.r, kernels);
-            k_pcg_z<double, false><<<C->G.nblk, kBlock, 0, st>>>(C->G, C->L64[0]);
+            launch_pdl(k_pcg_z<double, false>, C->G.nblk, kBlock, st, C->G, C->L64[0]);
         }
         kernels++;
         double *po = it == 0 ? C->pa : C->pb, *pn = it == 0 ? C->pb : C->pa;
-        k_pcg_dir<<<C->G.nblk, kBlock, 0, st>>>(C->G, po, pn);
-        k_pcg_update<<<C->G.nblk, kBlock, 0, st>>>(C->G, pn, cond, set);
+        launch_pdl(k_pcg_dir, C->G.nblk, kBlock, st, C->G, (const double *)po, pn);
+        launch_pdl(k_pcg_update, C->G.nblk, kBlock, st, C->G, (const double *)pn, cond, set);
         kernels += 2;
     }
 }

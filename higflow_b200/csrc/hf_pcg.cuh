@@ -49,6 +49,13 @@ constexpr int kCoarseCap = 1024;     // largest coarsest level accepted (stalled
 constexpr int kRPT = 4;
 constexpr int kBlockRows = kBlock * kRPT;
 
+// Programmatic dependent launch: the kernels of the CG loop body are launched
+// with programmatic stream serialization, so a kernel's grid is scheduled
+// while its predecessor's last blocks finish.  Each waits here, before its
+// first access to device memory, until the predecessor grid has completed
+// and its writes are visible (a no-op for a plain launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // rows [row0, row0 + cnt) of instance inst at one level (cnt <= kBlockRows);
 // first/nblk: the instance's block range in the same table (for reductions).
 // On the finest level pad0 <= 0 <= pad1 are the lowest and highest column
@@ -472,6 +479,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
 template <typename T, bool FINE, typename R = double>
 __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const R *__restrict__ r0, const IScal *S)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
     // (the finest level's descriptors up front: faster there, slower on the
@@ -504,6 +512,7 @@ __global__ void __launch_bounds__(kBlock) k_vc_down(VLev<T> L, const R *__restri
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, const IScal *S)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(Ln.ablk, S, B)) return;
 #pragma unroll
@@ -530,6 +539,7 @@ template <typename T, typename R = double>
 __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, const TailInst<T> *TI,
                                                         const R *__restrict__ r0, const IScal *S)
 {
+    pdl_wait();
     __shared__ TailInst<T> ti;
     __shared__ VLev<T> L, Ln;
     __shared__ int done;
@@ -625,6 +635,7 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_prolong(VLev<T> L, const T *__restrict__ e, const IScal *S)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
     const pcg::RowSet R = pcg::rowset(B);
@@ -640,6 +651,7 @@ __global__ void __launch_bounds__(kBlock) k_vc_prolong(VLev<T> L, const T *__res
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_vc_post(VLev<T> L, const IScal *S)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(L.sblk, S, B)) return;
 #pragma unroll
@@ -660,6 +672,7 @@ __global__ void __launch_bounds__(kBlock) k_vc_post(VLev<T> L, const IScal *S)
 template <typename T, bool JACOBI>
 __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
     const bool tail0 = G.S[B.inst].tail0;
@@ -695,6 +708,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
 // p_new = z + beta p_old ; q = A p_new ; alpha = r.z / p.q
 __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__restrict__ po, double *__restrict__ pn)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
     const IScal &sc = G.S[B.inst];
@@ -751,6 +765,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__r
 __global__ void __launch_bounds__(kBlock) k_pcg_update(PcgFine G, const double *__restrict__ pn,
                                                        cudaGraphConditionalHandle cond, int set_cond)
 {
+    pdl_wait();
     Blk B;
     const bool skip = pcg::load_blk(G.blk, G.S, B);
     if (!skip) {
@@ -891,6 +906,7 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
 // z32 from the V-cycle (finest post-smoothing or the tail's output), r.z
 __global__ void __launch_bounds__(kBlock) k_pcg_z32(PcgFine G, VLev<float> L0)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
     const bool tail0 = G.S[B.inst].tail0;
@@ -919,6 +935,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z32(PcgFine G, VLev<float> L0)
 // p = z + beta p_old ; q = A32 p ; alpha = r.z / p.q  (FP32 vectors)
 __global__ void __launch_bounds__(kBlock) k_pcg_dir32(PcgFine G, const float *__restrict__ po, float *__restrict__ pn)
 {
+    pdl_wait();
     Blk B;
     if (pcg::load_blk(G.blk, G.S, B)) return;
     const IScal &sc = G.S[B.inst];
@@ -976,6 +993,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_dir32(PcgFine G, const float *__
 __global__ void __launch_bounds__(kBlock) k_pcg_update32(PcgFine G, const float *__restrict__ pn,
                                                          cudaGraphConditionalHandle cond, int set_cond)
 {
+    pdl_wait();
     Blk B;
     const bool skip = pcg::load_blk(G.blk, G.S, B);
     if (!skip) {
