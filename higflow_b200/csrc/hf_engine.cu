@@ -1392,6 +1392,7 @@ struct hf_case {
     std::vector<int> foff[3];       // ninst + 1 per direction
     // batched AMG-PCG (hf_pcg.cuh) and the graphs that run one step each
     bool amg = false;
+    bool bi_amg = false;            // BiCGStab path preconditioned by the AMG V-cycle
     bool mixed = false;
     PcgFine G{};
     double *pa = nullptr, *pb = nullptr;   // CG directions (alternating)
@@ -2790,6 +2791,17 @@ int graph_steps(hf_case *C, int nsteps, bool sync)
     return take_error(C);
 }
 
+// w = M^-1 v with the instance's AMG V-cycle (the BiCGStab path with AMG:
+// right preconditioning, k_bi_p / k_bi_s's Jacobi values overwritten);
+// returns the kernels launched
+int bi_precondition(hf_case *C, const double *v, double *w, cudaStream_t st)
+{
+    int kernels = 0;
+    enqueue_vcycle<double, double>(C, st, C->L64, C->h64, C->t64, v, kernels);
+    launch_pdl(k_bi_amg_post, C->G.nblk, kBlock, st, C->G, C->L64[0], v, w);
+    return kernels;   // (enqueue_vcycle counts one more than it launches: the post kernel)
+}
+
 // BiCGStab (non-symmetric Poisson rows): one instance, host-driven loop
 template <int D>
 int bicg_step(hf_case *C)
@@ -2844,8 +2856,10 @@ int bicg_step(hf_case *C)
             PhaseTimer t(C, HF_PHASE_POISSON_ITER, launches);
             for (int k = 0; k < chunk; k++) {
                 k_bi_p<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
+                if (C->bi_amg) launches += bi_precondition(C, C->bi.p, C->bi.ph, st);
                 k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.ph, C->bi.v, 0);
                 k_bi_s<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
+                if (C->bi_amg) launches += bi_precondition(C, C->bi.s, C->bi.sh, st);
                 k_bi_spmv<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi, C->bi.sh, C->bi.t, 1);
                 k_bi_update<<<blocks(n), kBlock, 0, st>>>(C->M, C->bi);
                 launches += 5;
@@ -3447,8 +3461,9 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
     if (ni > 1 && !C->use_cg) return cleanup(fail(HF_ERR_UNSUPPORTED, "batches need symmetric Poisson rows (CG)"));
     if (opt.precision == HF_PREC_MIXED && !C->use_cg)
         return cleanup(fail(HF_ERR_UNSUPPORTED, "the mixed form needs the CG solver"));
-    C->amg = C->use_cg && opt.precond != HF_PRECOND_JACOBI;
-    C->mixed = C->amg && opt.precision == HF_PREC_MIXED;
+    C->amg = opt.precond != HF_PRECOND_JACOBI;   // BiCGStab too: the V-cycle preconditions it
+    C->bi_amg = !C->use_cg && C->amg;
+    C->mixed = C->use_cg && C->amg && opt.precision == HF_PREC_MIXED;
     DevMat &M = C->M;
     M.n = pg->ncell;
     if (!C->use_cg) {   // BiCGStab reads CSR; the CG path keeps the row templates
@@ -3487,6 +3502,14 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         UP(&V.sh, (const double *)nullptr, n);
         V.partials = partials;
         V.sc = sc;
+        if (C->bi_amg) {
+            // the instance's hierarchy for the preconditioner; its CG state
+            // stays idle (the instance is marked not done, so that the
+            // V-cycle kernels run on it)
+            if ((rc = build_pcg(C, mptr, mcol, mval, pins))) return cleanup(rc);
+            if (cudaMemsetAsync(&C->G.S[0].done, 0, sizeof(int32_t), C->stream) != cudaSuccess)
+                return cleanup(fail(HF_ERR_CUDA, "preconditioner state"));
+        }
     }
 #undef UP
     if (cudaStreamSynchronize(C->stream) != cudaSuccess) return cleanup(fail(HF_ERR_CUDA, "create sync"));

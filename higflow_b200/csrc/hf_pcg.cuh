@@ -705,6 +705,27 @@ __global__ void __launch_bounds__(kBlock) k_pcg_z(PcgFine G, VLev<T> L0)
     }
 }
 
+// w = M^-1 v on the BiCGStab path (a non-symmetric Poisson operator: AMR
+// interfaces): after the V-cycle on v, the finest level's post-smoothing
+// (k_pcg_z's arithmetic, without its reduction)
+__global__ void __launch_bounds__(kBlock) k_bi_amg_post(PcgFine G, VLev<double> L0, const double *__restrict__ v,
+                                                     double *__restrict__ w)
+{
+    pdl_wait();
+    Blk B;
+    if (pcg::load_blk(G.blk, G.S, B)) return;
+    const bool tail0 = G.S[B.inst].tail0;
+    const pcg::RowSet R = pcg::rowset(B);
+    double s[kRPT];
+    if (!tail0) pcg::trows(L0.At, R, s, [&](int j) { return L0.x[j]; });
+#pragma unroll
+    for (int q = 0; q < kRPT; q++) {
+        if (q >= R.nrow) break;
+        const int i = R.row[q];
+        w[i] = tail0 ? L0.out[i] : L0.x[i] + L0.dinv[i] * (v[i] - s[q]);
+    }
+}
+
 // p_new = z + beta p_old ; q = A p_new ; alpha = r.z / p.q
 __global__ void __launch_bounds__(kBlock) k_pcg_dir(PcgFine G, const double *__restrict__ po, double *__restrict__ pn)
 {
