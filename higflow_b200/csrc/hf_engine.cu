@@ -487,6 +487,8 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     const int f = e - pick<4>(P.off, d);
     const int nf = pick<3>(P.nf, d);
     const int32_t *__restrict__ sl = pick<3>(P.vslots, d);
+    const int inst = __ldg(pick<3>(P.finst, d) + f);
+    if (frozen(P, inst)) return;   // (before the slot loads: served batches hold frozen instances)
     // every slot code, then every slot value (a centre hit's field entry or a
     // general row's value from k_vrows), as independent loads issued together
     constexpr int NS = VE ? HF_V_NSLOT_VE(D) : HF_V_NSLOT_NEWT(D);
@@ -506,8 +508,6 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
 #define SLQ(s, fld) (val[s])
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
     const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
-    const int inst = __ldg(pick<3>(P.finst, d) + f);
-    if (frozen(P, inst)) return;
     const hf_params &par = P.ipar[inst];
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
@@ -2041,7 +2041,7 @@ int build_pcg(hf_case *C, const std::vector<int32_t> &mptr, const std::vector<in
         for (int i = 0; i < nf; i++) {
             key.clear();
             const int len = mptr[i + 1] - mptr[i];
-            if (len >= (1 << kTLenBits)) return fail(HF_ERR_UNSUPPORTED, "Poisson row with more than 63 entries");
+            if (len >= (1 << kTLenBits)) return fail(HF_ERR_UNSUPPORTED, "Poisson row with more than 127 entries");
             for (int k = mptr[i]; k < mptr[i + 1]; k++) {
                 const int32_t o = mcol[k] - i;
                 key.append((const char *)&o, sizeof o);
@@ -3505,10 +3505,18 @@ extern "C" int hf_case_create(const hf_program *pg, const hf_options *opt_in, hf
         if (C->bi_amg) {
             // the instance's hierarchy for the preconditioner; its CG state
             // stays idle (the instance is marked not done, so that the
-            // V-cycle kernels run on it)
-            if ((rc = build_pcg(C, mptr, mcol, mval, pins))) return cleanup(rc);
-            if (cudaMemsetAsync(&C->G.S[0].done, 0, sizeof(int32_t), C->stream) != cudaSuccess)
+            // V-cycle kernels run on it).  An operator the hierarchy's row
+            // encoding cannot hold keeps the Jacobi scaling.
+            rc = build_pcg(C, mptr, mcol, mval, pins);
+            if (rc == HF_ERR_UNSUPPORTED) {
+                C->bi_amg = false;
+                C->amg = false;
+                rc = HF_OK;
+            } else if (rc) {
+                return cleanup(rc);
+            } else if (cudaMemsetAsync(&C->G.S[0].done, 0, sizeof(int32_t), C->stream) != cudaSuccess) {
                 return cleanup(fail(HF_ERR_CUDA, "preconditioner state"));
+            }
         }
     }
 #undef UP

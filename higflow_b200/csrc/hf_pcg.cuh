@@ -105,7 +105,7 @@ struct Ctl {
 // templates per instance cover every row, so a row costs one 4-byte word
 // instead of its CSR columns and values (and one dependent load less than a
 // template index would).
-constexpr int kTLenBits = 6;   // rows of up to 63 entries
+constexpr int kTLenBits = 7;   // rows of up to 127 entries (AMR interface rows reach 75), 2^25 entries
 
 template <typename T>
 struct TRows {
