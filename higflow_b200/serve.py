@@ -2,8 +2,7 @@
 
 Requests (a recorded step program, a step count, optional initial fields)
 arrive at any time.  The scheduler groups the waiting requests that can share a
-batch (same dimension, flow type and time schemes) and have step counts within
-a factor of two of each other into a cohort: their
+batch (same dimension, flow type and time schemes) into a cohort: their
 programs are concatenated into one batch program and run as one engine case
 (hf_case_*: every kernel of a step covers all of the cohort's instances, one
 CUDA graph launch per step), each instance with its own step limit
@@ -42,12 +41,6 @@ def batch_key(prog: hp.Program):
     p = prog.par
     return (prog.dim, int(p["flowtype"]), int(p.get("tempdiscrtype", 0)), int(p.get("ve_discrtype", 0)))
 
-
-def step_class(steps: int) -> int:
-    """Requests of one cohort have step counts within a factor of two: a
-    cohort runs until its longest request is done, and an instance that has
-    taken its steps still costs the cohort part of a step."""
-    return max(1, int(steps)).bit_length()
 
 
 @dataclass
@@ -194,10 +187,9 @@ class BatchServer:
             return None
         held = sum(c.nbytes for c in self.cohorts)
         key = batch_key(self.queue[0].prog)
-        cls = step_class(self.queue[0].steps)
         pick, cells, est = [], 0, 0
         for r in list(self.queue):
-            if batch_key(r.prog) != key or step_class(r.steps) != cls:
+            if batch_key(r.prog) != key:
                 continue
             need = engine.device_bytes(r.prog, self.opts) * 3 // 2
             if pick and (cells + r.prog.ncell > self.max_cells or held + est + need > self.budget):
