@@ -721,8 +721,10 @@ __global__ void __launch_bounds__(kBlock) k_gptt_ml(DevProg P, DevFields F)
 // IMPL: the implicit constitutive step (hf_params.ve_discrtype, the same for
 // every instance of a case), a separate instantiation so that the explicit
 // kernel carries none of its code
-// MIX: the mixed form, whose CUBISTA cell convection is evaluated in FP32 (the
-// eigensystem, kernel transform and time update stay FP64)
+// MIX: the mixed form, whose CUBISTA cell convection is evaluated in FP32 and
+// whose velocity derivatives and M/De term multiply by reciprocals (within one
+// rounding of the quotients; the eigensystem, kernel transform and time
+// update stay FP64 and as the reference computes them)
 template <int D, bool IMPL, bool MIX>
 __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P, DevFields F)
 {
@@ -783,7 +785,8 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
                     vll = vu[Q + 3];
                     ur = 0.25 * (vll + vl[dim] + vr[dim] + vrr);
                 }
-                Du[dim][dim2] = (ur - ul) / (2.0 * 0.5 * cd[dim2]);
+                // (mixed form: times the reciprocal spacing, within one rounding)
+                Du[dim][dim2] = MIX ? (ur - ul) * (1.0 / cd[dim2]) : (ur - ul) / (2.0 * 0.5 * cd[dim2]);
                 F.Du[dim * D + dim2][cc] = Du[dim][dim2];
             }
         }
@@ -791,6 +794,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
     // constitutive step (hig-flow-step-viscoelastic.c:384-521); the self slot
     // is the cell's own index (checked at create)
     const double Re = pr.Re, De = pr.De, tol = pr.kernel_tol, small = HF_EPSMACH;
+    const double iDe = MIX ? 1.0 / De : 0.0;
     double S[D][D], K[D][D], KC[D][D];
     double trS = 0.0;
 #pragma unroll
@@ -879,7 +883,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
 #pragma unroll
         for (int j = 0; j < D; j++) {
             if (implicit) {
-                RHS[i][j] = 2.0 * BB[i][j] + MM[i][j] / De;
+                RHS[i][j] = 2.0 * BB[i][j] + (MIX ? MM[i][j] * iDe : MM[i][j] / De);
                 continue;
             }
             double ok = 0.0, ko = 0.0;
@@ -888,7 +892,7 @@ __global__ void __launch_bounds__(kVeBlock, D == 2 ? 8 : 4) k_ve_cell(DevProg P,
                 ok += Om[i][k] * K[k][j];
                 ko += K[i][k] * Om[k][j];
             }
-            RHS[i][j] = ok - ko + 2.0 * BB[i][j] + MM[i][j] / De;
+            RHS[i][j] = ok - ko + 2.0 * BB[i][j] + (MIX ? MM[i][j] * iDe : MM[i][j] / De);
         }
     // the kernel's neighbour values: per direction KL, KR, KLL, KRR (the same
     // codes for every component; a general row's pairs are the upper
