@@ -674,8 +674,22 @@ def served(args, device, rtol):
 
 
 def end_to_end(case, prog, args, world, device):
-    """The metric through the C ABI with pinned host buffers: every step copies
-    the state fields host -> device, steps, and copies them back."""
+    """The metric through the C ABI with pinned host buffers, two ways.
+
+    value: the drop-in's call pattern (higflow_b200/binding/hf_attach.c: the
+    fields stay on the device between the host's output points, as HigFlow's
+    main loop reads them only to print or save).  Every step copies each
+    instance's time step host -> device (hf_case_set_timestep uploads the
+    instances' parameters, as the host sets ns->par.dt; not for the
+    semi-implicit forms, whose dt is fixed), steps, and reads the step's
+    result back (hf_case_stats:
+    the Poisson iterations and residual that hf_step hands to the solver
+    parameters); the host's output point (hf_sync_to_host: u, p and the
+    kernel tensor, device -> host) comes once per timed region, i.e. every
+    args.steps steps.
+
+    full_state_every_step: every step copies the state fields host -> device,
+    steps, and copies them back (a host that edits the fields between steps)."""
     import ctypes as C
     import torch
     from higflow_b200 import engine
@@ -689,23 +703,52 @@ def end_to_end(case, prog, args, world, device):
         n = prog.field_size(fid, comp)
         pinned[(fid, comp)] = torch.empty(n, dtype=torch.float64, pin_memory=True)
         pinned[(fid, comp)].numpy()[:] = case.get(fid, comp)
-    h2d = sum(v.numel() * 8 for v in pinned.values())
+    fields = sum(v.numel() * 8 for v in pinned.values())
+    ninst = case.instances()
+    dts = torch.empty(ninst, dtype=torch.float64, pin_memory=True)
+    dts.numpy()[:] = [p["dt"] for p in prog.inst_par] if prog.inst_par else [prog.par["dt"]]
     L = engine.lib()
+    st = hp.HFStats()
+
+    def put(fid, comp, buf):
+        engine._check(L.hf_case_set_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
+                                          buf.numel()))
+
+    def get(fid, comp, buf):
+        engine._check(L.hf_case_get_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
+                                          buf.numel()))
+
+    # the drop-in's pattern
+    _barrier(world)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        engine._check(L.hf_case_set_timestep(case.h, C.cast(dts.data_ptr(), C.POINTER(C.c_double)), ninst))
+        engine._check(L.hf_case_step(case.h, 1))
+        engine._check(L.hf_case_stats(case.h, C.byref(st)))
+    for (fid, comp), buf in pinned.items():
+        get(fid, comp, buf)
+    t_plugin = _max_over_ranks(time.perf_counter() - t0, world, device)
+    # the whole state both ways every step
     _barrier(world)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     for k in range(args.steps):
         for (fid, comp), buf in pinned.items():
-            engine._check(L.hf_case_set_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
-                                              buf.numel()))
+            put(fid, comp, buf)
         case.step(1)
         for (fid, comp), buf in pinned.items():
-            engine._check(L.hf_case_get_field(case.h, fid, comp, C.cast(buf.data_ptr(), C.POINTER(C.c_double)),
-                                              buf.numel()))
-    t_e2e = _max_over_ranks(time.perf_counter() - t0, world, device)
-    e2e = {"value": cells * args.steps * world / t_e2e, "unit": UNIT,
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d}
-    return e2e
+            get(fid, comp, buf)
+    t_full = _max_over_ranks(time.perf_counter() - t0, world, device)
+    stats_bytes = C.sizeof(hp.HFStats) + 80 * ninst   # the stats struct and the instance scalars it reads
+    sie = int(prog.par.get("tempdiscrtype", 0)) in (hp.SEMI_IMPLICIT_EULER, hp.SEMI_IMPLICIT_CN, hp.SEMI_IMPLICIT_BDF2)
+    return {"value": cells * args.steps * world / t_plugin, "unit": UNIT,
+            "h2d_bytes_per_step": 0 if sie else C.sizeof(hp.HFParams) * ninst,
+            "d2h_bytes_per_step": stats_bytes + fields // args.steps,
+            "pattern": f"drop-in: per step the time steps in, one step, the step's solver result out; u, p and the "
+                       f"kernel tensor out once per {args.steps} steps (the host's output point)",
+            "full_state_every_step": {"value": cells * args.steps * world / t_full, "unit": UNIT,
+                                      "h2d_bytes_per_step": fields, "d2h_bytes_per_step": fields}}
 
 
 # ---------------------------------------------------------------------------

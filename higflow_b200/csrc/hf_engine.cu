@@ -487,8 +487,6 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     const int f = e - pick<4>(P.off, d);
     const int nf = pick<3>(P.nf, d);
     const int32_t *__restrict__ sl = pick<3>(P.vslots, d);
-    const int inst = __ldg(pick<3>(P.finst, d) + f);
-    if (frozen(P, inst)) return;   // (before the slot loads: served batches hold frozen instances)
     // every slot code, then every slot value (a centre hit's field entry or a
     // general row's value from k_vrows), as independent loads issued together
     constexpr int NS = VE ? HF_V_NSLOT_VE(D) : HF_V_NSLOT_NEWT(D);
@@ -508,6 +506,8 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
 #define SLQ(s, fld) (val[s])
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
     const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
+    const int inst = __ldg(pick<3>(P.finst, d) + f);
+    if (frozen(P, inst)) return;
     const hf_params &par = P.ipar[inst];
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
@@ -3711,8 +3711,12 @@ extern "C" int hf_case_set_timestep(hf_case *C, const double *dt, int32_t n)
         if (!(dt[i] > 0.0) || !std::isfinite(dt[i])) return fail(HF_ERR_INVALID, "time step must be positive and finite");
         same = same && dt[i] == C->h_ipar[i].dt;
     }
-    if (same) return HF_OK;
-    if (C->sie) return fail(HF_ERR_UNSUPPORTED, "new time step with the semi-implicit velocity (its matrix holds dt)");
+    if (C->sie) {
+        if (same) return HF_OK;
+        return fail(HF_ERR_UNSUPPORTED, "new time step with the semi-implicit velocity (its matrix holds dt)");
+    }
+    // (the parameters go to the device on every call, as the host's dt of
+    // each step; no step of this case is in flight past the synchronisation)
     for (int i = 0; i < n; i++) C->h_ipar[i].dt = dt[i];
     HF_CK(cudaMemcpyAsync((void *)C->P.ipar, C->h_ipar.data(), sizeof(hf_params) * n, cudaMemcpyHostToDevice,
                           C->stream));

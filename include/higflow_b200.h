@@ -364,8 +364,10 @@ int  hf_case_adjust_timestep(hf_case *c, double *cfl, double *dt, int32_t n);
 
 /* Set each instance's time step (n = ninst) for the next steps, as a case main
  * loop does when it changes ns->par.dt (higflow_adjust_timestep,
- * hig-flow-timestep.c:115-139, or a restart); HF_ERR_UNSUPPORTED for the
- * semi-implicit velocity when dt changes (its system matrix holds dt). */
+ * hig-flow-timestep.c:115-139, or a restart); the instances' parameters go to
+ * the device on every call (it waits for the case's stream).
+ * HF_ERR_UNSUPPORTED for the semi-implicit velocity when dt changes (its
+ * system matrix holds dt; an unchanged dt is accepted and not copied). */
 int  hf_case_set_timestep(hf_case *c, const double *dt, int32_t n);
 
 /* Per-instance step limits (no counterpart in the reference, which runs one
