@@ -92,7 +92,21 @@ struct PairRows {
     const int32_t *pcol0;
     const double *sw;
     double *val;
+    // under step limits (null otherwise): a pair of a frozen instance is
+    // skipped, its instance found from its first column's element
+    const int64_t *ilim;
+    const int32_t *finst[3];
+    const int32_t *cinst;
 };
+
+// the instance of a pair whose first column is `col` in the field of `tag`
+// (vtag_field's numbering: facet fields FU[d] 0-2 and u[d] 5-7, the rest cells)
+__device__ __forceinline__ int pair_inst(const int32_t *const finst[3], const int32_t *cinst, int tag, int col)
+{
+    if (tag <= 2) return __ldg(finst[tag] + col);
+    if (tag >= 5 && tag <= 7) return __ldg(finst[tag - 5] + col);
+    return __ldg(cinst + col);
+}
 
 // The mixed form's velocity-stage pairs by FP32 pattern.  The interpolation
 // weights HigTree computes for each row differ from row to row in their last
@@ -120,6 +134,9 @@ struct PatRows {
     const uint8_t *plen;    // per pattern: entry count
     const PatEntry *ent;
     double *val;
+    const int64_t *ilim;        // as in PairRows
+    const int32_t *finst[3];
+    const int32_t *cinst;
 };
 
 struct DevProg {
@@ -351,10 +368,15 @@ __global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= R.n) return;
-    const double *__restrict__ fb = vtag_field(F, __ldg(R.tag + u));
+    const int tag = __ldg(R.tag + u);
+    const double *__restrict__ fb = vtag_field(F, tag);
     if (C16) fb += __ldg(R.pcol0 + u);
     const int n = __ldg(R.plen + u);
     const int64_t e0 = __ldg(R.sptr + (u >> 5)) + (u & 31);
+    if (R.ilim && n > 0) {
+        const int c0 = C16 ? __ldg(R.pcol0 + u) + (int)__ldg(R.scol16 + e0) : __ldg(R.scol + e0);
+        if (__ldg(R.ilim + pair_inst(R.finst, R.cinst, tag, c0)) == 0) return;
+    }
     double res = 0.0;
     res += -__ldg(R.rhs + u);
     // the entries stream through once (evict-first loads keep L1 for the
@@ -380,7 +402,9 @@ __global__ void __launch_bounds__(512) k_vrows_pat(PatRows R, DevFields F)
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= R.n) return;
     const int p = __ldg(R.pid + u);
-    const double *__restrict__ fb = vtag_field(F, __ldg(R.tag + u)) + __ldg(R.col0 + u);
+    const int tag = __ldg(R.tag + u), c0 = __ldg(R.col0 + u);
+    if (R.ilim && __ldg(R.ilim + pair_inst(R.finst, R.cinst, tag, c0)) == 0) return;
+    const double *__restrict__ fb = vtag_field(F, tag) + c0;
     const int e0 = __ldg(R.pstart + p), n = __ldg(R.plen + p);
     const int2 *__restrict__ ent = reinterpret_cast<const int2 *>(R.ent) + e0;
     double res = 0.0;
@@ -487,6 +511,12 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
     const int f = e - pick<4>(P.off, d);
     const int nf = pick<3>(P.nf, d);
     const int32_t *__restrict__ sl = pick<3>(P.vslots, d);
+    int inst = -1;
+    if (P.ilim) {
+        // under step limits a frozen instance's facets skip their loads
+        inst = __ldg(pick<3>(P.finst, d) + f);
+        if (frozen(P, inst)) return;
+    }
     // every slot code, then every slot value (a centre hit's field entry or a
     // general row's value from k_vrows), as independent loads issued together
     constexpr int NS = VE ? HF_V_NSLOT_VE(D) : HF_V_NSLOT_NEWT(D);
@@ -506,8 +536,7 @@ __global__ void __launch_bounds__(256) k_velocity(DevProg P, DevFields F)
 #define SLQ(s, fld) (val[s])
     const double *fd = P.delta + (size_t)__ldg(pick<3>(P.vdelta, d) + f) * D;
     const uint32_t fl = __ldg(pick<3>(P.vflags, d) + f);
-    const int inst = __ldg(pick<3>(P.finst, d) + f);
-    if (frozen(P, inst)) return;
+    if (inst < 0) inst = __ldg(pick<3>(P.finst, d) + f);
     const hf_params &par = P.ipar[inst];
     int convec = par.convecdiscrtype;
     const int second = par.secondconvecdiscrtype;
@@ -3751,6 +3780,15 @@ extern "C" int hf_case_set_step_limits(hf_case *C, const int64_t *steps, int32_t
         C->bytes += bytes;
         C->P.ilim = C->ilim;
         C->G.ilim = C->ilim;
+        // the row-pair kernels skip frozen instances' pairs too
+        for (PairRows *R : {&C->P.vr, &C->P.cr}) {
+            R->ilim = C->ilim;
+            for (int d = 0; d < 3; d++) R->finst[d] = C->P.finst[d];
+            R->cinst = C->P.cinst;
+        }
+        C->vp.ilim = C->ilim;
+        for (int d = 0; d < 3; d++) C->vp.finst[d] = C->P.finst[d];
+        C->vp.cinst = C->P.cinst;
         destroy_graphs(C);   // the captured kernels hold the parameters without limits
     } else {
         HF_CK(cudaMemcpyAsync(C->ilim, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, C->stream));
