@@ -2272,28 +2272,6 @@ void launch_pdl(void (*kern)(KArgs...), int grid, int block, cudaStream_t st, Ar
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
-// The multigrid tail: one cluster of kTailCluster CTAs per instance, with
-// programmatic stream serialization like the loop's other kernels
-template <typename T, typename R>
-void launch_tail(int ninst, cudaStream_t st, const VLev<T> *H, const TailInst<T> *ti, const R *r0, const IScal *S)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(ninst * kTailCluster));
-    cfg.blockDim = dim3((unsigned)kTailThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[2];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kTailCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[1].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 2;
-    cudaLaunchKernelEx(&cfg, k_vc_tail<T, R>, H, ti, r0, S);
-}
-
 template <typename T, typename R>
 void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T> *H, const TailInst<T> *ti,
                     const R *r0, int &kernels)
@@ -2312,7 +2290,7 @@ void enqueue_vcycle(hf_case *C, cudaStream_t st, const VLev<T> *L, const VLev<T>
         }
     }
     // the small levels: one CTA per instance
-    launch_tail<T, R>(C->ninst, st, H, ti, r0, S);
+    launch_pdl(k_vc_tail<T, R>, C->ninst, kTailThreads, st, H, ti, r0, S);
     kernels++;
     for (int l = C->nreg - 1; l >= 0; l--) {
         if (!L[l].nsblk) continue;

@@ -182,16 +182,14 @@ struct VLev {
 
 // The small levels of one instance, from the first level with at most
 // kTailRows rows (s) down to its coarsest (clev, dense inverse), run by one
-// thread-block cluster of kTailCluster CTAs: phases separated by cluster
-// barriers instead of kernel launches.  2048 rows over the cluster's 2048
-// threads: a tail phase is at most one row per thread, so its dependent load
-// chains stay short, and every level that small leaves the level-synchronous
-// kernels (on the batched cavities of 32^2 to 256^2 cells that takes the third
-// level out of them: four launches fewer per CG iteration).  Larger levels run
-// level-synchronously.
-constexpr int kTailRows = 2048;
-constexpr int kTailCluster = 8;        // CTAs per instance (a portable cluster size)
-constexpr int kTailThreads = 256;      // threads per CTA
+// CTA: phases separated by __syncthreads instead of kernel launches.
+// 256 rows: a tail phase is then at most one row per thread, so the tail's
+// dependent load chains stay short; larger levels run level-synchronously
+// (measured on the batched cavities: taking levels of up to 2048 rows into
+// the tail saves four launches per CG iteration but doubles the tail's time,
+// 2.74 against 2.68 ms of Poisson iterations per step)
+constexpr int kTailRows = 256;
+constexpr int kTailThreads = 512;
 
 template <typename T>
 struct TailInst {
@@ -531,18 +529,12 @@ __global__ void __launch_bounds__(kBlock) k_vc_restrict(VLev<T> L, VLev<T> Ln, c
 }
 
 // The V-cycle of one instance from its tail level s down to its coarsest level
-// and back, one cluster of kTailCluster CTAs per instance (the clusters are
-// consecutive blocks: cluster c serves TI[c]).  H: the level table in device
-// memory; each CTA copies a level's descriptor to shared memory when it gets
-// there (a dynamic index into the kernel parameters would spill them).  Level
-// s's b is the regular restriction's output (or the CG residual when s is the
-// finest level); level s's out is the correction the regular prolongation
-// reads.  Same arithmetic as the level-synchronous kernels; the dense solve
-// splits each row over a warp.  Between phases every thread fences its
-// global writes and the cluster meets at its barrier: a phase reads what
-// other CTAs of the cluster wrote in the phase before.  The instance's done
-// flag is read once and is the same for every CTA of the cluster, so either
-// all of them return at the start or none does.
+// and back, one CTA per instance (H: the level table in device memory; levels
+// are copied to shared memory one at a time, a dynamic index into the kernel
+// parameters would spill them).  Level s's b is the regular restriction's
+// output (or the CG residual when s is the finest level); level s's out is the
+// correction the regular prolongation reads.  Same arithmetic as the
+// level-synchronous kernels; the dense solve splits each row over a warp.
 template <typename T, typename R = double>
 __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, const TailInst<T> *TI,
                                                         const R *__restrict__ r0, const IScal *S)
@@ -553,28 +545,21 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
     __shared__ int done;
     __shared__ T sb[kCoarseCap];
     if (threadIdx.x == 0) {
-        ti = TI[blockIdx.x / kTailCluster];
+        ti = TI[blockIdx.x];
         done = ((volatile const IScal *)S)[ti.inst].done;
     }
     __syncthreads();
     if (done) return;
-    constexpr int NT = kTailCluster * kTailThreads;
-    uint32_t rank;
-    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-    const int tid = (int)rank * kTailThreads + threadIdx.x;
-    auto phase_end = [&]() {
-        __threadfence();
-        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-    };
+    const int tid = threadIdx.x;
     // down: x = w D^-1 b, r = b - A x, b_next = R r
     for (int l = ti.s; l < ti.clev; l++) {
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             L = H[l];
             Ln = H[l + 1];
         }
         __syncthreads();
         const int a = ti.row0[l], e = a + ti.nrow[l];
-        for (int i = a + tid; i < e; i += NT) {
+        for (int i = a + tid; i < e; i += kTailThreads) {
             T bi, s = T(0);
             if (l == 0) {
                 bi = T(r0[i]);
@@ -589,24 +574,24 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
             L.x[i] = L.dinv[i] * bi;
             L.r[i] = bi - s;
         }
-        phase_end();
+        __syncthreads();
         const int an = ti.row0[l + 1], en = an + ti.nrow[l + 1];
-        for (int i = an + tid; i < en; i += NT) {
+        for (int i = an + tid; i < en; i += kTailThreads) {
             T s = T(0);
             for (int k = L.Rp[i]; k < L.Rp[i + 1]; k++) s += L.Rv[k] * L.r[L.Rc[k]];
             Ln.b[i] = s;
         }
-        phase_end();
+        __syncthreads();
     }
     // coarsest: out = inv b, one warp per row, lanes over the row
     {
-        if (threadIdx.x == 0) L = H[ti.clev];
+        if (tid == 0) L = H[ti.clev];
         __syncthreads();
         const int a = ti.row0[ti.clev], cn = ti.nrow[ti.clev];
-        for (int i = threadIdx.x; i < cn; i += kTailThreads) sb[i] = ti.clev == 0 ? T(r0[a + i]) : L.b[a + i];
+        for (int i = tid; i < cn; i += kTailThreads) sb[i] = ti.clev == 0 ? T(r0[a + i]) : L.b[a + i];
         __syncthreads();
-        const int lane = threadIdx.x & 31, warp = tid >> 5;
-        for (int i = warp; i < cn; i += NT / 32) {
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int i = warp; i < cn; i += kTailThreads / 32) {
             const T *row = ti.inv + (size_t)i * cn;
             T s = T(0);
             for (int k = lane; k < cn; k += 32) s += row[k] * sb[k];
@@ -614,23 +599,23 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) L.out[a + i] = s;
         }
-        phase_end();
+        __syncthreads();
     }
     // up: x += P e, out = x + w D^-1 (b - A x)
     for (int l = ti.clev - 1; l >= ti.s; l--) {
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             L = H[l];
             Ln = H[l + 1];
         }
         __syncthreads();
         const int a = ti.row0[l], e = a + ti.nrow[l];
-        for (int i = a + tid; i < e; i += NT) {
+        for (int i = a + tid; i < e; i += kTailThreads) {
             T s = T(0);
             for (int k = L.Pp[i]; k < L.Pp[i + 1]; k++) s += L.Pv[k] * Ln.out[L.Pc[k]];
             L.x[i] += s;
         }
-        phase_end();
-        for (int i = a + tid; i < e; i += NT) {
+        __syncthreads();
+        for (int i = a + tid; i < e; i += kTailThreads) {
             T bi, s;
             if (l == 0) {
                 bi = T(r0[i]);
@@ -642,7 +627,7 @@ __global__ void __launch_bounds__(kTailThreads) k_vc_tail(const VLev<T> *H, cons
             }
             L.out[i] = L.x[i] + L.dinv[i] * (bi - s);
         }
-        phase_end();
+        __syncthreads();
     }
 }
 
