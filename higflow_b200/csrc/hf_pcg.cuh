@@ -462,9 +462,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(DevProg P, DevFields F, Pcg
         s.bb = tot[1];
         const double t = fmax(G.rtol * sqrt(tot[1]), G.atol);
         s.tol2 = t * t;
-        // the inner sweep aims at half the outer target (its FP32 recurrence
-        // drifts from the true residual), or eta of where it starts
-        s.tol2in = G.r32 ? fmax(0.25 * s.tol2, G.eta * G.eta * tot[0]) : s.tol2;
+        // the inner sweep aims at the outer target, or eta of where it starts
+        s.tol2in = G.r32 ? fmax(s.tol2, G.eta * G.eta * tot[0]) : s.tol2;
         s.outer = 0;
         s.iters_prev = 0;
         s.fin = 0;
@@ -919,9 +918,12 @@ __global__ void __launch_bounds__(kBlock) k_step_end(PcgFine G)
 // ---------------------------------------------------------------------------
 // Each sweep runs the CG recurrences of the plain form in FP32 (vectors r32,
 // z32, q32, directions, e32; the finest operator's FP32 templates; the FP32
-// V-cycle) from e = 0 until ||r32|| <= max(eta ||r||, outer target / 2) or the
-// sweep's iteration cap (the sweep aims at half the outer target, so that one
-// correction usually meets it); then k_ir_correct adds e to the FP64 unknown and
+// V-cycle) from e = 0 until ||r32|| <= max(eta ||r||, outer target) or the
+// sweep's iteration cap (measured on the batched cavities: aiming at the outer
+// target itself, one correction still meets the FP64 test at nearly every
+// step, with 7.6 CG iterations per instance-step in the first steps and 3.8
+// later, against 8.0 and 4.1 when aiming at half of it; a second sweep runs
+// when it does not); then k_ir_correct adds e to the FP64 unknown and
 // updates the FP64 residual r -= A e with the FP64 operator, which decides
 // convergence against the plain form's test.  Dot products of FP32 vectors
 // are accumulated in FP64.
@@ -1118,7 +1120,7 @@ __global__ void __launch_bounds__(kBlock) k_ir_correct(PcgFine G, cudaGraphCondi
                 s.iters_prev += s.iters;
                 s.iters = 0;
                 s.beta = 0.0;
-                s.tol2in = fmax(0.25 * s.tol2, G.eta * G.eta * tot[0]);
+                s.tol2in = fmax(s.tol2, G.eta * G.eta * tot[0]);
                 s.done = 0;
                 atomicAdd(&G.ctl->active, 1);
             }
