@@ -554,7 +554,7 @@ def run_b200(args, rank, world, device):
     if mixed and wl.get("batch") == "c4" and not args.no_extras:
         extra["whole_configuration"] = whole_configuration(prog, rtol, workloads.batched_giesekus()[0].steps, world,
                                                            device)
-    if mixed and wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras:
+    if mixed and wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras and world == 1:
         draws = workloads.batched_giesekus()
         one = plain_one_case_at_a_time(draws, rtol["plain"], device)
         one["mixed_batched_over_it"] = value / one["value"]
@@ -604,7 +604,10 @@ def run_b200(args, rank, world, device):
         "host": host_info(),
     }
     line.update(extra)
-    if wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras and not args.no_serve:
+    # the served stream and the one-case-at-a-time comparison are one-device
+    # measurements: they run at N = 1 only
+    if (wl.get("batch") == "c4" and wl.get("count", 256) == 256 and not args.no_extras and not args.no_serve
+            and world == 1):
         try:
             line["served"] = served(args, device, rtol["mixed"])
             line["served"]["over_batched"] = line["served"]["cell_steps_per_s"] / value
