@@ -46,22 +46,6 @@ __device__ __forceinline__ W query(const Rows<W> &R, int32_t code, const F *__re
     return res;
 }
 
-// The same value with the general-row evaluation out of line, for call sites
-// where general rows are rare (cells away from boundaries hit centres): the
-// caller's code stays small, which matters in kernels with many query sites.
-template <typename W, typename F>
-__device__ __noinline__ W query_row(const Rows<W> R, int32_t code, const F *__restrict__ f)
-{
-    return query<W, F>(R, code, f);
-}
-
-template <typename W, typename F>
-__device__ __forceinline__ W query_cold(const Rows<W> &R, int32_t code, const F *__restrict__ f)
-{
-    if (code >= 0) return (W)__ldg(f + code);
-    return query_row<W, F>(R, code, f);
-}
-
 // hig_flow_jacobi (hig-flow-step-viscoelastic.c:1517-1600): cyclic Jacobi with
 // the reference's thresholds and sweep limit.
 template <int D>
