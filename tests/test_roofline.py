@@ -40,3 +40,19 @@ def test_velocity_rows_and_widths():
     ws = roofline.whole_step(p, False, iters=3.0)
     assert ws["bytes"] == pytest.approx(ws["fixed"] + 3.0 * roofline.poisson_iter_bytes(p, 8))
     assert roofline.poisson_iter_bytes(p, 8) == 4 * (p.ncell + 1) + p.p_col.size * 12 + 13 * 8 * p.ncell
+
+
+def test_bench_phase_bytes_split_the_stages():
+    """The per-kernel figures the bench line reports beside the phases:
+    velocity_rows is the velocity stage's stencil rows alone, ve_cell_main the
+    cell stage without its polymeric-tensor pass (8 D^2 x 3 bytes per cell)."""
+    import bench
+    p = _prog()
+    for mixed in (False, True):
+        pb, sb = bench.phase_bytes(p, mixed, iters_per_step=2.0, sweeps_per_step=1.0 if mixed else 0.0)
+        w = 4 if mixed else 8
+        v = sb["velocity"]
+        assert pb["velocity_rows"] == 4 * v["rows"] + v["row_entries"] * (4 + w)
+        assert 0 < pb["velocity_rows"] < pb["velocity"]
+        assert pb["ve_cell_main"] == pb["ve_cell"] - 8 * 4 * p.ncell * 3
+        assert pb["poisson_iter"] > 2.0 * roofline.poisson_iter_bytes(p, w) - 1
