@@ -141,3 +141,30 @@ def test_launch_shape_tuning_changes_no_result():
         case.close()
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_a_failed_instance_under_step_limits_is_frozen_alone():
+    """Under step limits an instance whose step fails (here a NaN in its
+    initial velocity) is frozen at that step and reported by
+    hf_case_instance_failures; the step call returns the failure; the other
+    instances go on and equal their runs alone (1e-10 relative L2)."""
+    names = VE_NAMES[:3]
+    progs, datas = zip(*[load_golden(n) for n in names])
+    batch = hp.Program.concatenate(progs)
+    case = engine.Case(batch, engine.options(rtol=1e-13, atol=1e-300))
+    for key, fid, comp in field_keys(progs[0]):
+        whole = np.concatenate([d["init_" + key] for d in datas])
+        if key == "u0":
+            whole[batch.facet_off[0][1] + 3] = np.nan      # instance 1
+        case.set(fid, comp, whole)
+    case.set_step_limits([4, 4, 4])
+    with pytest.raises(engine.EngineError) as e:
+        case.step(4)
+    assert e.value.code == -4
+    assert list(case.instance_failures()) == [0, -4, 0]
+    for i in (0, 2):
+        alone = _run_alone(names[i], 4)
+        got = {k: case.get_instance(fid, comp, i) for k, fid, comp in field_keys(progs[i])}
+        err = compare(got, alone, _keys(progs[i]))
+        assert max(err.values()) < 1e-10, (names[i], err)
+    case.close()
