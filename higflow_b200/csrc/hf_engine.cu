@@ -74,9 +74,11 @@ constexpr int kBlock = 256;
 // use into val: pair u's value is -rhs[u] + sum_k w_k * field(tag[u])[col_k]
 // in stencil order (dp_interpolate_from_stencil, pdomain.c:1026-1053).  Slot
 // codes of the kernels that read them index the pairs.  Sliced layout
-// (SELL-32): pair u is lane u % 32 of slice u / 32, and its entry k sits at
-// sptr[u / 32] + 32 k + u % 32, so a warp's k-th entries are one coalesced
-// load; plen[u] is the pair's entry count.  Columns are absolute (row base
+// (SELL-32, entries in pairs): pair u is lane l = u % 32 of slice u / 32, and
+// its entries 2j and 2j + 1 sit side by side at sptr[u / 32] + 64 j + 2 l, so
+// a warp reads two entries of its 32 pairs with one coalesced 16-byte weight
+// load and one 4-byte (or 8-byte) column load per thread; slices are padded
+// to an even length; plen[u] is the pair's entry count.  Columns are absolute (row base
 // added) in scol, or, when every pair's entries lie within +-32767 of its
 // first column pcol0[u] (interpolation stencils are local: 2D meshes up to
 // several thousand cells a side), 16-bit offsets in scol16 (scol null).
@@ -103,8 +105,10 @@ struct PairRows {
 // (vtag_field's numbering: facet fields FU[d] 0-2 and u[d] 5-7, the rest cells)
 __device__ __forceinline__ int pair_inst(const int32_t *const finst[3], const int32_t *cinst, int tag, int col)
 {
-    if (tag <= 2) return __ldg(finst[tag] + col);
-    if (tag >= 5 && tag <= 7) return __ldg(finst[tag - 5] + col);
+    // (selects, not a dynamic index: that would copy the parameters to local memory)
+    const int d = tag <= 2 ? tag : tag - 5;
+    const int32_t *fi = d == 0 ? finst[0] : d == 1 ? finst[1] : finst[2];
+    if (tag <= 2 || (tag >= 5 && tag <= 7)) return __ldg(fi + col);
     return __ldg(cinst + col);
 }
 
@@ -372,20 +376,31 @@ __global__ void __launch_bounds__(512) k_vrows(PairRows R, DevFields F)
     const double *__restrict__ fb = vtag_field(F, tag);
     if (C16) fb += __ldg(R.pcol0 + u);
     const int n = __ldg(R.plen + u);
-    const int64_t e0 = __ldg(R.sptr + (u >> 5)) + (u & 31);
+    const int64_t e0 = __ldg(R.sptr + (u >> 5)) + 2 * (u & 31);
     if (R.ilim && n > 0) {
         const int c0 = C16 ? __ldg(R.pcol0 + u) + (int)__ldg(R.scol16 + e0) : __ldg(R.scol + e0);
         if (__ldg(R.ilim + pair_inst(R.finst, R.cinst, tag, c0)) == 0) return;
     }
+    const double2 *__restrict__ w2 = reinterpret_cast<const double2 *>(R.sw + e0);
     double res = 0.0;
     res += -__ldg(R.rhs + u);
     // the entries stream through once (evict-first loads keep L1 for the
-    // field gathers); eight entries' loads in flight per thread
-#pragma unroll 8
-    for (int k = 0; k < n; k++) {
-        const int64_t at = e0 + 32 * (int64_t)k;
-        const int c = C16 ? (int)__ldcs(R.scol16 + at) : __ldcs(R.scol + at);
-        res += __ldg(fb + c) * __ldcs(R.sw + at);
+    // field gathers), two per load, eight entries' loads in flight per thread
+#pragma unroll 4
+    for (int j = 0; 2 * j < n; j++) {
+        const double2 w = __ldcs(w2 + 32 * j);
+        int ca, cb;
+        if (C16) {
+            const int c = __ldcs(reinterpret_cast<const int *>(R.scol16 + e0) + 32 * j);
+            ca = (int)(short)(c & 0xffff);
+            cb = c >> 16;
+        } else {
+            const int2 c = __ldcs(reinterpret_cast<const int2 *>(R.scol + e0) + 32 * j);
+            ca = c.x;
+            cb = c.y;
+        }
+        res += __ldg(fb + ca) * w.x;
+        if (2 * j + 1 < n) res += __ldg(fb + cb) * w.y;
     }
     R.val[u] = res;
 }
@@ -2986,7 +3001,7 @@ int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_progra
             plen[u] = (uint8_t)len;
             mx = std::max(mx, len);
         }
-        sptr[sl + 1] = sptr[sl] + 32 * mx;
+        sptr[sl + 1] = sptr[sl] + 32 * ((mx + 1) & ~(int64_t)1);   // entries in pairs (see PairRows)
     }
     const size_t ne = (size_t)sptr[nsl];
     // the columns: 16-bit offsets from the pair's first column when every
@@ -3006,8 +3021,8 @@ int build_pairs(hf_case *C, std::vector<void *> &own, double &B, const hf_progra
     std::vector<double> sw(ne, 0.0);
     for (size_t u = 0; u < np; u++) {
         const int64_t a0 = pg->tmpl_ptr[ptmpl[u]];
-        int64_t at = sptr[u / 32] + (int64_t)(u % 32);
-        for (int k = 0; k < plen[u]; k++, at += 32) {
+        for (int k = 0; k < plen[u]; k++) {
+            const int64_t at = sptr[u / 32] + 64 * (k / 2) + 2 * (int64_t)(u % 32) + (k % 2);
             const int64_t c = (int64_t)pbase[u] + pg->tmpl_col[a0 + k];
             if (c < 0 || c > INT32_MAX) return fail(HF_ERR_INVALID, std::string(what) + " column out of range");
             if (c16) scol16[at] = (int16_t)(c - pcol0[u]);
